@@ -1,0 +1,333 @@
+"""Throughput of the fusion hot path: frames/s of integrate + raycast.
+
+Workload (tabletop stream): 30 float32 point-map frames 640x480
+(fx=fy=525, cx=319.5, cy=239.5) ray traced from a seeded scene (plane y=0 +
+3 spheres), camera orbiting 1.0 m over 60 degrees, structured-light depth
+noise; voxel 4 mm, truncation 0.02 m, 200000 hash buckets, 200000 pool
+blocks; every frame is integrated, then ray cast at the same pose with
+min/max depth 0.2/3.0 m.  One step = reset + the whole 30-frame stream.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  --impl reference times the CPU restatement
+of the reference path (the reference has no CPU implementation of its own)
+on the host cores over a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "real-time-depth-fusion-directional-tsdf_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+sys.path.insert(0, PKG)
+
+import numpy as np  # noqa: E402
+
+METRIC = "frames/s integrate+raycast 640x480@4mm; batched & adjoint vs plain, same B200"
+WORKLOAD = "tabletop 30x640x480 point-map frames, voxel 4mm, trunc 0.02m, 200000 slots"
+VOXEL, TRUNC, SLOTS, BLOCKS = 0.004, 0.02, 200000, 200000
+MIN_D, MAX_D = 0.2, 3.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=30)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+               "--format=csv,noheader,nounits", "-lms", "100"]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thr = threading.Thread(target=self._read, daemon=True)
+            self.thr.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if "Active" in r[3 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_stream(args):
+    import synth
+
+    frames, K = synth.tabletop_stream(args.seed, args.frames)
+    return frames, K
+
+
+def cpu_baseline(frames, K, budget_s: float = 20.0) -> dict:
+    """Oracle (CPU restatement, OpenMP) on a bounded sample of the stream:
+    all frames integrated, a band of rows ray cast per frame."""
+    sys.path.insert(0, ORACLE)
+    import oracle
+
+    oracle.build()
+    threads = oracle.max_threads()
+    orc = oracle.OracleScene(VOXEL)
+    rows = 24
+    t_int = t_ren = 0.0
+    n = 0
+    for f in frames:
+        t0 = time.perf_counter()
+        orc.integrate(f.pointmap, f.rgb, TRUNC, f.pose, K.fx, K.fy, K.cx, K.cy)
+        t1 = time.perf_counter()
+        y0 = K.height // 2 - rows // 2
+        orc.render(K.width, K.height, f.pose, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D, rows=(y0, y0 + rows))
+        t2 = time.perf_counter()
+        t_int += t1 - t0
+        t_ren += (t2 - t1) * (K.height / rows)
+        n += 1
+        if t_int + t_ren > budget_s:
+            break
+    fps = n / (t_int + t_ren)
+    return {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
+            "sample": f"{n} frames integrated in full; ray cast on {rows} central rows per frame, "
+                      f"scaled to {K.height} rows"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    frames, K = make_stream(args)
+    res = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(frames[: max(2, min(len(frames), 4))], K, budget_s=15.0)
+        if i >= args.warmup:
+            res.append(r["value"])
+    v = statistics.median(res)
+    line = {"metric": METRIC, "value": v, "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "frames": args.frames, "sample": r["sample"]},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "frames/s", "cores": r["cores"], "kind": "port",
+                             "sample": r["sample"]},
+            "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    import vsg
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    frames, K = make_stream(args)
+    W, H = K.width, K.height
+    dev = [(torch.from_numpy(f.pointmap).cuda(), torch.from_numpy(f.rgb).cuda(),
+            torch.from_numpy(f.normals).cuda(), f.pose) for f in frames]
+    sc = vsg.Scene(voxel_size=VOXEL, truncation=TRUNC, hash_num_slots=SLOTS, num_sdf_blocks=BLOCKS)
+    rr = vsg.Renderer(W, H)
+
+    def step():
+        sc.reset()
+        for pm, rgb, nm, T in dev:
+            sc.integrate(pm, rgb, nm, W, H, TRUNC, T, K.fx, K.fy, K.cx, K.cy)
+            rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
+
+    # per-frame statistics (algorithmic bytes), outside the timed region
+    sc.reset()
+    per_frame = []
+    for pm, rgb, nm, T in dev:
+        sc.integrate(pm, rgb, nm, W, H, TRUNC, T, K.fx, K.fy, K.cx, K.cy)
+        rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
+        per_frame.append(sc.stats())
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            step()
+        ev1.record()
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    launches_per_step = 1 + len(dev) * (3 + 2)  # reset(3 kernels + memsets) + per frame
+    # per-kernel times (separate pass with events around each launch)
+    sc.timing(True)
+    sc.timing_reset()
+    step()
+    kms, kcnt = sc.timing_read()
+    sc.timing(False)
+    names = ["alloc", "integrate", "render"]
+    kern = {names[i]: {"ms_per_launch": float(kms[i] / max(kcnt[i], 1)), "launches": int(kcnt[i])}
+            for i in range(3)}
+    # algorithmic bytes per launch (canonical 8-B voxel)
+    npx = W * H
+    upd = np.mean([p["frame_updated_blocks"] for p in per_frame])
+    new = np.mean([p["frame_new_blocks"] for p in per_frame])
+    vis = np.mean([p["frame_visible_blocks"] for p in per_frame])
+    bytes_integ = upd * 512 * 16 + npx * 15
+    bytes_alloc = npx * 12 + new * 20 + vis * 16
+    n_ray = vis  # blocks the frame can see (upper estimate of blocks rays read)
+    bytes_render = n_ray * 512 * 5 + npx * (4 + 16 + 16 + 16)
+    kern["alloc"]["alg_bytes"] = bytes_alloc
+    kern["integrate"]["alg_bytes"] = bytes_integ
+    kern["render"]["alg_bytes"] = bytes_render
+    dom = max(kern, key=lambda k: kern[k]["ms_per_launch"])
+    peak, peak_kind = measured_peak_hbm()
+    ach = kern[dom]["alg_bytes"] / (kern[dom]["ms_per_launch"] * 1e-3) / 1e9
+    total_bytes = bytes_integ + bytes_alloc + bytes_render
+    fps = args.frames * args.steps * world / (ms * 1e-3)
+    line = {"metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "frames_per_step": args.frames,
+                       "l2": "inputs larger than L2 (30 resident frames, 250 MB per step)",
+                       "parallelism": f"replicas{world}", "mpix_per_s": fps * npx / 1e6},
+            "gpu_launches": launches_per_step * args.steps,
+            "kernels": kern,
+            "frame_bytes": total_bytes, "frame_gbps": total_bytes * fps / world / 1e9,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "traffic": None, "peak_kind": peak_kind},
+            "clocks": clk.summary()}
+    if not args.no_e2e:
+        line["e2e"] = e2e(args, frames, K, sc, rr)
+    if not args.no_cpu and rank == 0:
+        line["cpu_baseline"] = cpu_baseline(frames, K)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sc.close()
+    rr.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def e2e(args, frames, K, sc, rr) -> dict:
+    """Same stream through the C ABI with pinned host inputs: per frame H2D of
+    the point/colour/normal maps, integrate, ray cast, D2H of depth,
+    position and colour -- all inside the timed region."""
+    import torch
+
+    W, H = K.width, K.height
+    host = [(torch.from_numpy(f.pointmap).pin_memory(), torch.from_numpy(f.rgb).pin_memory(),
+             torch.from_numpy(f.normals).pin_memory(), f.pose) for f in frames]
+    dpm = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    drgb = torch.empty((H, W, 3), dtype=torch.uint8, device="cuda")
+    dnm = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    outs = rr.outputs()
+    od = torch.empty((H, W), dtype=torch.float32).pin_memory()
+    op = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    oc = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    import ctypes
+
+    lib = "/usr/local/cuda/lib64/libcudart.so.12"
+    cudart = ctypes.CDLL(lib) if os.path.exists(lib) else None
+
+    def d2h(dst, src_ptr, nbytes):
+        cudart.cudaMemcpyAsync(ctypes.c_void_p(dst.data_ptr()), ctypes.c_void_p(src_ptr), ctypes.c_size_t(nbytes),
+                               2, ctypes.c_void_p(0))
+
+    def step():
+        sc.reset()
+        for pm, rgb, nm, T in host:
+            dpm.copy_(pm, non_blocking=True)
+            drgb.copy_(rgb, non_blocking=True)
+            dnm.copy_(nm, non_blocking=True)
+            sc.integrate(dpm, drgb, dnm, W, H, TRUNC, T, K.fx, K.fy, K.cx, K.cy)
+            rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
+            d2h(od, outs["depth"], W * H * 4)
+            d2h(op, outs["position"], W * H * 16)
+            d2h(oc, outs["color"], W * H * 16)
+        torch.cuda.synchronize()
+
+    if cudart is None:
+        return {"value": None, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "note": "libcudart not found"}
+    steps = max(3, args.steps // 2)
+    for _ in range(2):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    dt = time.perf_counter() - t0
+    nf = len(host)
+    return {"value": nf * steps / dt, "unit": "frames/s",
+            "h2d_bytes_per_step": nf * W * H * (12 + 3 + 12), "d2h_bytes_per_step": nf * W * H * (4 + 16 + 16)}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

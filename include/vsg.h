@@ -1,0 +1,167 @@
+/*
+ * vsg.h -- C ABI of the B200 fusion library (libvsg.so).
+ *
+ * Plain C: opaque handles, POD structs, raw pointers and sizes.  Device
+ * buffers are CUDA device pointers; streams are cudaStream_t passed as
+ * void* (NULL = legacy default stream).  Every entry point returns a status
+ * code (VSG_OK = 0) instead of printing and returning void as the reference
+ * launchers do.
+ *
+ * Each entry point replaces a reference interface (paths within the VoxelSG
+ * project):
+ *   vsg_scene_create / destroy  VoxelScene::VoxelScene / ~VoxelScene,
+ *                               CUDAHashRef::HashDataAllocation
+ *                               (VoxelScene.h:58-63, CUDAHashRef.cu:40-178)
+ *   vsg_scene_reset             VoxelScene::reset, resetHashDataCUDA
+ *                               (VoxelScene.h:68, VoxelScene.cu:1166-1236)
+ *   vsg_integrate               VoxelScene::integrateFromScanData
+ *                               (VoxelScene.h:89-91, VoxelScene.cpp:404-833):
+ *                               allocBlocksFromDepthMapCUDA +
+ *                               compactifyHashCUDA +
+ *                               integrateDepthMapIntoBlocksCUDA
+ *                               (VoxelScene.h:22-40)
+ *   vsg_renderer_create         RayCastRender::initialize (RayCastRender.h:56)
+ *   vsg_render                  RayCastRender::render / rayCastRenderCUDA
+ *                               (RayCastRender.h:66-70, RayCastRender.cpp:28-32)
+ *   vsg_renderer_outputs        RayCastRender::getOutputDepth/Color/Normal/
+ *                               Positions (RayCastRender.h:114-117)
+ *   vsg_renderer_download       RayCastRender::downloadResults /
+ *                               downloadDepthFloat (RayCastRender.h:78-83)
+ *   vsg_scene_stats             VoxelScene::getHeapFreeCount /
+ *                               getNumIntegratedFrames / printStats
+ *                               (VoxelScene.h:104-115, 177)
+ *   vsg_scene_export            VoxelScene::getHashData (VoxelScene.h:129)
+ *                               read back to the host as sorted block records
+ */
+#ifndef VSG_H
+#define VSG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define VSG_API __attribute__((visibility("default")))
+#else
+#define VSG_API
+#endif
+
+typedef void* vsg_stream_t; /* cudaStream_t */
+typedef struct vsg_scene vsg_scene;
+typedef struct vsg_renderer vsg_renderer;
+
+/* status codes */
+enum {
+    VSG_OK = 0,
+    VSG_ERR_INVALID_ARG = 1,   /* null pointer, non-positive size, bad knob */
+    VSG_ERR_NOT_ALLOCATED = 2, /* handle not initialised */
+    VSG_ERR_CUDA = 3,          /* a CUDA runtime call failed */
+    VSG_ERR_OUT_OF_MEMORY = 4, /* device allocation failed */
+    VSG_ERR_TOO_LARGE = 5      /* a size exceeds a documented maximum */
+};
+
+/* sticky device-side condition flags (vsg_stats.flags) */
+enum {
+    VSG_FLAG_HEAP_EXHAUSTED = 1u,   /* voxel pool ran out; blocks were not allocated */
+    VSG_FLAG_CHAIN_EXHAUSTED = 2u,  /* bucket overflow chain pool ran out */
+    VSG_FLAG_COORD_RANGE = 4u,      /* a block coordinate outside +-2^20 was skipped */
+    VSG_FLAG_INSERT_RETRY = 8u,     /* a bounded insert retry loop gave up */
+    VSG_FLAG_MARCH_LIMIT = 16u      /* a ray hit the iteration guard */
+};
+
+/* GlobalParamsConfig knobs (globalPramasConfig.h:101-109) and the sizes
+ * Params derives from them (CUDAHashData.h:14-29). */
+typedef struct vsg_params {
+    float voxel_size;         /* g_SDFVoxelSize (m) */
+    float truncation;         /* g_SDFTruncation (m); frames pass their own */
+    float truncation_scale;   /* g_SDFTruncationScale (not read on the path) */
+    uint32_t hash_num_slots;  /* g_hashNumSlots: number of hash buckets */
+    uint32_t num_sdf_blocks;  /* g_hashNumSDFBlocks: 8^3-voxel blocks in the pool */
+    uint32_t max_chain_nodes; /* bucket-overflow entries; 0 = 2 * hash_num_slots */
+    uint32_t occupancy_log2;  /* occupancy grid is 2^k cells per axis (0 = 8) */
+} vsg_params;
+
+typedef struct vsg_stats {
+    uint32_t allocated_blocks;   /* blocks currently in the hash */
+    uint32_t free_blocks;        /* heap free count (getHeapFreeCount) */
+    uint32_t high_water;         /* highest pool index in use + 1 */
+    uint32_t chain_nodes_used;   /* bucket-overflow entries consumed */
+    uint32_t integrated_frames;  /* getNumIntegratedFrames */
+    uint32_t frame_valid_pixels; /* last frame: pixels with a non-zero point */
+    uint32_t frame_new_blocks;   /* last frame: blocks allocated */
+    uint32_t frame_visible_blocks; /* last frame: blocks passed to integration */
+    uint32_t frame_updated_blocks; /* last frame: blocks with >= 1 voxel updated */
+    uint32_t frame_updated_voxels; /* last frame: voxels updated */
+    uint32_t render_hits;        /* last render: rays that found a surface */
+    uint32_t render_misses;      /* last render: rays that did not */
+    uint32_t flags;              /* VSG_FLAG_* (sticky since reset) */
+} vsg_stats;
+
+/* Reference defaults of the knobs used by the tests (README.md:79-83). */
+VSG_API int vsg_params_default(vsg_params* p);
+
+VSG_API int vsg_scene_create(const vsg_params* p, vsg_scene** out);
+VSG_API int vsg_scene_destroy(vsg_scene* s);
+VSG_API int vsg_scene_reset(vsg_scene* s, vsg_stream_t stream);
+VSG_API int vsg_scene_params(const vsg_scene* s, vsg_params* out);
+
+/* Integrate one frame: allocate the blocks along each pixel's truncation
+ * band, select the blocks the frame can touch, update their voxels.
+ * pointmap: device float3[w*h] camera-space points ((0,0,0) = invalid);
+ * rgb: device uchar3[w*h]; normals: device float3[w*h] (must be non-null,
+ * as in the reference, but is not read); pose: HOST float[16] row-major
+ * camera->world.  Stream-ordered; does not synchronise. */
+VSG_API int vsg_integrate(vsg_scene* s, const float* pointmap, const uint8_t* rgb, const float* normals, int w,
+                  int h, float truncation, const float pose[16], float fx, float fy, float cx, float cy,
+                  vsg_stream_t stream);
+
+/* Counters of the scene and of its last frame / render.  Synchronises. */
+VSG_API int vsg_scene_stats(vsg_scene* s, vsg_stats* out);
+
+/* Read every allocated block back: coords int32[n*3] sorted by (x,y,z) and
+ * 512 voxels each as 8-byte records (float sdf, uint8 r, g, b, weight).
+ * voxels may be NULL.  Fails with VSG_ERR_TOO_LARGE when more than
+ * max_blocks are allocated (n_out still receives the count).  Synchronises. */
+VSG_API int vsg_scene_export(vsg_scene* s, int32_t* coords, uint8_t* voxels, uint32_t max_blocks,
+                     uint32_t* n_out);
+
+VSG_API int vsg_renderer_create(int w, int h, vsg_renderer** out);
+VSG_API int vsg_renderer_destroy(vsg_renderer* r);
+
+/* Ray cast the scene.  pose_dev: DEVICE float[16] row-major camera->world
+ * (the reference passes a caller-owned device matrix); only its rotation is
+ * read, cam_pos (host float[3]) is the ray origin.  When the scene holds no
+ * block the outputs are left untouched, as in the reference. */
+VSG_API int vsg_render(vsg_renderer* r, const vsg_scene* s, const float cam_pos[3], const float* pose_dev,
+               float fx, float fy, float cx, float cy, float min_depth, float max_depth,
+               vsg_stream_t stream);
+/* Same with a HOST pose. */
+VSG_API int vsg_render_hostpose(vsg_renderer* r, const vsg_scene* s, const float cam_pos[3], const float pose[16],
+                        float fx, float fy, float cx, float cy, float min_depth, float max_depth,
+                        vsg_stream_t stream);
+
+/* Device output buffers: depth float[w*h]; position, colour, normal float4
+ * [w*h].  Misses hold 1e10 in every component. */
+VSG_API int vsg_renderer_outputs(const vsg_renderer* r, float** depth, float** position, float** color,
+                         float** normal);
+/* Copy the outputs to host memory (any pointer may be NULL); synchronous. */
+VSG_API int vsg_renderer_download(const vsg_renderer* r, float* depth, float* position, float* color,
+                          float* normal);
+
+/* Per-kernel device time (ms) since the last vsg_timing_reset, measured
+ * with CUDA events on the launching stream when timing is enabled.
+ * Slots: 0 alloc, 1 integrate, 2 render. counts[i] = launches. */
+VSG_API int vsg_timing_enable(vsg_scene* s, int enable);
+VSG_API int vsg_timing_read(vsg_scene* s, double* ms, uint32_t* counts, int n_slots);
+VSG_API int vsg_timing_reset(vsg_scene* s);
+
+/* Library version string. */
+VSG_API const char* vsg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VSG_H */

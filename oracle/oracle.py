@@ -1,0 +1,179 @@
+"""ctypes wrapper of the CPU oracle (vsg_oracle.c) -- TEST INFRASTRUCTURE ONLY.
+
+Imported by the tests, the smoke check and the CPU-baseline leg of the
+benchmark as the checker.  The product path never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_vsg.so")
+
+_f = ctypes.c_float
+_i = ctypes.c_int
+_i64 = ctypes.c_int64
+_p = ctypes.c_void_p
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "vsg_oracle.c")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        cmd = ["gcc", "-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+               "-Wall", "-o", LIB_PATH, src, "-lm"]
+        subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.orc_create.restype = _p
+        L.orc_create.argtypes = [_f]
+        L.orc_destroy.argtypes = [_p]
+        L.orc_reset.argtypes = [_p]
+        L.orc_num_blocks.restype = _i64
+        L.orc_num_blocks.argtypes = [_p]
+        L.orc_coord_range_drops.restype = _i64
+        L.orc_coord_range_drops.argtypes = [_p]
+        L.orc_dda_blocks.restype = _i
+        L.orc_dda_blocks.argtypes = [_p, _p, _f, _p]
+        L.orc_alloc.restype = _i64
+        L.orc_alloc.argtypes = [_p, _p, _i, _i, _f, _p, _p]
+        L.orc_integrate_blocks.argtypes = [_p, _p, _p, _i, _i, _f, _p, _p, _f, _f, _f, _f, _p]
+        L.orc_integrate.argtypes = [_p, _p, _p, _i, _i, _f, _p, _f, _f, _f, _f, _p]
+        L.orc_render.argtypes = [_p, _i, _i, _p, _p, _f, _f, _f, _f, _f, _f, _p, _p, _p, _p, _p]
+        L.orc_render_rows.argtypes = [_p, _i, _i, _i, _i, _p, _p, _f, _f, _f, _f, _f, _f, _p, _p, _p,
+                                      _p, _p]
+        L.orc_render_touched_blocks.restype = _i64
+        L.orc_render_touched_blocks.argtypes = [_p, _i, _i, _p, _p, _f, _f, _f, _f, _f, _f]
+        L.orc_export.argtypes = [_p, _p, _p]
+        L.orc_import.argtypes = [_p, _i64, _p, _p]
+        L.orc_bucket_hash.restype = ctypes.c_uint32
+        L.orc_bucket_hash.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]
+        L.orc_max_threads.restype = _i
+        L.orc_set_threads.argtypes = [_i]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_p)
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class OracleScene:
+    """CPU TSDF scene with reference semantics (ideal allocation)."""
+
+    def __init__(self, voxel_size: float):
+        self.L = lib()
+        self.h = self.L.orc_create(_f(voxel_size))
+        self.voxel = voxel_size
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.orc_destroy(self.h)
+            self.h = None
+
+    def reset(self):
+        self.L.orc_reset(self.h)
+
+    @property
+    def num_blocks(self) -> int:
+        return int(self.L.orc_num_blocks(self.h))
+
+    def integrate(self, pointmap, rgb, trunc, pose, fx, fy, cx, cy) -> dict:
+        pm = _f32(pointmap)
+        cm = np.ascontiguousarray(rgb, dtype=np.uint8)
+        T = _f32(pose).reshape(16)
+        H, W = pm.shape[:2]
+        out = np.zeros(4, np.int64)
+        self.L.orc_integrate(self.h, _ptr(pm), _ptr(cm), W, H, _f(trunc), _ptr(T), _f(fx), _f(fy),
+                             _f(cx), _f(cy), _ptr(out))
+        return {"new_blocks": int(out[0]), "updated_blocks": int(out[1]), "updated_voxels": int(out[2]),
+                "blocks": int(out[3])}
+
+    def alloc(self, pointmap, trunc, pose) -> int:
+        pm = _f32(pointmap)
+        T = _f32(pose).reshape(16)
+        cam = np.array([T[3], T[7], T[11]], np.float32)
+        H, W = pm.shape[:2]
+        return int(self.L.orc_alloc(self.h, _ptr(pm), W, H, _f(trunc), _ptr(T), _ptr(cam)))
+
+    def render(self, W, H, pose, fx, fy, cx, cy, min_depth, max_depth, cam=None, rows=None) -> dict:
+        T = _f32(pose).reshape(16)
+        cam = np.array([T[3], T[7], T[11]], np.float32) if cam is None else _f32(cam)
+        depth = np.full((H, W), 1e10, np.float32)
+        pos = np.full((H, W, 4), 1e10, np.float32)
+        col = np.full((H, W, 4), 1e10, np.float32)
+        nrm = np.full((H, W, 4), 1e10, np.float32)
+        st = np.zeros(3, np.int64)
+        if rows is None:
+            self.L.orc_render(self.h, W, H, _ptr(cam), _ptr(T), _f(fx), _f(fy), _f(cx), _f(cy),
+                              _f(min_depth), _f(max_depth), _ptr(depth), _ptr(pos), _ptr(col), _ptr(nrm),
+                              _ptr(st))
+        else:
+            self.L.orc_render_rows(self.h, W, H, rows[0], rows[1], _ptr(cam), _ptr(T), _f(fx), _f(fy),
+                                   _f(cx), _f(cy), _f(min_depth), _f(max_depth), _ptr(depth), _ptr(pos),
+                                   _ptr(col), _ptr(nrm), _ptr(st))
+        return {"depth": depth, "position": pos, "color": col, "normal": nrm, "hits": int(st[0]),
+                "misses": int(st[1]), "samples": int(st[2])}
+
+    def touched_blocks(self, W, H, pose, fx, fy, cx, cy, min_depth, max_depth) -> int:
+        T = _f32(pose).reshape(16)
+        cam = np.array([T[3], T[7], T[11]], np.float32)
+        return int(self.L.orc_render_touched_blocks(self.h, W, H, _ptr(cam), _ptr(T), _f(fx), _f(fy),
+                                                    _f(cx), _f(cy), _f(min_depth), _f(max_depth)))
+
+    def export(self, with_voxels: bool = True):
+        """(coords (n,3) int32 sorted by x,y,z; voxels (n,512) structured)."""
+        n = self.num_blocks
+        coords = np.zeros((n, 3), np.int32)
+        vox = np.zeros((n, 512 * 8), np.uint8) if with_voxels else None
+        self.L.orc_export(self.h, _ptr(coords), _ptr(vox) if with_voxels else None)
+        return coords, (split_voxels(vox) if with_voxels else None)
+
+    def load(self, coords, voxel_bytes):
+        coords = np.ascontiguousarray(coords, dtype=np.int32)
+        vb = np.ascontiguousarray(voxel_bytes, dtype=np.uint8)
+        self.L.orc_import(self.h, coords.shape[0], _ptr(coords), _ptr(vb))
+
+
+def split_voxels(vox_bytes: np.ndarray) -> dict:
+    """(n, 4096) raw bytes -> dict of sdf (n,512) f32, rgb (n,512,3) u8, weight (n,512) u8."""
+    v = vox_bytes.reshape(-1, 512, 8)
+    sdf = np.ascontiguousarray(v[:, :, :4]).view(np.float32).reshape(-1, 512)
+    return {"sdf": sdf, "rgb": v[:, :, 4:7].copy(), "weight": v[:, :, 7].copy(), "raw": vox_bytes}
+
+
+def dda_blocks(start, end, voxel) -> np.ndarray:
+    s = _f32(start)
+    e = _f32(end)
+    out = np.zeros((1024, 3), np.int32)
+    n = lib().orc_dda_blocks(_ptr(s), _ptr(e), _f(voxel), _ptr(out))
+    return out[:n].copy()
+
+
+def bucket_hash(x, y, z, num_buckets) -> int:
+    return int(lib().orc_bucket_hash(int(x), int(y), int(z), int(num_buckets)))
+
+
+def set_threads(n: int):
+    lib().orc_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().orc_max_threads())

@@ -1,0 +1,694 @@
+/*
+ * vsg_oracle.c -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement of the VoxelSG fusion hot path (block allocation, TSDF
+ * integration, ray casting, marching cubes).  It is the parity checker for
+ * the CUDA library: only the tests, the smoke check and the CPU-baseline leg
+ * of the benchmark load it.  Nothing in the product links or calls it.
+ *
+ * Every function restates the reference kernel named in its comment
+ * (file:line within the VoxelSG project).  Floating point follows the
+ * reference operation by operation in IEEE binary32 with no contraction
+ * (build with -ffp-contract=off, no fast-math), so integer decisions (pixel
+ * rounding, DDA steps, truncation rejects, marching-cubes signs) are
+ * reproducible bit for bit.  Float->int conversions emulate the CUDA
+ * saturating round-toward-zero conversion (NaN -> 0), which the reference
+ * relies on implicitly for pixels that project from behind the camera.
+ *
+ * Documented semantic choices (the reference behaviour they replace is a
+ * scheduling race, not a specification):
+ *  - "ideal" allocation: every block the per-pixel DDA visits is allocated.
+ *    The reference takes a per-bucket lock at most once per frame and never
+ *    releases it (VoxelScene.cu:176-203), so a second new block hashing to
+ *    the same bucket in the same frame is dropped at random.
+ *  - integration visits every allocated block (VoxelScene.cu:1275-1300 puts
+ *    all of them in the compact list); voxels that do not project into a
+ *    valid pixel inside the truncation band are left untouched.
+ *  - the write-only voxel flags isUpdated / isZeroCrossing are not kept:
+ *    nothing on the path reads them.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define BS 8
+#define VPB 512
+#define KEY_EMPTY 0xFFFFFFFFFFFFFFFFull
+#define COORD_LIM (1 << 20)
+
+typedef struct {
+    float sdf;
+    uint8_t r, g, b, w;
+} ovox; /* canonical 8-byte voxel: sdf, colour, weight */
+
+typedef struct {
+    float voxel;
+    /* open-addressing map: packed block key -> block index */
+    uint64_t* mkeys;
+    int32_t* mvals;
+    int64_t mcap;
+    /* dense block storage */
+    int64_t n, cap;
+    uint64_t* keys;
+    ovox* vox;
+    int64_t coord_range_drops;
+} orc_scene;
+
+/* ---------------------------------------------------------------- helpers */
+
+/* CUDA cvt.rzi.s32.f32: truncation toward zero, saturating, NaN -> 0. */
+static inline int32_t f2i(float x) {
+    if (x != x) return 0;
+    if (x >= 2147483648.0f) return INT32_MAX;
+    if (x <= -2147483648.0f) return INT32_MIN;
+    return (int32_t)x;
+}
+
+static inline int32_t wrap_sub7(int32_t a) { return (int32_t)((uint32_t)a - 7u); }
+
+static inline uint64_t pack_key(int32_t x, int32_t y, int32_t z) {
+    const uint64_t m = 0x1FFFFFull;
+    return (((uint64_t)(uint32_t)x & m) << 42) | (((uint64_t)(uint32_t)y & m) << 21) |
+           ((uint64_t)(uint32_t)z & m);
+}
+
+static inline int32_t sext21(uint64_t v) {
+    v &= 0x1FFFFFull;
+    return (int32_t)(v & 0x100000ull ? (v | 0xFFFFFFFFFFE00000ull) : v);
+}
+
+static inline void unpack_key(uint64_t k, int32_t* b) {
+    b[0] = sext21(k >> 42);
+    b[1] = sext21(k >> 21);
+    b[2] = sext21(k);
+}
+
+static inline int in_range(const int32_t* b) {
+    return b[0] >= -COORD_LIM && b[0] < COORD_LIM && b[1] >= -COORD_LIM && b[1] < COORD_LIM &&
+           b[2] >= -COORD_LIM && b[2] < COORD_LIM;
+}
+
+static inline uint64_t mix64(uint64_t k) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return k;
+}
+
+/* Bucket hash of the reference, VoxelScene.cu:61-66 (32-bit wrapping). */
+uint32_t orc_bucket_hash(int32_t x, int32_t y, int32_t z, uint32_t num_buckets) {
+    uint32_t h = ((uint32_t)x * 73856093u) ^ ((uint32_t)y * 19349663u) ^ ((uint32_t)z * 83492791u);
+    return h % num_buckets;
+}
+
+/* ---------------------------------------------------------------- CPU map */
+
+static int64_t map_find(const orc_scene* s, uint64_t key) {
+    if (s->mcap == 0) return -1;
+    uint64_t m = (uint64_t)s->mcap - 1;
+    uint64_t i = mix64(key) & m;
+    for (;;) {
+        uint64_t k = s->mkeys[i];
+        if (k == key) return s->mvals[i];
+        if (k == KEY_EMPTY) return -1;
+        i = (i + 1) & m;
+    }
+}
+
+static void map_put_raw(uint64_t* mk, int32_t* mv, int64_t cap, uint64_t key, int32_t val) {
+    uint64_t m = (uint64_t)cap - 1;
+    uint64_t i = mix64(key) & m;
+    while (mk[i] != KEY_EMPTY) i = (i + 1) & m;
+    mk[i] = key;
+    mv[i] = val;
+}
+
+static void map_grow(orc_scene* s, int64_t need) {
+    if (s->mcap >= 2 * need && s->mcap > 0) return;
+    int64_t cap = s->mcap ? s->mcap : 1024;
+    while (cap < 2 * need) cap *= 2;
+    uint64_t* mk = (uint64_t*)malloc(sizeof(uint64_t) * cap);
+    int32_t* mv = (int32_t*)malloc(sizeof(int32_t) * cap);
+    for (int64_t i = 0; i < cap; i++) mk[i] = KEY_EMPTY;
+    for (int64_t i = 0; i < s->n; i++) map_put_raw(mk, mv, cap, s->keys[i], (int32_t)i);
+    free(s->mkeys);
+    free(s->mvals);
+    s->mkeys = mk;
+    s->mvals = mv;
+    s->mcap = cap;
+}
+
+/* insert a block (zero voxels) if absent; returns 1 when new */
+static int scene_add(orc_scene* s, uint64_t key) {
+    if (map_find(s, key) >= 0) return 0;
+    if (s->n + 1 > s->cap) {
+        int64_t nc = s->cap ? s->cap * 2 : 1024;
+        s->keys = (uint64_t*)realloc(s->keys, sizeof(uint64_t) * nc);
+        s->vox = (ovox*)realloc(s->vox, sizeof(ovox) * VPB * nc);
+        s->cap = nc;
+    }
+    map_grow(s, s->n + 1);
+    s->keys[s->n] = key;
+    memset(s->vox + s->n * VPB, 0, sizeof(ovox) * VPB);
+    map_put_raw(s->mkeys, s->mvals, s->mcap, key, (int32_t)s->n);
+    s->n++;
+    return 1;
+}
+
+orc_scene* orc_create(float voxel) {
+    orc_scene* s = (orc_scene*)calloc(1, sizeof(orc_scene));
+    s->voxel = voxel;
+    return s;
+}
+
+void orc_reset(orc_scene* s) {
+    s->n = 0;
+    if (s->mkeys)
+        for (int64_t i = 0; i < s->mcap; i++) s->mkeys[i] = KEY_EMPTY;
+    s->coord_range_drops = 0;
+}
+
+void orc_destroy(orc_scene* s) {
+    if (!s) return;
+    free(s->mkeys);
+    free(s->mvals);
+    free(s->keys);
+    free(s->vox);
+    free(s);
+}
+
+int64_t orc_num_blocks(const orc_scene* s) { return s->n; }
+int64_t orc_coord_range_drops(const orc_scene* s) { return s->coord_range_drops; }
+
+/* ------------------------------------------------------- allocation (DDA) */
+
+/* worldToSDFBlock, VoxelScene.cu:74-96: voxel = int(p/v + 0.5*sign)
+ * (truncation toward zero), negative voxels shifted by -7, then C division. */
+static inline void world_to_block_alloc(const float* p, float v, int32_t* b) {
+    for (int a = 0; a < 3; a++) {
+        float q = p[a] / v;
+        float sg = (q > 0) ? 1.0f : ((q < 0) ? -1.0f : 0.0f);
+        int32_t iv = f2i(q + sg * 0.5f);
+        if (iv < 0) iv = wrap_sub7(iv);
+        b[a] = iv / BS;
+    }
+}
+
+/* row-major camera->world transform of a camera-space point,
+ * VoxelScene.cu:561-565 (same operation order everywhere in the reference) */
+static inline void xform_point(const float* T, const float* p, float* o) {
+    o[0] = T[0] * p[0] + T[1] * p[1] + T[2] * p[2] + T[3];
+    o[1] = T[4] * p[0] + T[5] * p[1] + T[6] * p[2] + T[7];
+    o[2] = T[8] * p[0] + T[9] * p[1] + T[10] * p[2] + T[11];
+}
+
+/* allocateBlocksAlongRay, VoxelScene.cu:295-481.  Writes the visited block
+ * coordinates to out (up to 1024 triples); returns how many. */
+int orc_dda_blocks(const float* s, const float* e, float v, int32_t* out) {
+    int32_t cur[3], end[3];
+    world_to_block_alloc(s, v, cur);
+    world_to_block_alloc(e, v, end);
+    if (cur[0] == end[0] && cur[1] == end[1] && cur[2] == end[2]) return 0; /* :345-348 */
+    float d[3] = {e[0] - s[0], e[1] - s[1], e[2] - s[2]};
+    float len = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    if (len < 1e-6f) return 0;
+    d[0] /= len;
+    d[1] /= len;
+    d[2] /= len;
+    float step[3], tmax[3], tdel[3];
+    const float ext = (float)BS * v;
+    for (int a = 0; a < 3; a++) {
+        step[a] = (d[a] > 0) ? 1.0f : -1.0f;
+        float sc = (step[a] > 0) ? 1.0f : 0.0f;
+        float bnd = ((float)cur[a] + sc) * ext - 0.5f * v; /* :373-377 */
+        tmax[a] = (bnd - s[a]) / d[a];
+        tdel[a] = (step[a] * ext) / d[a];
+    }
+    for (int a = 0; a < 3; a++)
+        if (d[a] == 0.0f) {
+            tmax[a] = 1e6f;
+            tdel[a] = 1e6f;
+        }
+    int n = 0;
+    for (int it = 0; it < 1024; it++) { /* :417 */
+        out[3 * n + 0] = cur[0];
+        out[3 * n + 1] = cur[1];
+        out[3 * n + 2] = cur[2];
+        n++;
+        if (cur[0] == end[0] && cur[1] == end[1] && cur[2] == end[2]) break;
+        if (tmax[0] < tmax[1] && tmax[0] < tmax[2]) { /* :464-475 */
+            tmax[0] += tdel[0];
+            cur[0] += (int32_t)step[0];
+        } else if (tmax[1] < tmax[2]) {
+            tmax[1] += tdel[1];
+            cur[1] += (int32_t)step[1];
+        } else {
+            tmax[2] += tdel[2];
+            cur[2] += (int32_t)step[2];
+        }
+    }
+    return n;
+}
+
+/* allocBlocksFromDepthMapMethod1Kernel, VoxelScene.cu:487-633, per pixel.
+ * Returns the number of blocks written to out. */
+static int pixel_alloc_blocks(const float* p, float trunc, const float* T, const float* cam, float v,
+                              int32_t* out) {
+    if (p[2] <= 1e-6f) return 0; /* :548 (NaN passes, as on the GPU) */
+    float w[3];
+    xform_point(T, p, w);
+    float rd[3] = {w[0] - cam[0], w[1] - cam[1], w[2] - cam[2]};
+    float rl = sqrtf(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2]);
+    if (rl < 1e-6f) return 0;
+    float cmin[3] = {p[0], p[1], p[2] - trunc};
+    float cmax[3] = {p[0], p[1], p[2] + trunc};
+    float rmin[3], rmax[3];
+    xform_point(T, cmin, rmin);
+    xform_point(T, cmax, rmax);
+    return orc_dda_blocks(rmin, rmax, v, out);
+}
+
+/* Allocate every block the per-pixel DDA visits ("ideal" allocation).
+ * Returns the number of newly allocated blocks. */
+int64_t orc_alloc(orc_scene* s, const float* pm, int W, int H, float trunc, const float* T,
+                  const float* cam) {
+    int64_t npx = (int64_t)W * H;
+    int nthr = 1;
+#ifdef _OPENMP
+    nthr = omp_get_max_threads();
+#endif
+    uint64_t** lists = (uint64_t**)calloc(nthr, sizeof(uint64_t*));
+    int64_t* lens = (int64_t*)calloc(nthr, sizeof(int64_t));
+    int64_t* caps = (int64_t*)calloc(nthr, sizeof(int64_t));
+    int64_t drops = 0;
+#pragma omp parallel reduction(+ : drops)
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        int32_t* buf = (int32_t*)malloc(sizeof(int32_t) * 3 * 1024);
+        uint64_t last = KEY_EMPTY;
+#pragma omp for schedule(dynamic, 4096)
+        for (int64_t i = 0; i < npx; i++) {
+            int n = pixel_alloc_blocks(pm + 3 * i, trunc, T, cam, s->voxel, buf);
+            for (int j = 0; j < n; j++) {
+                if (!in_range(buf + 3 * j)) {
+                    drops++;
+                    continue;
+                }
+                uint64_t k = pack_key(buf[3 * j], buf[3 * j + 1], buf[3 * j + 2]);
+                if (k == last) continue;
+                last = k;
+                if (lens[tid] == caps[tid]) {
+                    caps[tid] = caps[tid] ? caps[tid] * 2 : 4096;
+                    lists[tid] = (uint64_t*)realloc(lists[tid], sizeof(uint64_t) * caps[tid]);
+                }
+                lists[tid][lens[tid]++] = k;
+            }
+        }
+        free(buf);
+    }
+    int64_t added = 0;
+    for (int t = 0; t < nthr; t++) {
+        for (int64_t j = 0; j < lens[t]; j++) added += scene_add(s, lists[t][j]);
+        free(lists[t]);
+    }
+    free(lists);
+    free(lens);
+    free(caps);
+    s->coord_range_drops += drops;
+    return added;
+}
+
+/* ---------------------------------------------------------- integration */
+
+/* integrateDepthMapIntoBlocksKernel, VoxelScene.cu:918-1146, for one voxel.
+ * Returns 1 when the voxel was updated. */
+static inline int integrate_voxel(ovox* vx, int bx, int by, int bz, int idx, const float* pm,
+                                  const uint8_t* rgb, int W, int H, float trunc, const float* T,
+                                  const float* cam, float v, float fx, float fy, float cx, float cy) {
+    int lx = idx % BS, ly = (idx / BS) % BS, lz = idx / (BS * BS);
+    /* (blockCoord*8 + local) * voxelSize, :959-963 (int arithmetic wraps) */
+    float wx = (float)(int32_t)((uint32_t)bx * 8u + (uint32_t)lx) * v;
+    float wy = (float)(int32_t)((uint32_t)by * 8u + (uint32_t)ly) * v;
+    float wz = (float)(int32_t)((uint32_t)bz * 8u + (uint32_t)lz) * v;
+    float rx = wx - T[3], ry = wy - T[7], rz = wz - T[11]; /* :970-974 */
+    float px = T[0] * rx + T[4] * ry + T[8] * rz;          /* :976-980 */
+    float py = T[1] * rx + T[5] * ry + T[9] * rz;
+    float pz = T[2] * rx + T[6] * ry + T[10] * rz;
+    float sx = px * fx / pz + cx; /* :984-987 */
+    float sy = py * fy / pz + cy;
+    int ix = f2i(sx + 0.5f), iy = f2i(sy + 0.5f); /* :990-993 */
+    if (!(ix >= 0 && ix < W && iy >= 0 && iy < H)) return 0;
+    int64_t pi = (int64_t)iy * W + ix;
+    const float* P = pm + 3 * pi;
+    if (!(P[0] != 0.0f || P[1] != 0.0f || P[2] != 0.0f)) return 0; /* :1040-1046 */
+    float Pw[3];
+    xform_point(T, P, Pw); /* :1052-1056 */
+    float dx = wx - Pw[0], dy = wy - Pw[1], dz = wz - Pw[2];
+    float sdf = sqrtf(dx * dx + dy * dy + dz * dz);
+    float ex = Pw[0] - cam[0], ey = Pw[1] - cam[1], ez = Pw[2] - cam[2];
+    float cdist = sqrtf(ex * ex + ey * ey + ez * ez);
+    float vdist = sqrtf((wx - cam[0]) * (wx - cam[0]) + (wy - cam[1]) * (wy - cam[1]) +
+                        (wz - cam[2]) * (wz - cam[2]));
+    if (vdist < cdist) sdf = -sdf; /* :1064-1066 */
+    if (sdf < -trunc || sdf > trunc) return 0;
+    sdf = fmaxf(-trunc, fminf(trunc, sdf));
+    const uint8_t* c = rgb + 3 * pi;
+    /* running average with weight increment 1, :1096-1126 */
+    float oldS = vx->sdf;
+    float oldW = (float)vx->w;
+    float newW = oldW + 1.0f;
+    if (newW > 0.0f) {
+        vx->sdf = (oldS * oldW + sdf * 1.0f) / newW;
+        vx->w = (uint8_t)fminf(255.0f, newW);
+        float ncr = ((float)vx->r * oldW + (float)c[0] * 1.0f) / newW;
+        float ncg = ((float)vx->g * oldW + (float)c[1] * 1.0f) / newW;
+        float ncb = ((float)vx->b * oldW + (float)c[2] * 1.0f) / newW;
+        vx->r = (uint8_t)ncr;
+        vx->g = (uint8_t)ncg;
+        vx->b = (uint8_t)ncb;
+    }
+    return 1;
+}
+
+/* Integrate one frame into every allocated block.  out[0] = blocks with at
+ * least one updated voxel, out[1] = updated voxels. */
+void orc_integrate_blocks(orc_scene* s, const float* pm, const uint8_t* rgb, int W, int H, float trunc,
+                          const float* T, const float* cam, float fx, float fy, float cx, float cy,
+                          int64_t* out) {
+    int64_t nupd = 0, nvox = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : nupd, nvox)
+    for (int64_t b = 0; b < s->n; b++) {
+        int32_t bc[3];
+        unpack_key(s->keys[b], bc);
+        ovox* blk = s->vox + b * VPB;
+        int cnt = 0;
+        for (int i = 0; i < VPB; i++)
+            cnt += integrate_voxel(blk + i, bc[0], bc[1], bc[2], i, pm, rgb, W, H, trunc, T, cam, s->voxel,
+                                   fx, fy, cx, cy);
+        nvox += cnt;
+        nupd += cnt > 0;
+    }
+    out[0] = nupd;
+    out[1] = nvox;
+}
+
+/* VoxelScene::integrateFromScanData, VoxelScene.cpp:404-833: camera position
+ * is the translation column of the row-major camera->world matrix
+ * (:462-466); allocation, then integration.  out[0]=new blocks,
+ * out[1]=updated blocks, out[2]=updated voxels, out[3]=total blocks. */
+void orc_integrate(orc_scene* s, const float* pm, const uint8_t* rgb, int W, int H, float trunc,
+                   const float* T, float fx, float fy, float cx, float cy, int64_t* out) {
+    float cam[3] = {T[3], T[7], T[11]};
+    out[0] = orc_alloc(s, pm, W, H, trunc, T, cam);
+    int64_t r[2];
+    orc_integrate_blocks(s, pm, rgb, W, H, trunc, T, cam, fx, fy, cx, cy, r);
+    out[1] = r[0];
+    out[2] = r[1];
+    out[3] = s->n;
+}
+
+/* ------------------------------------------------------------- ray casting */
+
+/* worldToVirtualVoxelPos / virtualVoxelPosToSDFBlock / virtualVoxelPosToLocal,
+ * RayCastRender.cu:17-42 (floorf variant, unlike allocation). */
+static inline const ovox* get_voxel(const orc_scene* s, const float* p, uint8_t* mark) {
+    int32_t vp[3], b[3], l[3];
+    for (int a = 0; a < 3; a++) {
+        float q = p[a] / s->voxel;
+        float sg = (q > 0) ? 1.0f : ((q < 0) ? -1.0f : 0.0f);
+        vp[a] = f2i(floorf(q + 0.5f * sg));
+        int32_t t = vp[a];
+        if (t < 0) t = wrap_sub7(t);
+        b[a] = t / BS;
+        l[a] = ((vp[a] % BS) + BS) % BS;
+    }
+    if (!in_range(b)) return NULL;
+    int64_t bi = map_find(s, pack_key(b[0], b[1], b[2]));
+    if (bi < 0) return NULL;
+    if (mark) mark[bi] = 1;
+    return s->vox + bi * VPB + (l[0] + l[1] * BS + l[2] * BS * BS);
+}
+
+static inline float frac01(float v) { return v - floorf(v); }
+
+/* trilinearInterpolationSimpleFastFast, RayCastRender.cu:127-215 */
+static int trilinear(const orc_scene* s, const float* pos, float* dist, uint8_t* color, uint8_t* mark) {
+    const float off = s->voxel;
+    float pd[3] = {pos[0] - off / 2.0f, pos[1] - off / 2.0f, pos[2] - off / 2.0f};
+    float vf[3] = {pd[0] / s->voxel, pd[1] / s->voxel, pd[2] / s->voxel};
+    float wt[3] = {frac01(vf[0]), frac01(vf[1]), frac01(vf[2])};
+    float d = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f, vws = 0.0f;
+    for (int i = 0; i < 8; i++) {
+        float q[3] = {pd[0] + ((i & 1) ? off : 0.0f), pd[1] + ((i & 2) ? off : 0.0f),
+                      pd[2] + ((i & 4) ? off : 0.0f)};
+        const ovox* vx = get_voxel(s, q, mark);
+        if (!vx || vx->w == 0) continue;
+        float w = ((i & 1) ? wt[0] : (1.0f - wt[0])) * ((i & 2) ? wt[1] : (1.0f - wt[1])) *
+                  ((i & 4) ? wt[2] : (1.0f - wt[2]));
+        d += w * vx->sdf;
+        cr += w * (float)vx->r;
+        cg += w * (float)vx->g;
+        cb += w * (float)vx->b;
+        vws += w;
+    }
+    if (vws <= 1e-6f) return 0;
+    float inv = 1.0f / vws;
+    d *= inv;
+    cr *= inv;
+    cg *= inv;
+    cb *= inv;
+    *dist = d;
+    if (color) {
+        color[0] = (uint8_t)cr;
+        color[1] = (uint8_t)cg;
+        color[2] = (uint8_t)cb;
+    }
+    return 1;
+}
+
+/* findIntersectionBisection, RayCastRender.cu:229-271 (3 regula-falsi steps) */
+static int bisection(const orc_scene* s, const float* o, const float* dir, float d0, float r0, float d1,
+                     float r1, float* alpha, uint8_t* color, uint8_t* mark) {
+    float a = r0, ad = d0, b = r1, bd = d1, c = 0.0f;
+    for (int i = 0; i < 3; i++) {
+        c = a + (ad / (ad - bd)) * (b - a);
+        float cd;
+        float sp[3] = {o[0] + c * dir[0], o[1] + c * dir[1], o[2] + c * dir[2]};
+        if (!trilinear(s, sp, &cd, color, mark)) return 0;
+        if (ad * cd > 0.0f) {
+            a = c;
+            ad = cd;
+        } else {
+            b = c;
+            bd = cd;
+        }
+    }
+    *alpha = c;
+    return 1;
+}
+
+#define MINF 1e10f
+
+/* renderKernel + traverseCoarseGridSimpleSampleAll, RayCastRender.cu:407-517,
+ * 276-398.  One pixel.  Returns 1 on a hit. steps_out counts samples. */
+static int render_pixel(const orc_scene* s, int x, int y, const float* cam, const float* T, float fx,
+                        float fy, float cx, float cy, float minD, float maxD, float* depth, float* pos4,
+                        float* col4, float* nrm4, int64_t* steps_out, uint8_t* mark) {
+    *depth = MINF;
+    for (int k = 0; k < 4; k++) pos4[k] = col4[k] = nrm4[k] = MINF;
+    float cd[3] = {((float)x - cx) / fx, ((float)y - cy) / fy, 1.0f};
+    float cl = sqrtf(cd[0] * cd[0] + cd[1] * cd[1] + cd[2] * cd[2]);
+    if (cl > 1e-6f) {
+        cd[0] /= cl;
+        cd[1] /= cl;
+        cd[2] /= cl;
+    }
+    float wd[3] = {T[0] * cd[0] + T[1] * cd[1] + T[2] * cd[2], T[4] * cd[0] + T[5] * cd[1] + T[6] * cd[2],
+                   T[8] * cd[0] + T[9] * cd[1] + T[10] * cd[2]};
+    float wl = sqrtf(wd[0] * wd[0] + wd[1] * wd[1] + wd[2] * wd[2]);
+    if (wl > 1e-6f) {
+        wd[0] /= wl;
+        wd[1] /= wl;
+        wd[2] /= wl;
+    }
+    if (minD == 0 || minD == MINF) return 0;
+    if (maxD == 0 || maxD == MINF) return 0;
+    float lastSdf = 0.0f, lastAlpha = 0.0f;
+    unsigned lastW = 0;
+    const float d2r = 1.0f / cd[2];
+    float rc = d2r * fmaxf(minD, minD);
+    float re = d2r * fminf(maxD, maxD);
+    int64_t steps = 0;
+    while (rc < re) {
+        float p[3] = {cam[0] + rc * wd[0], cam[1] + rc * wd[1], cam[2] + rc * wd[2]};
+        float dist;
+        steps++;
+        if (trilinear(s, p, &dist, NULL, mark)) {
+            if (lastW > 0 && lastSdf < 0.0f && dist > 0.0f) {
+                float alpha = 0.0f;
+                uint8_t c2[3] = {0, 0, 0};
+                int b = bisection(s, cam, wd, lastSdf, lastAlpha, dist, rc, &alpha, c2, mark);
+                float iso[3] = {cam[0] + alpha * wd[0], cam[1] + alpha * wd[1], cam[2] + alpha * wd[2]};
+                float th = s->voxel * 3;
+                if (b && fabsf(lastSdf - dist) < th) {
+                    if (fabsf(dist) < th) {
+                        *depth = alpha / d2r;
+                        pos4[0] = iso[0];
+                        pos4[1] = iso[1];
+                        pos4[2] = iso[2];
+                        pos4[3] = 1.0f;
+                        col4[0] = (float)c2[0] / 255.0f;
+                        col4[1] = (float)c2[1] / 255.0f;
+                        col4[2] = (float)c2[2] / 255.0f;
+                        col4[3] = 1.0f;
+                        *steps_out += steps;
+                        return 1;
+                    }
+                }
+            }
+            lastSdf = dist;
+            lastAlpha = rc;
+            lastW = 1;
+            rc += s->voxel * 0.5f;
+        } else {
+            lastW = 0;
+            rc += s->voxel * 0.5f;
+        }
+    }
+    *steps_out += steps;
+    return 0;
+}
+
+/* RayCastRender::render, RayCastRender.cpp:123-183 / rayCastRenderCUDA,
+ * RayCastRender.cu:526-620.  T is the row-major camera->world matrix; only
+ * its rotation is used, the ray origin is cam.  With no allocated block the
+ * reference returns before launching (:552-555) and leaves the outputs
+ * untouched; so does this.  stats[0]=hits, [1]=misses, [2]=samples. */
+void orc_render(const orc_scene* s, int W, int H, const float* cam, const float* T, float fx, float fy,
+                float cx, float cy, float minD, float maxD, float* depth, float* pos4, float* col4,
+                float* nrm4, int64_t* stats) {
+    stats[0] = stats[1] = stats[2] = 0;
+    if (s->n == 0) return;
+    int64_t hits = 0, miss = 0, steps = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : hits, miss, steps)
+    for (int64_t i = 0; i < (int64_t)W * H; i++) {
+        int x = (int)(i % W), y = (int)(i / W);
+        int h = render_pixel(s, x, y, cam, T, fx, fy, cx, cy, minD, maxD, depth + i, pos4 + 4 * i,
+                             col4 + 4 * i, nrm4 + 4 * i, &steps, NULL);
+        hits += h;
+        miss += !h;
+    }
+    stats[0] = hits;
+    stats[1] = miss;
+    stats[2] = steps;
+}
+
+/* Render a sub-rectangle of rows [y0, y1) only (bounded CPU-baseline
+ * samples); outputs are full-frame sized. */
+void orc_render_rows(const orc_scene* s, int W, int H, int y0, int y1, const float* cam, const float* T,
+                     float fx, float fy, float cx, float cy, float minD, float maxD, float* depth,
+                     float* pos4, float* col4, float* nrm4, int64_t* stats) {
+    stats[0] = stats[1] = stats[2] = 0;
+    if (s->n == 0) return;
+    if (y0 < 0) y0 = 0;
+    if (y1 > H) y1 = H;
+    int64_t hits = 0, miss = 0, steps = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : hits, miss, steps)
+    for (int64_t i = (int64_t)y0 * W; i < (int64_t)y1 * W; i++) {
+        int x = (int)(i % W), y = (int)(i / W);
+        int h = render_pixel(s, x, y, cam, T, fx, fy, cx, cy, minD, maxD, depth + i, pos4 + 4 * i,
+                             col4 + 4 * i, nrm4 + 4 * i, &steps, NULL);
+        hits += h;
+        miss += !h;
+    }
+    stats[0] = hits;
+    stats[1] = miss;
+    stats[2] = steps;
+}
+
+/* Distinct blocks the reference ray march reads (any tap that resolves to an
+ * allocated block), over the whole image.  Used for the algorithmic-byte
+ * count of the ray caster; not part of the reference. */
+int64_t orc_render_touched_blocks(const orc_scene* s, int W, int H, const float* cam, const float* T,
+                                  float fx, float fy, float cx, float cy, float minD, float maxD) {
+    if (s->n == 0) return 0;
+    uint8_t* mark = (uint8_t*)calloc(s->n, 1);
+    int64_t steps = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : steps)
+    for (int64_t i = 0; i < (int64_t)W * H; i++) {
+        float d, p4[4], c4[4], n4[4];
+        render_pixel(s, (int)(i % W), (int)(i / W), cam, T, fx, fy, cx, cy, minD, maxD, &d, p4, c4, n4,
+                     &steps, mark);
+    }
+    int64_t n = 0;
+    for (int64_t b = 0; b < s->n; b++) n += mark[b];
+    free(mark);
+    return n;
+}
+
+/* ------------------------------------------------------- export / import */
+
+static int cmp_key3(const void* a, const void* b) {
+    const int32_t* x = (const int32_t*)a;
+    const int32_t* y = (const int32_t*)b;
+    for (int i = 0; i < 3; i++) {
+        if (x[i] < y[i]) return -1;
+        if (x[i] > y[i]) return 1;
+    }
+    return 0;
+}
+
+typedef struct {
+    int32_t c[3];
+    int32_t idx;
+} keyidx;
+
+/* Sorted (x, y, z) block coordinates and their 512 voxels each (8 bytes per
+ * voxel: sdf f32, r, g, b, weight). */
+void orc_export(const orc_scene* s, int32_t* coords, uint8_t* voxels) {
+    keyidx* t = (keyidx*)malloc(sizeof(keyidx) * (s->n ? s->n : 1));
+    for (int64_t i = 0; i < s->n; i++) {
+        unpack_key(s->keys[i], t[i].c);
+        t[i].idx = (int32_t)i;
+    }
+    qsort(t, s->n, sizeof(keyidx), cmp_key3);
+    for (int64_t i = 0; i < s->n; i++) {
+        memcpy(coords + 3 * i, t[i].c, sizeof(int32_t) * 3);
+        if (voxels) memcpy(voxels + i * VPB * 8, s->vox + (int64_t)t[i].idx * VPB, VPB * 8);
+    }
+    free(t);
+}
+
+/* Replace the scene with the given blocks (coordinates + 8-byte voxels). */
+void orc_import(orc_scene* s, int64_t n, const int32_t* coords, const uint8_t* voxels) {
+    orc_reset(s);
+    for (int64_t i = 0; i < n; i++) {
+        uint64_t k = pack_key(coords[3 * i], coords[3 * i + 1], coords[3 * i + 2]);
+        if (scene_add(s, k)) memcpy(s->vox + (s->n - 1) * VPB, voxels + i * VPB * 8, VPB * 8);
+    }
+}
+
+int orc_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}

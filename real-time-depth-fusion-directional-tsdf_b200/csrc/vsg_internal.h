@@ -1,0 +1,62 @@
+// vsg_internal.h -- host-side objects behind the opaque C handles.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/vsg.h"
+#include "vsg_device.cuh"
+
+namespace vsg {
+
+enum TimingSlot { kSlotAlloc = 0, kSlotIntegrate = 1, kSlotRender = 2, kNumSlots = 8 };
+
+struct Timing {
+    bool enabled = false;
+    static constexpr int kRing = 64;
+    cudaEvent_t ev[kNumSlots][kRing][2] = {};
+    int head[kNumSlots] = {};
+    int pending[kNumSlots] = {};
+    double ms[kNumSlots] = {};
+    uint32_t count[kNumSlots] = {};
+    bool created = false;
+};
+
+struct Scene {
+    vsg_params params{};
+    int occ_log2 = 8;
+    int sm_count = 148;
+    int device = 0;
+    SceneDev dev{};
+    uint32_t integrated_frames = 0;
+    Timing timing;
+};
+
+struct Renderer {
+    int w = 0, h = 0;
+    int device = 0;
+    float* depth = nullptr;
+    float4* position = nullptr;
+    float4* color = nullptr;
+    float4* normal = nullptr;
+    int sm_count = 148;
+};
+
+int scene_alloc_device(Scene* sc);
+void scene_free_device(Scene* sc);
+int scene_reset_device(Scene* sc, cudaStream_t st);
+int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H, float trunc,
+                    const float* pose, float fx, float fy, float cx, float cy, cudaStream_t st);
+int render_launch(Renderer* r, Scene* sc, const float cam[3], const float* pose_dev, const float* pose_host,
+                  float fx, float fy, float cx, float cy, float min_depth, float max_depth, cudaStream_t st);
+
+void timing_begin(Scene* sc, int slot, cudaStream_t st);
+void timing_end(Scene* sc, int slot, cudaStream_t st);
+
+}  // namespace vsg
+
+struct vsg_scene {
+    vsg::Scene impl;
+};
+struct vsg_renderer {
+    vsg::Renderer impl;
+};

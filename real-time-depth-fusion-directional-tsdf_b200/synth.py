@@ -1,0 +1,256 @@
+"""Seeded synthetic depth streams for the fusion path.
+
+The reference runs on proprietary intra-oral scans that are not available, so
+its inputs (VoxelScene::integrateFromScanData, VoxelScene.h:89-91: a
+camera-space point map float3, a colour map uchar3 and a normal map float3 per
+pixel, plus a row-major 4x4 camera->world pose) are produced here by ray
+tracing analytic scenes.  Depth noise follows a structured-light model
+sigma(z) = 0.0012 + 0.0019 (z - 0.4)^2 applied to z along each pixel ray; the
+point map is then p = ((u - cx) z / fx, (v - cy) z / fy, z), the convention of
+CustomDepthMapGenerator.cpp:81-222 (pixel (0,0,0) = invalid).
+
+Camera frame convention: x right, y down, z forward (OpenCV).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Intrinsics:
+    width: int
+    height: int
+    fx: float
+    fy: float
+    cx: float
+    cy: float
+
+
+@dataclasses.dataclass
+class Frame:
+    pointmap: np.ndarray  # (H, W, 3) float32, camera space, 0 = invalid
+    rgb: np.ndarray  # (H, W, 3) uint8
+    normals: np.ndarray  # (H, W, 3) float32, camera space
+    depth: np.ndarray  # (H, W) float32, 0 = invalid
+    pose: np.ndarray  # (4, 4) float32 camera->world, row-major
+
+
+@dataclasses.dataclass
+class Scene:
+    planes: list  # (point(3), normal(3)) one-sided planes
+    spheres: list  # (centre(3), radius)
+    boxes: list  # (min(3), max(3)) solid axis-aligned boxes
+    room: tuple | None = None  # (min(3), max(3)) viewed from inside
+
+
+def look_at(eye, target, up=(0.0, 1.0, 0.0)) -> np.ndarray:
+    """Camera->world pose with z toward target, y down in the image."""
+    eye = np.asarray(eye, np.float64)
+    f = np.asarray(target, np.float64) - eye
+    f /= np.linalg.norm(f)
+    x = np.cross(f, np.asarray(up, np.float64))
+    x /= np.linalg.norm(x)
+    y = np.cross(f, x)
+    T = np.eye(4)
+    T[:3, 0], T[:3, 1], T[:3, 2], T[:3, 3] = x, y, f, eye
+    return T
+
+
+def _trace(scene: Scene, o: np.ndarray, d: np.ndarray):
+    """Nearest hit distance along unit rays d (N,3) from origin o (3,)."""
+    n = d.shape[0]
+    tbest = np.full(n, np.inf)
+    nbest = np.zeros((n, 3))
+    eps = 1e-9
+    for (p0, nrm) in scene.planes:
+        nrm = np.asarray(nrm, np.float64)
+        den = d @ nrm
+        t = ((np.asarray(p0) - o) @ nrm) / np.where(np.abs(den) < eps, eps, den)
+        ok = (den < -eps) & (t > 0) & (t < tbest)
+        tbest = np.where(ok, t, tbest)
+        nbest[ok] = nrm
+    for (c, r) in scene.spheres:
+        oc = o - np.asarray(c)
+        b = d @ oc
+        cc = oc @ oc - r * r
+        disc = b * b - cc
+        sq = np.sqrt(np.maximum(disc, 0.0))
+        t = -b - sq
+        ok = (disc > 0) & (t > 0) & (t < tbest)
+        tbest = np.where(ok, t, tbest)
+        if ok.any():
+            hp = o + d[ok] * t[ok, None]
+            nbest[ok] = (hp - np.asarray(c)) / r
+    inv = 1.0 / np.where(np.abs(d) < eps, eps, d)
+    for (lo, hi) in scene.boxes:
+        t0 = (np.asarray(lo) - o) * inv
+        t1 = (np.asarray(hi) - o) * inv
+        tmin = np.minimum(t0, t1)
+        tmax = np.maximum(t0, t1)
+        tn = tmin.max(axis=1)
+        tf = tmax.min(axis=1)
+        ok = (tn <= tf) & (tn > 0) & (tn < tbest)
+        tbest = np.where(ok, tn, tbest)
+        if ok.any():
+            ax = tmin[ok].argmax(axis=1)
+            nn = np.zeros((ok.sum(), 3))
+            nn[np.arange(ax.size), ax] = -np.sign(d[ok][np.arange(ax.size), ax])
+            nbest[ok] = nn
+    if scene.room is not None:
+        lo, hi = np.asarray(scene.room[0]), np.asarray(scene.room[1])
+        t0 = (lo - o) * inv
+        t1 = (hi - o) * inv
+        tmax = np.maximum(t0, t1)
+        tf = tmax.min(axis=1)
+        ax = tmax.argmin(axis=1)
+        ok = (tf > 0) & (tf < tbest)
+        tbest = np.where(ok, tf, tbest)
+        if ok.any():
+            nn = np.zeros((ok.sum(), 3))
+            nn[np.arange(ax[ok].size), ax[ok]] = -np.sign(d[ok][np.arange(ax[ok].size), ax[ok]])
+            nbest[ok] = nn
+    return tbest, nbest
+
+
+def height_ramp(y: np.ndarray, top: float) -> np.ndarray:
+    """RGB colour ramp on world height (uint8)."""
+    t = np.clip(y / top, 0.0, 1.0)
+    rgb = np.stack([255.0 * t, 255.0 * (1.0 - np.abs(2.0 * t - 1.0)), 255.0 * (1.0 - t)], -1)
+    return np.clip(rgb, 0, 255).astype(np.uint8)
+
+
+def noise_sigma(z: np.ndarray) -> np.ndarray:
+    return 0.0012 + 0.0019 * (z - 0.4) ** 2
+
+
+def render_frame(scene: Scene, K: Intrinsics, pose: np.ndarray, rng: np.random.Generator | None,
+                 zmin: float = 0.2, zmax: float = 3.0, color_top: float = 0.7) -> Frame:
+    """Ray trace one frame.  Returns float32 maps; depths outside
+    [zmin, zmax] (the sensor range) are invalid."""
+    W, H = K.width, K.height
+    u, v = np.meshgrid(np.arange(W, dtype=np.float64), np.arange(H, dtype=np.float64))
+    dc = np.stack([(u - K.cx) / K.fx, (v - K.cy) / K.fy, np.ones_like(u)], -1).reshape(-1, 3)
+    R = pose[:3, :3].astype(np.float64)
+    o = pose[:3, 3].astype(np.float64)
+    dn = dc / np.linalg.norm(dc, axis=1, keepdims=True)
+    dw = dn @ R.T
+    t, nw = _trace(scene, o, dw)
+    z = t * dn[:, 2]
+    if rng is not None:
+        z = z + rng.standard_normal(z.shape) * noise_sigma(np.where(np.isfinite(z), z, 0.0))
+    valid = np.isfinite(z) & (z >= zmin) & (z <= zmax)
+    zz = np.where(valid, z, 0.0)
+    pts = dc * zz[:, None]
+    hw = o + dw * np.where(valid, t, 0.0)[:, None]
+    rgb = height_ramp(hw[:, 1], color_top)
+    rgb[~valid] = 0
+    nc = nw @ R
+    nc[~valid] = 0
+    return Frame(
+        pointmap=pts.reshape(H, W, 3).astype(np.float32),
+        rgb=rgb.reshape(H, W, 3),
+        normals=nc.reshape(H, W, 3).astype(np.float32),
+        depth=zz.reshape(H, W).astype(np.float32),
+        pose=pose.astype(np.float32),
+    )
+
+
+# ------------------------------------------------------------------ workloads
+
+def tabletop_scene(seed: int) -> Scene:
+    """Ground plane y=0 plus 3 spheres, radius U(0.1,0.3), centres
+    U([-0.4,0.4] x [0.1,0.4] x [-0.4,0.4])."""
+    rng = np.random.default_rng(seed)
+    spheres = []
+    for _ in range(3):
+        r = rng.uniform(0.1, 0.3)
+        c = np.array([rng.uniform(-0.4, 0.4), rng.uniform(0.1, 0.4), rng.uniform(-0.4, 0.4)])
+        spheres.append((c, r))
+    return Scene(planes=[((0.0, 0.0, 0.0), (0.0, 1.0, 0.0))], spheres=spheres, boxes=[])
+
+
+def orbit_poses(n: int, radius: float = 1.0, arc_deg: float = 60.0, elev_deg: float = 36.87) -> list:
+    """Camera orbit at `radius` metres from the origin over `arc_deg`,
+    elevated `elev_deg`, looking at the origin."""
+    poses = []
+    e = math.radians(elev_deg)
+    for i in range(n):
+        a = math.radians(arc_deg) * (i / max(n - 1, 1))
+        eye = (radius * math.cos(e) * math.cos(a), radius * math.sin(e), radius * math.cos(e) * math.sin(a))
+        poses.append(look_at(eye, (0.0, 0.0, 0.0)))
+    return poses
+
+
+TABLETOP_K = Intrinsics(640, 480, 525.0, 525.0, 319.5, 239.5)
+
+
+def scaled_intrinsics(K: Intrinsics, width: int, height: int) -> Intrinsics:
+    sx, sy = width / K.width, height / K.height
+    return Intrinsics(width, height, K.fx * sx, K.fy * sy, (K.cx + 0.5) * sx - 0.5, (K.cy + 0.5) * sy - 0.5)
+
+
+def tabletop_stream(seed: int = 0, frames: int = 30, width: int = 640, height: int = 480,
+                    noise: bool = True) -> tuple[list, Intrinsics]:
+    """Plain-method tabletop workload: 640x480 (fx=fy=525, cx=319.5,
+    cy=239.5), orbit of 1.0 m over 60 degrees; smaller sizes scale the
+    intrinsics."""
+    scene = tabletop_scene(seed)
+    K = TABLETOP_K if (width, height) == (640, 480) else scaled_intrinsics(TABLETOP_K, width, height)
+    out = []
+    for i, T in enumerate(orbit_poses(frames)):
+        rng = np.random.default_rng([seed, i]) if noise else None
+        out.append(render_frame(scene, K, T, rng))
+    return out, K
+
+
+def room_scene(seed: int, n_boxes: int = 40, n_spheres: int = 20) -> Scene:
+    """4 x 3 x 2.5 m room (x in [-2,2], z in [-1.5,1.5], y in [0,2.5]) with
+    axis-aligned boxes (sides U(0.05,0.6)) and spheres."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.array([-2.0, 0.0, -1.5]), np.array([2.0, 2.5, 1.5])
+    boxes = []
+    for _ in range(n_boxes):
+        s = rng.uniform(0.05, 0.6, 3)
+        c = rng.uniform(lo + s / 2, hi - s / 2)
+        boxes.append((c - s / 2, c + s / 2))
+    spheres = []
+    for _ in range(n_spheres):
+        r = rng.uniform(0.05, 0.3)
+        spheres.append((rng.uniform(lo + r, hi - r), r))
+    return Scene(planes=[], spheres=spheres, boxes=boxes, room=(tuple(lo), tuple(hi)))
+
+
+def random_walk_poses(n: int, seed: int, step_m: float = 0.005, step_deg: float = 0.3,
+                      start=(0.0, 1.25, 0.0)) -> list:
+    rng = np.random.default_rng(seed + 7919)
+    T = look_at(start, (start[0] + 1.0, start[1] - 0.2, start[2] + 0.3))
+    poses = []
+    for _ in range(n):
+        poses.append(T.copy())
+        dt = rng.standard_normal(3)
+        dt *= step_m / max(np.linalg.norm(dt), 1e-12)
+        ax = rng.standard_normal(3)
+        ax /= max(np.linalg.norm(ax), 1e-12)
+        ang = math.radians(step_deg)
+        Kx = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+        dR = np.eye(3) + math.sin(ang) * Kx + (1 - math.cos(ang)) * Kx @ Kx
+        T[:3, :3] = T[:3, :3] @ dR
+        T[:3, 3] = np.clip(T[:3, 3] + dt, (-1.6, 0.4, -1.1), (1.6, 2.1, 1.1))
+    return poses
+
+
+ROOM_K = Intrinsics(1280, 720, 910.0, 910.0, 639.5, 359.5)
+
+
+def room_stream(seed: int = 1, frames: int = 300, width: int = 1280, height: int = 720,
+                frame_ids=None) -> tuple[list, Intrinsics]:
+    """Larger single stream: seeded room, random-walk trajectory."""
+    scene = room_scene(seed)
+    K = ROOM_K if (width, height) == (1280, 720) else scaled_intrinsics(ROOM_K, width, height)
+    poses = random_walk_poses(frames, seed)
+    ids = range(frames) if frame_ids is None else frame_ids
+    return [render_frame(scene, K, poses[i], np.random.default_rng([seed, i]), zmin=0.2, zmax=4.0,
+                         color_top=2.5) for i in ids], K

@@ -1,0 +1,238 @@
+"""Thin ctypes binding of libvsg.so (include/vsg.h) for Python callers and tests.
+
+Device buffers are passed as torch CUDA tensors (their data_ptr) or raw
+integers; host buffers as numpy arrays.  The library must be built
+(build.py); there is no fallback implementation: loading fails loudly when
+libvsg.so is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvsg.so")
+
+VSG_OK = 0
+STATUS = {0: "VSG_OK", 1: "VSG_ERR_INVALID_ARG", 2: "VSG_ERR_NOT_ALLOCATED", 3: "VSG_ERR_CUDA",
+          4: "VSG_ERR_OUT_OF_MEMORY", 5: "VSG_ERR_TOO_LARGE"}
+FLAG_HEAP_EXHAUSTED, FLAG_CHAIN_EXHAUSTED, FLAG_COORD_RANGE, FLAG_INSERT_RETRY, FLAG_MARCH_LIMIT = 1, 2, 4, 8, 16
+
+# every symbol include/vsg.h declares
+EXPORTS = [
+    "vsg_params_default", "vsg_scene_create", "vsg_scene_destroy", "vsg_scene_reset", "vsg_scene_params",
+    "vsg_integrate", "vsg_scene_stats", "vsg_scene_export", "vsg_renderer_create", "vsg_renderer_destroy",
+    "vsg_render", "vsg_render_hostpose", "vsg_renderer_outputs", "vsg_renderer_download",
+    "vsg_timing_enable", "vsg_timing_read", "vsg_timing_reset", "vsg_version",
+]
+
+
+class VsgError(RuntimeError):
+    def __init__(self, fn: str, code: int):
+        super().__init__(f"{fn} failed: {STATUS.get(code, code)}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("voxel_size", ctypes.c_float), ("truncation", ctypes.c_float),
+                ("truncation_scale", ctypes.c_float), ("hash_num_slots", ctypes.c_uint32),
+                ("num_sdf_blocks", ctypes.c_uint32), ("max_chain_nodes", ctypes.c_uint32),
+                ("occupancy_log2", ctypes.c_uint32)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in (
+        "allocated_blocks", "free_blocks", "high_water", "chain_nodes_used", "integrated_frames",
+        "frame_valid_pixels", "frame_new_blocks", "frame_visible_blocks", "frame_updated_blocks",
+        "frame_updated_voxels", "render_hits", "render_misses", "flags")]
+
+    def as_dict(self) -> dict:
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
+_lib = None
+_P = ctypes.c_void_p
+_F = ctypes.c_float
+_I = ctypes.c_int
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run build.py (no CPU fallback exists)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name in EXPORTS:
+            getattr(L, name).restype = ctypes.c_int
+        L.vsg_version.restype = ctypes.c_char_p
+        L.vsg_params_default.argtypes = [ctypes.POINTER(Params)]
+        L.vsg_scene_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(_P)]
+        L.vsg_scene_destroy.argtypes = [_P]
+        L.vsg_scene_reset.argtypes = [_P, _P]
+        L.vsg_scene_params.argtypes = [_P, ctypes.POINTER(Params)]
+        L.vsg_integrate.argtypes = [_P, _P, _P, _P, _I, _I, _F, _P, _F, _F, _F, _F, _P]
+        L.vsg_scene_stats.argtypes = [_P, ctypes.POINTER(Stats)]
+        L.vsg_scene_export.argtypes = [_P, _P, _P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
+        L.vsg_renderer_create.argtypes = [_I, _I, ctypes.POINTER(_P)]
+        L.vsg_renderer_destroy.argtypes = [_P]
+        L.vsg_render.argtypes = [_P, _P, _P, _P, _F, _F, _F, _F, _F, _F, _P]
+        L.vsg_render_hostpose.argtypes = [_P, _P, _P, _P, _F, _F, _F, _F, _F, _F, _P]
+        L.vsg_renderer_outputs.argtypes = [_P] + [ctypes.POINTER(_P)] * 4
+        L.vsg_renderer_download.argtypes = [_P, _P, _P, _P, _P]
+        L.vsg_timing_enable.argtypes = [_P, _I]
+        L.vsg_timing_read.argtypes = [_P, _P, _P, _I]
+        L.vsg_timing_reset.argtypes = [_P]
+        _lib = L
+    return _lib
+
+
+def check(fn: str, code: int):
+    if code != VSG_OK:
+        raise VsgError(fn, code)
+
+
+def _dptr(x) -> int:
+    """Device pointer of a torch tensor or an int."""
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    return int(x.data_ptr())
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        return 0
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)
+
+
+def _hptr(a: np.ndarray):
+    return a.ctypes.data_as(_P)
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    check("vsg_params_default", lib().vsg_params_default(ctypes.byref(p)))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class Scene:
+    """VoxelScene over the C ABI (vsg_scene_*, vsg_integrate)."""
+
+    def __init__(self, params: Params | None = None, **kw):
+        self.L = lib()
+        self.params = params if params is not None else default_params(**kw)
+        h = _P()
+        check("vsg_scene_create", self.L.vsg_scene_create(ctypes.byref(self.params), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.vsg_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reset(self, stream=None):
+        check("vsg_scene_reset", self.L.vsg_scene_reset(self.h, _stream(stream)))
+
+    def integrate(self, pointmap, rgb, normals, width, height, truncation, pose, fx, fy, cx, cy, stream=None):
+        T = np.ascontiguousarray(np.asarray(pose, np.float32).reshape(16))
+        check("vsg_integrate", self.L.vsg_integrate(
+            self.h, _dptr(pointmap), _dptr(rgb), _dptr(normals), int(width), int(height), _F(truncation),
+            _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _stream(stream)))
+
+    def stats(self) -> dict:
+        st = Stats()
+        check("vsg_scene_stats", self.L.vsg_scene_stats(self.h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def export(self, with_voxels: bool = True):
+        """(coords (n,3) int32 sorted, voxel bytes (n, 4096) uint8 or None)."""
+        n = ctypes.c_uint32(0)
+        dummy = np.zeros(3, np.int32)
+        rc = self.L.vsg_scene_export(self.h, _hptr(dummy), None, 0, ctypes.byref(n))
+        if rc not in (VSG_OK, 5):
+            check("vsg_scene_export", rc)
+        cnt = int(n.value)
+        coords = np.zeros((max(cnt, 1), 3), np.int32)
+        vox = np.zeros((max(cnt, 1), 4096), np.uint8) if with_voxels else None
+        check("vsg_scene_export", self.L.vsg_scene_export(
+            self.h, _hptr(coords), _hptr(vox) if with_voxels else None, cnt, ctypes.byref(n)))
+        return coords[:cnt], (vox[:cnt] if with_voxels else None)
+
+    def timing(self, enable: bool):
+        check("vsg_timing_enable", self.L.vsg_timing_enable(self.h, int(enable)))
+
+    def timing_read(self) -> tuple[np.ndarray, np.ndarray]:
+        ms = np.zeros(8, np.float64)
+        cnt = np.zeros(8, np.uint32)
+        check("vsg_timing_read", self.L.vsg_timing_read(self.h, _hptr(ms), _hptr(cnt), 8))
+        return ms, cnt
+
+    def timing_reset(self):
+        check("vsg_timing_reset", self.L.vsg_timing_reset(self.h))
+
+
+class Renderer:
+    """RayCastRender over the C ABI (vsg_renderer_*, vsg_render)."""
+
+    def __init__(self, width: int, height: int):
+        self.L = lib()
+        h = _P()
+        check("vsg_renderer_create", self.L.vsg_renderer_create(int(width), int(height), ctypes.byref(h)))
+        self.h = h
+        self.width, self.height = width, height
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.vsg_renderer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, scene: Scene, pose, fx, fy, cx, cy, min_depth, max_depth, cam_pos=None, pose_dev=None,
+               stream=None):
+        T = np.ascontiguousarray(np.asarray(pose, np.float32).reshape(16))
+        cam = np.ascontiguousarray(np.array([T[3], T[7], T[11]], np.float32) if cam_pos is None
+                                   else np.asarray(cam_pos, np.float32))
+        if pose_dev is not None:
+            check("vsg_render", self.L.vsg_render(self.h, scene.h, _hptr(cam), _dptr(pose_dev), _F(fx), _F(fy),
+                                                  _F(cx), _F(cy), _F(min_depth), _F(max_depth), _stream(stream)))
+        else:
+            check("vsg_render_hostpose", self.L.vsg_render_hostpose(
+                self.h, scene.h, _hptr(cam), _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _F(min_depth),
+                _F(max_depth), _stream(stream)))
+
+    def outputs(self) -> dict:
+        ps = [_P() for _ in range(4)]
+        check("vsg_renderer_outputs", self.L.vsg_renderer_outputs(self.h, *[ctypes.byref(p) for p in ps]))
+        return {k: int(p.value or 0) for k, p in zip(("depth", "position", "color", "normal"), ps)}
+
+    def download(self) -> dict:
+        n = self.width * self.height
+        d = np.zeros((self.height, self.width), np.float32)
+        p = np.zeros((self.height, self.width, 4), np.float32)
+        c = np.zeros((self.height, self.width, 4), np.float32)
+        nm = np.zeros((self.height, self.width, 4), np.float32)
+        check("vsg_renderer_download", self.L.vsg_renderer_download(self.h, _hptr(d), _hptr(p), _hptr(c), _hptr(nm)))
+        assert n == d.size
+        return {"depth": d, "position": p, "color": c, "normal": nm}
+
+
+def version() -> str:
+    return lib().vsg_version().decode()
