@@ -91,7 +91,7 @@ class ClockSampler:
         sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
         mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if "Active" in r[3 + i]})
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].strip() == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.rows)}
 
@@ -217,16 +217,17 @@ def run_ours(args):
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    launches_per_step = 1 + len(dev) * (3 + 2)  # reset(3 kernels + memsets) + per frame
+    # per step: reset (3 kernels) + per frame: frame_begin, alloc, select, integrate, render_begin, render
+    launches_per_step = 3 + len(dev) * 6
     # per-kernel times (separate pass with events around each launch)
     sc.timing(True)
     sc.timing_reset()
     step()
     kms, kcnt = sc.timing_read()
     sc.timing(False)
-    names = ["alloc", "integrate", "render"]
-    kern = {names[i]: {"ms_per_launch": float(kms[i] / max(kcnt[i], 1)), "launches": int(kcnt[i])}
-            for i in range(3)}
+    names = {0: "alloc", 1: "integrate", 2: "render", 3: "select"}
+    kern = {nm: {"ms_per_launch": float(kms[i] / max(kcnt[i], 1)), "launches": int(kcnt[i])}
+            for i, nm in names.items()}
     # algorithmic bytes per launch (canonical 8-B voxel)
     npx = W * H
     upd = np.mean([p["frame_updated_blocks"] for p in per_frame])
@@ -239,6 +240,10 @@ def run_ours(args):
     kern["alloc"]["alg_bytes"] = bytes_alloc
     kern["integrate"]["alg_bytes"] = bytes_integ
     kern["render"]["alg_bytes"] = bytes_render
+    kern["select"]["alg_bytes"] = float(np.mean([p["high_water"] for p in per_frame])) * 9 + vis * 4
+    kern["render"]["samples_full_per_frame"] = float(np.mean([p["render_samples_full"] for p in per_frame]))
+    for k in ("samples_skipped", "jumps", "singles"):
+        kern["render"][k + "_per_frame"] = float(np.mean([p["render_" + k] for p in per_frame]))
     dom = max(kern, key=lambda k: kern[k]["ms_per_launch"])
     peak, peak_kind = measured_peak_hbm()
     ach = kern[dom]["alg_bytes"] / (kern[dom]["ms_per_launch"] * 1e-3) / 1e9

@@ -80,7 +80,8 @@ typedef struct vsg_params {
     uint32_t hash_num_slots;  /* g_hashNumSlots: number of hash buckets */
     uint32_t num_sdf_blocks;  /* g_hashNumSDFBlocks: 8^3-voxel blocks in the pool */
     uint32_t max_chain_nodes; /* bucket-overflow entries; 0 = 2 * hash_num_slots */
-    uint32_t occupancy_log2;  /* occupancy grid is 2^k cells per axis (0 = 8) */
+    uint32_t occupancy_log2;  /* toroidal block grids (dense index, skip masks) are
+                                 2^k block positions per axis, k in 5..9 (0 = 7) */
 } vsg_params;
 
 typedef struct vsg_stats {
@@ -96,6 +97,10 @@ typedef struct vsg_stats {
     uint32_t frame_updated_voxels; /* last frame: voxels updated */
     uint32_t render_hits;        /* last render: rays that found a surface */
     uint32_t render_misses;      /* last render: rays that did not */
+    uint32_t render_samples_full;    /* last render: march samples evaluated */
+    uint32_t render_samples_skipped; /* last render: samples skipped as empty */
+    uint32_t render_jumps;           /* last render: O(1) jumps over skipped runs */
+    uint32_t render_singles;         /* last render: samples rejected one at a time */
     uint32_t flags;              /* VSG_FLAG_* (sticky since reset) */
 } vsg_stats;
 

@@ -105,14 +105,14 @@ int vsg_scene_create(const vsg_params* p, vsg_scene** out) {
     // GlobalParamsConfig::validateParameters analogue (globalParamasConfig.cpp:404-417)
     if (!(p->voxel_size > 0.0f) || p->hash_num_slots == 0u || p->num_sdf_blocks == 0u) return VSG_ERR_INVALID_ARG;
     if (p->num_sdf_blocks > (1u << 26) || p->hash_num_slots > (1u << 28)) return VSG_ERR_TOO_LARGE;
-    if (p->occupancy_log2 > 10u) return VSG_ERR_TOO_LARGE;
+    // (pools above 2^22 - 3 blocks resolve every block through the hash)
+    if (p->occupancy_log2 > 9u || (p->occupancy_log2 != 0u && p->occupancy_log2 < 5u)) return VSG_ERR_TOO_LARGE;
     vsg_scene* h = new (std::nothrow) vsg_scene();
     if (!h) return VSG_ERR_OUT_OF_MEMORY;
     Scene& sc = h->impl;
     sc.params = *p;
     if (sc.params.max_chain_nodes == 0u) sc.params.max_chain_nodes = 2u * p->hash_num_slots;
-    sc.occ_log2 = p->occupancy_log2 ? (int)p->occupancy_log2 : 8;
-    if (sc.occ_log2 < 2) sc.occ_log2 = 2;
+    sc.bidx_log2 = p->occupancy_log2 ? (int)p->occupancy_log2 : 7;
     if (cudaGetDevice(&sc.device) != cudaSuccess) {
         delete h;
         return VSG_ERR_CUDA;
@@ -188,6 +188,10 @@ int vsg_scene_stats(vsg_scene* s, vsg_stats* out) {
     out->frame_updated_voxels = f.n_upd_voxels;
     out->render_hits = f.hits;
     out->render_misses = f.misses;
+    out->render_samples_full = f.samples_full;
+    out->render_samples_skipped = f.samples_skipped;
+    out->render_jumps = f.jumps;
+    out->render_singles = f.singles;
     out->flags = c.flags;
     return VSG_OK;
 }

@@ -11,9 +11,22 @@
 //   block_key   u64[B]            pool block -> packed coordinate (EMPTY = free)
 //   block_slot  i32[B]            pool block -> entry index (>= S*8: chain node)
 //   block_fresh u8[B]             1 until the block's first integration pass
+//   block_wmask u64[B]            bit (sz*4+sy)*4+sx: sub-cube (2x2x2 voxels)
+//                                 holds a voxel with weight > 0
 //   heap        u32[B]            free-list stack of pool indices
-//   occ_raw     u32[cells/32]     toroidal bit per allocated block
-//   occ_dil     u32[cells/32]     same, dilated by one block in every direction
+//   bindex      u64[2^(3k)]       dense toroidal block index: cell (x,y,z) mod 2^k
+//                                 holds ptr (22 bits) | high coordinate bits
+//                                 (tag) << 22 of the one block mapped there;
+//                                 ~0 = none, ~0-1 = several (use the hash)
+//   dwm         u64[2^(3k)]       per toroidal block position: sub-cubes that
+//                                 have a weighted sub-cube within one sub-cube
+//                                 (3x3x3, across block faces); ray-march skip
+//   sup         u32[2^(3(k-3))/32] per toroidal super-cell (8^3 block
+//                                 positions): some dwm word in it is non-zero
+//   visible     u32[B]            pool indices the current frame integrates
+//   pix_world   float4[W*H]       per pixel of the current frame: world point
+//                                 T*p and its camera distance (-1: invalid)
+//   pix_rgb     u32[W*H]          per pixel colour, packed
 //
 // Packed block key: 21-bit two's complement per axis, x in bits 42..62,
 // y in 21..41, z in 0..20; ~0 = empty, ~0-1 = deleted (tombstone).
@@ -74,10 +87,14 @@ struct FrameCounters {
     uint32_t n_visible;      // blocks passed to integration
     uint32_t n_upd_blocks;   // blocks with >= 1 updated voxel
     uint32_t n_upd_voxels;   // voxels updated
-    uint32_t chunk;          // integration work queue
+    uint32_t chunk;          // selection / integration work queues
+    uint32_t work;
     uint32_t hits;           // render counters
     uint32_t misses;
-    uint32_t pad[5];
+    uint32_t samples_full;   // march samples evaluated with trilinear taps
+    uint32_t samples_skipped;  // march samples skipped as provably invalid
+    uint32_t jumps;          // O(1) jumps over runs of skipped samples
+    uint32_t singles;        // samples evaluated at a cell boundary (no jump)
 };
 
 struct SceneDev {
@@ -88,16 +105,20 @@ struct SceneDev {
     unsigned long long* block_key;
     int* block_slot;
     uint8_t* block_fresh;
+    unsigned long long* block_wmask;  // per block: 2x2x2-voxel sub-cubes holding a weighted voxel
     uint32_t* heap;
-    uint32_t* occ_raw;
-    uint32_t* occ_dil;
+    unsigned long long* bindex;
+    unsigned long long* dwm;
+    uint32_t* sup;
     uint32_t* visible;
+    float4* pix_world;   // per pixel of the current frame: T*p and |T*p - c| (-1 = invalid)
+    uint32_t* pix_rgb;   // per pixel: r | g<<8 | b<<16
     SceneCounters* ctr;
     FrameCounters* frame;
     uint32_t num_buckets;
     int num_blocks;
     int max_nodes;
-    int occ_log2;
+    int bidx_log2;  // k: toroidal block grid of 2^k positions per axis
     float voxel;
 };
 
@@ -156,16 +177,46 @@ __host__ __device__ __forceinline__ float ord2f(uint32_t u) {
 #endif
 }
 
-// --------------------------------------------------------- occupancy grid
+// ------------------------------------------- sub-cube masks and skip grid
 
-__device__ __forceinline__ uint32_t occ_bit(int x, int y, int z, int lg) {
+// 4x4x4 sub-cubes (2x2x2 voxels each) of a block: bit (cz*4 + cy)*4 + cx
+constexpr unsigned long long kX0 = 0x1111111111111111ull, kX3 = 0x8888888888888888ull;
+constexpr unsigned long long kY0 = 0x000F000F000F000Full, kY3 = 0xF000F000F000F000ull;
+constexpr unsigned long long kZ0 = 0x000000000000FFFFull, kZ3 = 0xFFFF000000000000ull;
+
+// Part of the one-sub-cube dilation of mask m that falls in the neighbour
+// block at offset d (-1, 0, +1) along x / y / z.
+__host__ __device__ __forceinline__ unsigned long long dil_x(unsigned long long m, int d) {
+    return d == 0 ? (m | ((m & ~kX3) << 1) | ((m & ~kX0) >> 1)) : d > 0 ? ((m & kX3) >> 3) : ((m & kX0) << 3);
+}
+__host__ __device__ __forceinline__ unsigned long long dil_y(unsigned long long m, int d) {
+    return d == 0 ? (m | ((m & ~kY3) << 4) | ((m & ~kY0) >> 4)) : d > 0 ? ((m & kY3) >> 12) : ((m & kY0) << 12);
+}
+__host__ __device__ __forceinline__ unsigned long long dil_z(unsigned long long m, int d) {
+    return d == 0 ? (m | ((m & ~kZ3) << 16) | ((m & ~kZ0) >> 16)) : d > 0 ? ((m & kZ3) >> 48) : ((m & kZ0) << 48);
+}
+
+__host__ __device__ __forceinline__ uint32_t grid_bit(int x, int y, int z, int lg) {
     const uint32_t m = (1u << lg) - 1u;
     return (((uint32_t)z & m) << (2 * lg)) | (((uint32_t)y & m) << lg) | ((uint32_t)x & m);
 }
 
-__device__ __forceinline__ bool occ_test(const uint32_t* occ, int x, int y, int z, int lg) {
-    uint32_t b = occ_bit(x, y, z, lg);
-    return (__ldg(occ + (b >> 5)) >> (b & 31)) & 1u;
+// ------------------------------------------------------ dense block index
+
+constexpr unsigned long long kIdxEmpty = 0xFFFFFFFFFFFFFFFFull;
+constexpr unsigned long long kIdxShared = 0xFFFFFFFFFFFFFFFEull;
+constexpr uint32_t kIdxPtrMask = 0x3FFFFFu;  // pools up to 2^22 - 3 blocks use the index
+
+__host__ __device__ __forceinline__ uint32_t bidx_cell(int x, int y, int z, int k) {
+    const uint32_t m = (1u << k) - 1u;
+    return (((uint32_t)z & m) << (2 * k)) | (((uint32_t)y & m) << k) | ((uint32_t)x & m);
+}
+
+__host__ __device__ __forceinline__ unsigned long long bidx_tag(int x, int y, int z, int k) {
+    const int hb = 21 - k;
+    const unsigned long long m = (1ull << hb) - 1ull;
+    return ((((unsigned long long)(unsigned)(x >> k)) & m) << (2 * hb)) |
+           ((((unsigned long long)(unsigned)(y >> k)) & m) << hb) | (((unsigned long long)(unsigned)(z >> k)) & m);
 }
 
 // ------------------------------------------------------------ hash lookup
@@ -191,6 +242,16 @@ __device__ __forceinline__ int lookup_block(const SceneDev& s, unsigned long lon
         n = (int)e.w;
     }
     return -1;
+}
+
+// Pool index of block (x,y,z) through the dense index; the hash resolves
+// cells shared by several blocks.  -1 = not allocated.
+__device__ __forceinline__ int block_ptr(const SceneDev& s, int x, int y, int z) {
+    if (!coord_ok(x, y, z)) return -1;
+    const unsigned long long e = __ldg(s.bindex + bidx_cell(x, y, z, s.bidx_log2));
+    if (e == kIdxEmpty) return -1;
+    if (e == kIdxShared) return lookup_block(s, pack_key(x, y, z), x, y, z);
+    return ((e >> 22) == bidx_tag(x, y, z, s.bidx_log2)) ? (int)(e & kIdxPtrMask) : -1;
 }
 
 __device__ __forceinline__ uint32_t pack_rgbw(uint32_t r, uint32_t g, uint32_t b, uint32_t w) {

@@ -1,17 +1,21 @@
 // vsg_fusion.cu -- block allocation, visible-block selection and TSDF
 // integration kernels, plus the scene half of the C ABI (include/vsg.h).
 //
-// One frame is three stream-ordered launches and no host synchronisation:
+// One frame is four stream-ordered launches and no host synchronisation:
 //   k_frame_begin   clear the per-frame counters
 //   k_alloc         per 16x16 pixel tile: DDA along each pixel's truncation
 //                   band (VoxelScene.cu:295-633), de-duplicate the visited
 //                   blocks in shared memory, insert the unique ones with a
 //                   warp-cooperative atomicCAS bucket probe (8 lanes per
-//                   key, one 128-B bucket line) and a linked-list overflow
-//   k_integrate     persistent: warps take 32 pool blocks at a time, keep the
-//                   ones the frame can touch (conservative frustum and depth
-//                   band test, or new this frame) by ballot + popc, append
-//                   them to the visible list and update their 512 voxels
+//                   key, one 128-B bucket line) and a linked-list overflow;
+//                   also writes each pixel's world point T*p and camera
+//                   distance once (bit-identical to the per-voxel
+//                   recomputation of VoxelScene.cu:1052-1062)
+//   k_select        visible-block compaction: one thread per pool block,
+//                   conservative frustum + depth-band test (or new this
+//                   frame), ballot + popc + one atomic per warp
+//   k_integrate     persistent: one warp per visible block, 8 voxels per
+//                   lane per batch with all gathers issued before use
 //                   (VoxelScene.cu:918-1146)
 #include <cuda_runtime.h>
 
@@ -38,6 +42,7 @@ constexpr int kMaxDDA = 1024;    // VoxelScene.cu:417
 struct AllocArgs {
     SceneDev s;
     const float* pm;
+    const uint8_t* rgb;
     int W, H;
     float trunc;
     Pose pose;
@@ -67,22 +72,11 @@ __device__ __forceinline__ void xform(const Pose& P, float x, float y, float z, 
     oz = P.T[8] * x + P.T[9] * y + P.T[10] * z + P.T[11];
 }
 
-__device__ __forceinline__ void set_occupancy(const SceneDev& s, int x, int y, int z) {
-    uint32_t b = occ_bit(x, y, z, s.occ_log2);
-    atomicOr(s.occ_raw + (b >> 5), 1u << (b & 31));
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                uint32_t d = occ_bit(x + dx, y + dy, z + dz, s.occ_log2);
-                atomicOr(s.occ_dil + (d >> 5), 1u << (d & 31));
-            }
-}
-
 // Give a freshly inserted key storage.  entry_key / entry_ptr are the
 // fields of the slot (bucket entry or chain node) the caller now owns.
 // Heap pop as consumeHeap in VoxelScene.cu:183-195 (reference pops index
 // heapCounter, we pop free_count - 1: the same stack).
-__device__ bool claim_block(const SceneDev& s, unsigned long long key, unsigned long long* entry_key,
+__device__ __noinline__ bool claim_block(const SceneDev& s, unsigned long long key, unsigned long long* entry_key,
                             int* entry_ptr, int slot_index) {
     int old = atomicSub(&s.ctr->free_count, 1);
     if (old <= 0) {
@@ -100,14 +94,22 @@ __device__ bool claim_block(const SceneDev& s, unsigned long long key, unsigned 
     atomicMax(&s.ctr->high_water, blk + 1);
     int x, y, z;
     unpack_key(key, x, y, z);
-    set_occupancy(s, x, y, z);
+    // dense index: first block of a cell owns it, a second one marks it shared
+    {
+        unsigned long long* cell = s.bindex + bidx_cell(x, y, z, s.bidx_log2);
+        const unsigned long long mine = blk < kIdxPtrMask - 2u
+                                            ? ((bidx_tag(x, y, z, s.bidx_log2) << 22) | (unsigned long long)blk)
+                                            : kIdxShared;
+        const unsigned long long prev = atomicCAS(cell, kIdxEmpty, mine);
+        if (prev != kIdxEmpty && prev != mine && prev != kIdxShared) atomicExch(cell, kIdxShared);
+    }
     atomicAdd(&s.frame->n_new, 1u);
     return true;
 }
 
 // Search the overflow chain of bucket b for key; append it when absent.
 // Lock-free: a node is published by CAS on the tail link.
-__device__ void chain_insert(const SceneDev& s, uint32_t b, unsigned long long key, bool insert) {
+__device__ __noinline__ void chain_insert(const SceneDev& s, uint32_t b, unsigned long long key, bool insert) {
     int* link = s.bucket_next + b;
     int mine = -1;
     const int base = (int)s.num_buckets * kBucketSlots;
@@ -153,7 +155,7 @@ __device__ bool chain_contains(const SceneDev& s, uint32_t b, unsigned long long
 }
 
 // Single-thread insert (fallback when the shared set overflows).
-__device__ void insert_single(const SceneDev& s, unsigned long long key, int x, int y, int z) {
+__device__ __noinline__ void insert_single(const SceneDev& s, unsigned long long key, int x, int y, int z) {
     const uint32_t b = bucket_of(x, y, z, s.num_buckets);
     Entry* bk = s.buckets + (size_t)b * kBucketSlots;
     for (int it = 0; it < 4 * kBucketSlots; ++it) {
@@ -272,7 +274,13 @@ __global__ void __launch_bounds__(kTile* kTile) k_alloc(AllocArgs a) {
         const float p1 = __ldg(a.pm + 3 * pi + 1);
         const float p2 = __ldg(a.pm + 3 * pi + 2);
         // integration validity (VoxelScene.cu:1040-1046) drives the depth band
+        float4 prep = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
         if (p0 != 0.0f || p1 != 0.0f || p2 != 0.0f) {
+            // depthPos_world and cameraDist, VoxelScene.cu:1052-1062
+            float Px, Py, Pz;
+            xform(a.pose, p0, p1, p2, Px, Py, Pz);
+            const float ex = Px - a.pose.T[3], ey = Py - a.pose.T[7], ez = Pz - a.pose.T[11];
+            prep = make_float4(Px, Py, Pz, sqrtf(ex * ex + ey * ey + ez * ez));
             atomicAdd(&s_valid, 1u);
             if (isfinite(p0) && isfinite(p1) && isfinite(p2)) {
                 atomicMin(&s_zmin, f2ord(p2));
@@ -281,6 +289,9 @@ __global__ void __launch_bounds__(kTile* kTile) k_alloc(AllocArgs a) {
                 s_nonfinite = 1u;
             }
         }
+        s.pix_world[pi] = prep;
+        s.pix_rgb[pi] = (uint32_t)__ldg(a.rgb + 3 * pi) | ((uint32_t)__ldg(a.rgb + 3 * pi + 1) << 8) |
+                        ((uint32_t)__ldg(a.rgb + 3 * pi + 2) << 16);
         // allocBlocksFromDepthMapMethod1Kernel, VoxelScene.cu:547-633
         if (!(p2 <= 1e-6f)) {
             const float cx = a.pose.T[3], cy = a.pose.T[7], cz = a.pose.T[11];
@@ -376,8 +387,6 @@ __global__ void __launch_bounds__(kTile* kTile) k_alloc(AllocArgs a) {
 
 struct IntegArgs {
     SceneDev s;
-    const float* pm;
-    const uint8_t* rgb;
     int W, H;
     float trunc;
     Pose pose;
@@ -423,8 +432,55 @@ __device__ bool block_maybe_updated(const IntegArgs& a, int bx, int by, int bz, 
     return true;
 }
 
+// Visible-block compaction: one thread per pool block in [0, high_water),
+// ballot + popc, one atomic per warp.  Stands in for compactifyHashKernel
+// (VoxelScene.cu:1275-1300), which lists every allocated block: blocks the
+// test rejects cannot have a voxel updated this frame, so integrating only
+// the listed ones leaves every voxel as the full pass would.
+__global__ void __launch_bounds__(256) k_select(IntegArgs a) {
+    const SceneDev& s = a.s;
+    const int lane = threadIdx.x & 31;
+    const uint32_t hw = *(volatile uint32_t*)&s.ctr->high_water;
+    const FrameCounters fc = *s.frame;
+    const bool any_valid = fc.n_valid_px > 0;
+    const bool cull = fc.nonfinite == 0u && fc.zmin_ord != 0xFFFFFFFFu;
+    const float eps = 1e-3f + 2.0f * s.voxel;
+    const float zlo = cull ? ord2f(fc.zmin_ord) - a.trunc - eps : 0.0f;
+    const float zhi = cull ? ord2f(fc.zmax_ord) + a.trunc + eps : 0.0f;
+    for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < hw; b0 += gridDim.x * blockDim.x) {
+        const uint32_t b = b0 + threadIdx.x;
+        bool vis = false;
+        if (b < hw) {
+            const unsigned long long key = s.block_key[b];
+            if (key != kKeyEmpty && key != kKeyTomb) {
+                if (s.block_fresh[b]) {
+                    vis = true;
+                } else if (any_valid) {
+                    if (!cull) {
+                        vis = true;
+                    } else {
+                        int bx, by, bz;
+                        unpack_key(key, bx, by, bz);
+                        vis = block_maybe_updated(a, bx, by, bz, zlo, zhi);
+                    }
+                }
+            }
+        }
+        const unsigned mask = __ballot_sync(0xFFFFFFFFu, vis);
+        if (!mask) continue;
+        uint32_t pos = 0;
+        if (lane == 0) pos = atomicAdd(&s.frame->n_visible, (uint32_t)__popc(mask));
+        pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
+        if (vis) s.visible[pos + __popc(mask & ((1u << lane) - 1u))] = b;
+    }
+}
+
+constexpr int kIntegBatch = 8;  // voxels per lane with loads in flight together
+
 // Per-voxel TSDF update, VoxelScene.cu:954-1126, for the 16 voxels lane
-// `lane` owns in block blk: idx = 32k + lane.
+// `lane` owns in block blk (idx = 32k + lane), in batches of kIntegBatch:
+// projection of the whole batch, then its point gathers, then the SDF
+// decisions, then the voxel / colour loads, then the updates.
 __device__ void integrate_block(const IntegArgs& a, int blk, unsigned long long key, bool fresh, int lane) {
     const SceneDev& s = a.s;
     int bx, by, bz;
@@ -438,126 +494,140 @@ __device__ void integrate_block(const IntegArgs& a, int blk, unsigned long long 
     const float wx = (float)(int)((unsigned)bx * 8u + (unsigned)lx) * v;
     const float rx = wx - T[3];
     int cnt = 0;
-#pragma unroll 2
-    for (int k = 0; k < 16; ++k) {
-        const int ly = (lane >> 3) + ((k & 1) << 2);
-        const int lz = k >> 1;
-        const int idx = k * 32 + lane;
-        const float wy = (float)(int)((unsigned)by * 8u + (unsigned)ly) * v;
-        const float wz = (float)(int)((unsigned)bz * 8u + (unsigned)lz) * v;
-        const float ry = wy - T[7], rz = wz - T[11];
-        const float cxp = T[0] * rx + T[4] * ry + T[8] * rz;
-        const float cyp = T[1] * rx + T[5] * ry + T[9] * rz;
-        const float czp = T[2] * rx + T[6] * ry + T[10] * rz;
-        const float sx = cxp * a.fx / czp + a.cx;
-        const float sy = cyp * a.fy / czp + a.cy;
-        const int ix = __float2int_rz(sx + 0.5f), iy = __float2int_rz(sy + 0.5f);
-        bool upd = false;
-        float sdf = 0.0f;
-        size_t pi = 0;
-        if (ix >= 0 && ix < a.W && iy >= 0 && iy < a.H) {
-            pi = (size_t)iy * a.W + ix;
-            const float P0 = __ldg(a.pm + 3 * pi + 0);
-            const float P1 = __ldg(a.pm + 3 * pi + 1);
-            const float P2 = __ldg(a.pm + 3 * pi + 2);
-            if (P0 != 0.0f || P1 != 0.0f || P2 != 0.0f) {
-                const float Px = T[0] * P0 + T[1] * P1 + T[2] * P2 + T[3];
-                const float Py = T[4] * P0 + T[5] * P1 + T[6] * P2 + T[7];
-                const float Pz = T[8] * P0 + T[9] * P1 + T[10] * P2 + T[11];
-                const float dx = wx - Px, dy = wy - Py, dz = wz - Pz;
-                sdf = sqrtf(dx * dx + dy * dy + dz * dz);
-                const float ex = Px - camx, ey = Py - camy, ez = Pz - camz;
-                const float cdist = sqrtf(ex * ex + ey * ey + ez * ez);
+    unsigned long long wm = 0ull;  // sub-cubes that received a weight this frame
+#pragma unroll 1
+    for (int k0 = 0; k0 < 16; k0 += kIntegBatch) {
+        int pix[kIntegBatch];
+#pragma unroll
+        for (int j = 0; j < kIntegBatch; ++j) {
+            const int k = k0 + j;
+            const int ly = (lane >> 3) + ((k & 1) << 2);
+            const int lz = k >> 1;
+            const float wy = (float)(int)((unsigned)by * 8u + (unsigned)ly) * v;
+            const float wz = (float)(int)((unsigned)bz * 8u + (unsigned)lz) * v;
+            const float ry = wy - T[7], rz = wz - T[11];
+            const float cxp = T[0] * rx + T[4] * ry + T[8] * rz;
+            const float cyp = T[1] * rx + T[5] * ry + T[9] * rz;
+            const float czp = T[2] * rx + T[6] * ry + T[10] * rz;
+            const float sx = cxp * a.fx / czp + a.cx;
+            const float sy = cyp * a.fy / czp + a.cy;
+            const int ix = __float2int_rz(sx + 0.5f), iy = __float2int_rz(sy + 0.5f);
+            pix[j] = (ix >= 0 && ix < a.W && iy >= 0 && iy < a.H) ? iy * a.W + ix : -1;
+        }
+        float4 P[kIntegBatch];
+#pragma unroll
+        for (int j = 0; j < kIntegBatch; ++j)
+            P[j] = pix[j] >= 0 ? __ldg(s.pix_world + pix[j]) : make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        float sdfv[kIntegBatch];
+        bool upd[kIntegBatch];
+#pragma unroll
+        for (int j = 0; j < kIntegBatch; ++j) {
+            const int k = k0 + j;
+            const int ly = (lane >> 3) + ((k & 1) << 2);
+            const int lz = k >> 1;
+            const float wy = (float)(int)((unsigned)by * 8u + (unsigned)ly) * v;
+            const float wz = (float)(int)((unsigned)bz * 8u + (unsigned)lz) * v;
+            upd[j] = false;
+            sdfv[j] = 0.0f;
+            if (!(P[j].w < 0.0f)) {  // pixel valid: point != (0,0,0)
+                const float dx = wx - P[j].x, dy = wy - P[j].y, dz = wz - P[j].z;
+                float sdf = sqrtf(dx * dx + dy * dy + dz * dz);
                 const float vdist = sqrtf((wx - camx) * (wx - camx) + (wy - camy) * (wy - camy) +
                                           (wz - camz) * (wz - camz));
-                if (vdist < cdist) sdf = -sdf;
+                if (vdist < P[j].w) sdf = -sdf;
                 if (!(sdf < -t || sdf > t)) {
-                    sdf = fmaxf(-t, fminf(t, sdf));
-                    upd = true;
+                    sdfv[j] = fmaxf(-t, fminf(t, sdf));
+                    upd[j] = true;
                 }
             }
         }
-        if (upd) {
-            const Voxel old = fresh ? Voxel{0.0f, 0u} : vb[idx];
-            const float oldW = (float)(old.rgbw >> 24);
-            const float newW = oldW + 1.0f;
-            const float nsdf = (old.sdf * oldW + sdf * 1.0f) / newW;
-            const uint32_t nw = (uint32_t)fminf(255.0f, newW);
-            const float c0 = (float)__ldg(a.rgb + 3 * pi + 0);
-            const float c1 = (float)__ldg(a.rgb + 3 * pi + 1);
-            const float c2 = (float)__ldg(a.rgb + 3 * pi + 2);
-            const float nr = ((float)(old.rgbw & 0xFFu) * oldW + c0 * 1.0f) / newW;
-            const float ng = ((float)((old.rgbw >> 8) & 0xFFu) * oldW + c1 * 1.0f) / newW;
-            const float nb = ((float)((old.rgbw >> 16) & 0xFFu) * oldW + c2 * 1.0f) / newW;
-            Voxel nv;
-            nv.sdf = nsdf;
-            nv.rgbw = pack_rgbw((uint32_t)nr, (uint32_t)ng, (uint32_t)nb, nw);
-            vb[idx] = nv;
-            ++cnt;
-        } else if (fresh) {
-            vb[idx] = Voxel{0.0f, 0u};
+        Voxel old[kIntegBatch];
+        uint32_t col[kIntegBatch];
+#pragma unroll
+        for (int j = 0; j < kIntegBatch; ++j) {
+            const int idx = (k0 + j) * 32 + lane;
+            old[j] = Voxel{0.0f, 0u};
+            col[j] = 0u;
+            if (upd[j]) {
+                if (!fresh) old[j] = vb[idx];
+                col[j] = __ldg(s.pix_rgb + pix[j]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kIntegBatch; ++j) {
+            const int idx = (k0 + j) * 32 + lane;
+            if (upd[j]) {
+                const float oldW = (float)(old[j].rgbw >> 24);
+                const float newW = oldW + 1.0f;
+                const float nsdf = (old[j].sdf * oldW + sdfv[j] * 1.0f) / newW;
+                const uint32_t nw = (uint32_t)fminf(255.0f, newW);
+                const float nr = ((float)(old[j].rgbw & 0xFFu) * oldW + (float)(col[j] & 0xFFu) * 1.0f) / newW;
+                const float ng =
+                    ((float)((old[j].rgbw >> 8) & 0xFFu) * oldW + (float)((col[j] >> 8) & 0xFFu) * 1.0f) / newW;
+                const float nb =
+                    ((float)((old[j].rgbw >> 16) & 0xFFu) * oldW + (float)((col[j] >> 16) & 0xFFu) * 1.0f) / newW;
+                Voxel nv;
+                nv.sdf = nsdf;
+                nv.rgbw = pack_rgbw((uint32_t)nr, (uint32_t)ng, (uint32_t)nb, nw);
+                vb[idx] = nv;
+                ++cnt;
+                const int k = k0 + j;
+                const int ly = (lane >> 3) + ((k & 1) << 2), lz = k >> 1;
+                wm |= 1ull << ((((lz >> 1) * 4 + (ly >> 1)) * 4) + (lx >> 1));
+            } else if (fresh) {
+                vb[idx] = Voxel{0.0f, 0u};
+            }
         }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, o);
+    const unsigned wlo = __reduce_or_sync(0xFFFFFFFFu, (unsigned)wm);
+    const unsigned whi = __reduce_or_sync(0xFFFFFFFFu, (unsigned)(wm >> 32));
+    const unsigned long long old_wm = fresh ? 0ull : s.block_wmask[blk];
+    const unsigned long long newbits = (((unsigned long long)whi << 32) | wlo) & ~old_wm;
+    if (newbits && lane < 27) {
+        // newly weighted sub-cubes: dilate by one sub-cube into this block
+        // position and its 26 neighbours (one lane per neighbour)
+        const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
+        const unsigned long long mk = dil_z(dil_y(dil_x(newbits, dx), dy), dz);
+        if (mk) {
+            const int nx = bx + dx, ny = by + dy, nz = bz + dz;
+            atomicOr(s.dwm + bidx_cell(nx, ny, nz, s.bidx_log2), mk);
+            const uint32_t q = grid_bit(nx >> 3, ny >> 3, nz >> 3, s.bidx_log2 - 3);
+            atomicOr(s.sup + (q >> 5), 1u << (q & 31));
+        }
+    }
+    __syncwarp();
     if (lane == 0) {
         if (cnt) {
             atomicAdd(&s.frame->n_upd_blocks, 1u);
             atomicAdd(&s.frame->n_upd_voxels, (uint32_t)cnt);
         }
-        if (fresh) s.block_fresh[blk] = 0;
+        // only this warp touches the block during the launch
+        const unsigned long long nw = ((unsigned long long)whi << 32) | wlo;
+        if (fresh) {
+            s.block_wmask[blk] = nw;
+            s.block_fresh[blk] = 0;
+        } else if (nw) {
+            s.block_wmask[blk] |= nw;
+        }
     }
 }
 
+// One warp per visible block, taken from a work counter.
 __global__ void __launch_bounds__(256) k_integrate(IntegArgs a) {
     const SceneDev& s = a.s;
     const int lane = threadIdx.x & 31;
-    const uint32_t hw = *(volatile uint32_t*)&s.ctr->high_water;
-    const FrameCounters fc = *s.frame;
-    const bool any_valid = fc.n_valid_px > 0;
-    const bool cull = fc.nonfinite == 0u && fc.zmin_ord != 0xFFFFFFFFu;
-    const float eps = 1e-3f + 2.0f * s.voxel;
-    const float zlo = cull ? ord2f(fc.zmin_ord) - a.trunc - eps : 0.0f;
-    const float zhi = cull ? ord2f(fc.zmax_ord) + a.trunc + eps : 0.0f;
+    const uint32_t n = *(volatile uint32_t*)&s.frame->n_visible;
     for (;;) {
-        uint32_t chunk = 0;
-        if (lane == 0) chunk = atomicAdd(&s.frame->chunk, 1u);
-        chunk = __shfl_sync(0xFFFFFFFFu, chunk, 0);
-        const uint32_t base = chunk * 32u;
-        if (base >= hw) break;
-        const uint32_t b = base + lane;
-        bool vis = false, fresh = false;
-        unsigned long long key = kKeyEmpty;
-        if (b < hw) {
-            key = s.block_key[b];
-            if (key != kKeyEmpty && key != kKeyTomb) {
-                fresh = s.block_fresh[b] != 0;
-                if (fresh) {
-                    vis = true;
-                } else if (any_valid) {
-                    if (!cull) {
-                        vis = true;
-                    } else {
-                        int bx, by, bz;
-                        unpack_key(key, bx, by, bz);
-                        vis = block_maybe_updated(a, bx, by, bz, zlo, zhi);
-                    }
-                }
-            }
-        }
-        unsigned mask = __ballot_sync(0xFFFFFFFFu, vis);
-        if (!mask) continue;
-        uint32_t pos = 0;
-        if (lane == 0) pos = atomicAdd(&s.frame->n_visible, (uint32_t)__popc(mask));
-        pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
-        if (vis) s.visible[pos + __popc(mask & ((1u << lane) - 1u))] = b;
-        while (mask) {
-            const int j = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const unsigned long long kj = __shfl_sync(0xFFFFFFFFu, key, j);
-            const bool fj = __shfl_sync(0xFFFFFFFFu, fresh, j);
-            integrate_block(a, (int)(base + j), kj, fj, lane);
-        }
+        uint32_t i = 0;
+        if (lane == 0) i = atomicAdd(&s.frame->work, 1u);
+        i = __shfl_sync(0xFFFFFFFFu, i, 0);
+        if (i >= n) break;
+        const uint32_t b = s.visible[i];
+        const unsigned long long key = s.block_key[b];
+        const bool fresh = s.block_fresh[b] != 0;
+        integrate_block(a, (int)b, key, fresh, lane);
     }
 }
 
@@ -589,7 +659,7 @@ __global__ void k_frame_begin(FrameCounters* f) {
 // host side
 // ====================================================================
 
-static int occ_words(int lg) { return (int)((1ull << (3 * lg)) / 32ull); }
+static size_t sup_words(int k) { return ((1ull << (3 * (k - 3))) + 31ull) / 32ull; }
 
 int scene_alloc_device(Scene* sc) {
     SceneDev& d = sc->dev;
@@ -608,25 +678,34 @@ int scene_alloc_device(Scene* sc) {
     VSG_MALLOC(d.block_key, B * sizeof(unsigned long long));
     VSG_MALLOC(d.block_slot, B * sizeof(int));
     VSG_MALLOC(d.block_fresh, B);
+    VSG_MALLOC(d.block_wmask, B * sizeof(unsigned long long));
     VSG_MALLOC(d.heap, B * sizeof(uint32_t));
-    VSG_MALLOC(d.occ_raw, (size_t)occ_words(sc->occ_log2) * 4);
-    VSG_MALLOC(d.occ_dil, (size_t)occ_words(sc->occ_log2) * 4);
+    VSG_MALLOC(d.bindex, sizeof(unsigned long long) << (3 * sc->bidx_log2));
+    VSG_MALLOC(d.dwm, sizeof(unsigned long long) << (3 * sc->bidx_log2));
+    VSG_MALLOC(d.sup, sup_words(sc->bidx_log2) * 4);
     VSG_MALLOC(d.visible, B * sizeof(uint32_t));
+    d.pix_world = nullptr;
+    d.pix_rgb = nullptr;
+    sc->pix_capacity = 0;
     VSG_MALLOC(d.ctr, sizeof(SceneCounters));
     VSG_MALLOC(d.frame, sizeof(FrameCounters));
 #undef VSG_MALLOC
     d.num_buckets = (uint32_t)S;
     d.num_blocks = (int)B;
     d.max_nodes = (int)M;
-    d.occ_log2 = sc->occ_log2;
+    d.bidx_log2 = sc->bidx_log2;
     d.voxel = sc->params.voxel_size;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_integrate, 256, 0);
+    sc->integ_ctas_per_sm = per_sm > 0 ? per_sm : 2;
     return VSG_OK;
 }
 
 void scene_free_device(Scene* sc) {
     SceneDev& d = sc->dev;
-    void* ptrs[] = {d.buckets, d.bucket_next, d.nodes, d.voxels, d.block_key, d.block_slot, d.block_fresh,
-                    d.heap,    d.occ_raw,     d.occ_dil, d.visible, d.ctr,      d.frame};
+    void* ptrs[] = {d.sup,       d.dwm,     d.bindex,    d.block_wmask, d.buckets,   d.bucket_next,
+                    d.nodes,     d.voxels,  d.block_key, d.block_slot,  d.block_fresh, d.heap,
+                    d.visible,   d.pix_world, d.pix_rgb, d.ctr,         d.frame};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     memset(&d, 0, sizeof(d));
@@ -641,8 +720,9 @@ int scene_reset_device(Scene* sc, cudaStream_t st) {
     cudaMemsetAsync(d.nodes, 0xFF, M * sizeof(Node), st);
     cudaMemsetAsync(d.block_key, 0xFF, B * sizeof(unsigned long long), st);
     cudaMemsetAsync(d.block_fresh, 0, B, st);
-    cudaMemsetAsync(d.occ_raw, 0, (size_t)occ_words(sc->occ_log2) * 4, st);
-    cudaMemsetAsync(d.occ_dil, 0, (size_t)occ_words(sc->occ_log2) * 4, st);
+    cudaMemsetAsync(d.bindex, 0xFF, sizeof(unsigned long long) << (3 * sc->bidx_log2), st);
+    cudaMemsetAsync(d.dwm, 0, sizeof(unsigned long long) << (3 * sc->bidx_log2), st);
+    cudaMemsetAsync(d.sup, 0, sup_words(sc->bidx_log2) * 4, st);
     k_init_heap<<<(unsigned)((B + 255) / 256), 256, 0, st>>>(d.heap, (int)B);
     k_init_counters<<<1, 1, 0, st>>>(d.ctr, (int)B);
     k_frame_begin<<<1, 1, 0, st>>>(d.frame);
@@ -650,14 +730,32 @@ int scene_reset_device(Scene* sc, cudaStream_t st) {
     return cudaGetLastError() == cudaSuccess ? VSG_OK : VSG_ERR_CUDA;
 }
 
+static int ensure_pixel_buffers(Scene* sc, size_t npx) {
+    if (npx <= sc->pix_capacity) return VSG_OK;
+    // grows only: a first frame of a larger resolution allocates (outside
+    // any capture), later frames reuse
+    cudaFree(sc->dev.pix_world);
+    cudaFree(sc->dev.pix_rgb);
+    sc->dev.pix_world = nullptr;
+    sc->dev.pix_rgb = nullptr;
+    sc->pix_capacity = 0;
+    if (cudaMalloc(&sc->dev.pix_world, npx * sizeof(float4)) != cudaSuccess) return VSG_ERR_OUT_OF_MEMORY;
+    if (cudaMalloc(&sc->dev.pix_rgb, npx * sizeof(uint32_t)) != cudaSuccess) return VSG_ERR_OUT_OF_MEMORY;
+    sc->pix_capacity = npx;
+    return VSG_OK;
+}
+
 int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H, float trunc,
                     const float* pose, float fx, float fy, float cx, float cy, cudaStream_t st) {
+    const int prc = ensure_pixel_buffers(sc, (size_t)W * H);
+    if (prc != VSG_OK) return prc;
     Pose P;
     memcpy(P.T, pose, sizeof(P.T));
     k_frame_begin<<<1, 1, 0, st>>>(sc->dev.frame);
     AllocArgs aa;
     aa.s = sc->dev;
     aa.pm = pm;
+    aa.rgb = rgb;
     aa.W = W;
     aa.H = H;
     aa.trunc = trunc;
@@ -668,8 +766,6 @@ int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H
     timing_end(sc, kSlotAlloc, st);
     IntegArgs ia;
     ia.s = sc->dev;
-    ia.pm = pm;
-    ia.rgb = rgb;
     ia.W = W;
     ia.H = H;
     ia.trunc = trunc;
@@ -678,8 +774,11 @@ int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H
     ia.fy = fy;
     ia.cx = cx;
     ia.cy = cy;
+    timing_begin(sc, kSlotSelect, st);
+    k_select<<<sc->sm_count * 4, 256, 0, st>>>(ia);
+    timing_end(sc, kSlotSelect, st);
     timing_begin(sc, kSlotIntegrate, st);
-    k_integrate<<<sc->sm_count * 8, 256, 0, st>>>(ia);
+    k_integrate<<<sc->sm_count * sc->integ_ctas_per_sm, 256, 0, st>>>(ia);
     timing_end(sc, kSlotIntegrate, st);
     sc->integrated_frames++;
     return cudaGetLastError() == cudaSuccess ? VSG_OK : VSG_ERR_CUDA;

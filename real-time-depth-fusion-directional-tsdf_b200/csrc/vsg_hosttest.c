@@ -1,0 +1,19 @@
+/* Host build of the header-only helpers for CPU unit tests (tests load this
+ * through ctypes; the device library compiles the same headers). */
+#include "vsg_fpchain.h"
+
+float vsg_test_chain_advance(float r, float h, float target, int max_steps, int* steps) {
+    *steps = 0;
+    return vsg_chain_advance(r, h, target, max_steps, steps);
+}
+
+/* reference: serial additions */
+float vsg_test_chain_serial(float r, float h, float target, int max_steps, int* steps) {
+    int n = 0;
+    while (r < target && n < max_steps) {
+        r = r + h;
+        ++n;
+    }
+    *steps = n;
+    return r;
+}

@@ -8,7 +8,7 @@
 
 namespace vsg {
 
-enum TimingSlot { kSlotAlloc = 0, kSlotIntegrate = 1, kSlotRender = 2, kNumSlots = 8 };
+enum TimingSlot { kSlotAlloc = 0, kSlotIntegrate = 1, kSlotRender = 2, kSlotSelect = 3, kNumSlots = 8 };
 
 struct Timing {
     bool enabled = false;
@@ -23,10 +23,12 @@ struct Timing {
 
 struct Scene {
     vsg_params params{};
-    int occ_log2 = 8;
+    int bidx_log2 = 7;
     int sm_count = 148;
     int device = 0;
     SceneDev dev{};
+    size_t pix_capacity = 0;  // pixels the per-frame buffers hold
+    int integ_ctas_per_sm = 2;
     uint32_t integrated_frames = 0;
     Timing timing;
 };

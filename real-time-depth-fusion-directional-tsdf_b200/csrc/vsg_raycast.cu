@@ -1,21 +1,28 @@
 // vsg_raycast.cu -- ray caster (RayCastRender.cu:14-620 restated).
 //
-// One thread per pixel, warps on 8x4 pixel tiles.  The march replays the
-// reference's fixed half-voxel FP32 step sequence exactly (rayCurrent +=
-// 0.5 v, RayCastRender.cu:389-392) so hits, depths and colours match the
-// reference bit for bit, but skips the work of samples that cannot be valid:
-//   - block-cell DDA over the dilated occupancy grid: inside a cell whose
-//     3x3x3 block neighbourhood holds no allocated block, every trilinear tap
-//     of every sample misses, so the samples are invalid; only the FP32 step
-//     additions are replayed;
-//   - inside occupied cells, a tap in a block whose raw occupancy bit is
-//     clear is a miss without a hash probe; the last probed block is cached.
+// One thread per pixel, warps on 8x4 pixel tiles.  The march visits the
+// reference's FP32 sample sequence exactly (rayCurrent += 0.5 v,
+// RayCastRender.cu:389-392) so hits, depths and colours match the reference
+// bit for bit, but only evaluates samples that can be valid:
+// a sample's 8 taps lie in voxels floor(p/v)-1 .. floor(p/v)+2 per axis
+// (RayCastRender.cu:17-25, 127-170, with a voxel of slack for rounding), so
+// it can only be valid if a weighted voxel lies within one 2x2x2 sub-cube of
+// the sample's sub-cube.  The dwm grid holds that bit per sub-cube (one
+// 64-bit word per block position), the sup grid one bit per 8^3 block
+// positions.  Cells whose bit is clear are skipped whole:
+//   64-voxel cells (sup bit clear), 8-voxel cells (dwm word zero),
+//   2-voxel cells (dwm bit clear).
+// Skipped runs are replayed in O(1) by vsg_chain_advance, which lands on the
+// exact float the serial additions produce.  Surviving samples take the full
+// trilinear interpolation (8 taps, blocks resolved through the dense block
+// index, cached across samples).
 #include <cuda_runtime.h>
 
 #include <cstring>
 
 #include "../../include/vsg.h"
 #include "vsg_device.cuh"
+#include "vsg_fpchain.h"
 #include "vsg_internal.h"
 
 namespace vsg {
@@ -35,9 +42,20 @@ struct RenderArgs {
     float4* nrm;
 };
 
+// Pool indices of the blocks holding a sample's 8 trilinear taps.  The taps
+// of one sample span at most two blocks per axis (tap voxels x0 <= x1 <=
+// x0 + 2); tp[i] is the block of tap i.  Consecutive samples mostly reuse
+// the same blocks, so the entry is kept across samples.
 struct TapCache {
-    unsigned long long key;
-    int ptr;
+    int bx, by, bz, span;
+    int t0, t1, t2, t3, t4, t5, t6, t7;
+    __device__ __forceinline__ int get(int i) const {
+        return i == 0 ? t0 : i == 1 ? t1 : i == 2 ? t2 : i == 3 ? t3 : i == 4 ? t4 : i == 5 ? t5 : i == 6 ? t6 : t7;
+    }
+    __device__ __forceinline__ void set(int i, int v) {
+        if (i == 0) t0 = v; else if (i == 1) t1 = v; else if (i == 2) t2 = v; else if (i == 3) t3 = v;
+        else if (i == 4) t4 = v; else if (i == 5) t5 = v; else if (i == 6) t6 = v; else t7 = v;
+    }
 };
 
 // worldToVirtualVoxelPos, RayCastRender.cu:17-25 (floorf variant)
@@ -53,31 +71,64 @@ __device__ __forceinline__ int vox_to_block(int v) {
 
 __device__ __forceinline__ int vox_local(int v) { return ((v % kBlock) + kBlock) % kBlock; }
 
-// getVoxel, RayCastRender.cu:55-121: returns false for a missing block.
-__device__ __forceinline__ bool fetch_voxel(const SceneDev& s, int vx, int vy, int vz, TapCache& tc,
-                                            Voxel& out) {
-    const int bx = vox_to_block(vx), by = vox_to_block(vy), bz = vox_to_block(vz);
-    if (!occ_test(s.occ_raw, bx, by, bz, s.occ_log2)) return false;
-    if (!coord_ok(bx, by, bz)) return false;
-    const unsigned long long key = pack_key(bx, by, bz);
-    if (key != tc.key) {
-        tc.key = key;
-        tc.ptr = lookup_block(s, key, bx, by, bz);
+// getVoxel's block search (RayCastRender.cu:55-121) for the taps' blocks;
+// -1 = block not allocated (the tap reads as weight 0).
+__device__ __forceinline__ void refill_taps(const SceneDev& s, TapCache& tc, int bx0, int by0, int bz0, int span) {
+    tc.bx = bx0;
+    tc.by = by0;
+    tc.bz = bz0;
+    tc.span = span;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int c = i & span;
+        if (c == i) {
+            const int bx = bx0 + (i & 1), by = by0 + ((i >> 1) & 1), bz = bz0 + ((i >> 2) & 1);
+            tc.set(i, block_ptr(s, bx, by, bz));
+        } else {
+            int p = tc.t0;
+#pragma unroll
+            for (int j = 1; j < i; ++j)
+                if (c == j) p = tc.get(j);
+            tc.set(i, p);
+        }
     }
-    if (tc.ptr < 0) return false;
-    const int li = vox_local(vx) + vox_local(vy) * kBlock + vox_local(vz) * kBlock * kBlock;
-    const uint2 u = __ldg(reinterpret_cast<const uint2*>(s.voxels + (size_t)tc.ptr * kVoxPerBlock + li));
-    out.sdf = __uint_as_float(u.x);
-    out.rgbw = u.y;
-    return true;
 }
 
 __device__ __forceinline__ float frac01(float v) { return v - floorf(v); }
 
+
+// Ray parameter interval inside the axis-aligned cell [c*S, (c+1)*S)^3.
+// Approximate arithmetic: callers keep a margin from both ends.
+struct RayInv {
+    float ox, oy, oz, ix, iy, iz;
+    bool hx, hy, hz;
+};
+
+__device__ __forceinline__ void cell_interval(const RayInv& R, int cx, int cy, int cz, float S, float& tlo,
+                                              float& thi) {
+    tlo = -3.4e38f;
+    thi = 3.4e38f;
+    if (R.hx) {
+        const float t0 = ((float)cx * S - R.ox) * R.ix, t1 = ((float)(cx + 1) * S - R.ox) * R.ix;
+        tlo = fmaxf(tlo, fminf(t0, t1));
+        thi = fminf(thi, fmaxf(t0, t1));
+    }
+    if (R.hy) {
+        const float t0 = ((float)cy * S - R.oy) * R.iy, t1 = ((float)(cy + 1) * S - R.oy) * R.iy;
+        tlo = fmaxf(tlo, fminf(t0, t1));
+        thi = fminf(thi, fmaxf(t0, t1));
+    }
+    if (R.hz) {
+        const float t0 = ((float)cz * S - R.oz) * R.iz, t1 = ((float)(cz + 1) * S - R.oz) * R.iz;
+        tlo = fmaxf(tlo, fminf(t0, t1));
+        thi = fminf(thi, fmaxf(t0, t1));
+    }
+}
+
 // trilinearInterpolationSimpleFastFast, RayCastRender.cu:127-215.  The
 // colour is only accumulated when asked for (it never steers the march).
-__device__ __forceinline__ bool trilinear(const SceneDev& s, float px, float py, float pz, float& dist, bool want_color,
-                          uint32_t& rgb, TapCache& tc) {
+__device__ __forceinline__ bool trilinear(const SceneDev& s, float px, float py, float pz, float& dist,
+                                          bool want_color, uint32_t& rgb, TapCache& tc) {
     const float off = s.voxel;
     const float v = s.voxel;
     const float dx = px - off / 2.0f, dy = py - off / 2.0f, dz = pz - off / 2.0f;
@@ -85,18 +136,31 @@ __device__ __forceinline__ bool trilinear(const SceneDev& s, float px, float py,
     const float wx = frac01(fx), wy = frac01(fy), wz = frac01(fz);
     const int ax0 = tap_voxel(fx), ay0 = tap_voxel(fy), az0 = tap_voxel(fz);
     const int ax1 = tap_voxel((dx + off) / v), ay1 = tap_voxel((dy + off) / v), az1 = tap_voxel((dz + off) / v);
+    const int bx0 = vox_to_block(ax0), by0 = vox_to_block(ay0), bz0 = vox_to_block(az0);
+    const int span = (vox_to_block(ax1) != bx0 ? 1 : 0) | (vox_to_block(ay1) != by0 ? 2 : 0) |
+                     (vox_to_block(az1) != bz0 ? 4 : 0);
+    if (!(tc.bx == bx0 && tc.by == by0 && tc.bz == bz0 && tc.span == span)) refill_taps(s, tc, bx0, by0, bz0, span);
+    const int lx0 = vox_local(ax0), ly0 = vox_local(ay0) * kBlock, lz0 = vox_local(az0) * kBlock * kBlock;
+    const int lx1 = vox_local(ax1), ly1 = vox_local(ay1) * kBlock, lz1 = vox_local(az1) * kBlock * kBlock;
+    uint2 raw[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        raw[i] = make_uint2(0u, 0u);
+        if (tc.get(i) >= 0) {
+            const int li = ((i & 1) ? lx1 : lx0) + ((i & 2) ? ly1 : ly0) + ((i & 4) ? lz1 : lz0);
+            raw[i] = __ldg(reinterpret_cast<const uint2*>(s.voxels + (size_t)tc.get(i) * kVoxPerBlock + li));
+        }
+    }
     float d = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f, vws = 0.0f;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        Voxel vx;
-        if (!fetch_voxel(s, (i & 1) ? ax1 : ax0, (i & 2) ? ay1 : ay0, (i & 4) ? az1 : az0, tc, vx)) continue;
-        if ((vx.rgbw >> 24) == 0u) continue;
+        if ((raw[i].y >> 24) == 0u) continue;
         const float w = ((i & 1) ? wx : (1.0f - wx)) * ((i & 2) ? wy : (1.0f - wy)) * ((i & 4) ? wz : (1.0f - wz));
-        d += w * vx.sdf;
+        d += w * __uint_as_float(raw[i].x);
         if (want_color) {
-            cr += w * (float)(vx.rgbw & 0xFFu);
-            cg += w * (float)((vx.rgbw >> 8) & 0xFFu);
-            cb += w * (float)((vx.rgbw >> 16) & 0xFFu);
+            cr += w * (float)(raw[i].y & 0xFFu);
+            cg += w * (float)((raw[i].y >> 8) & 0xFFu);
+            cb += w * (float)((raw[i].y >> 16) & 0xFFu);
         }
         vws += w;
     }
@@ -112,28 +176,7 @@ __device__ __forceinline__ bool trilinear(const SceneDev& s, float px, float py,
     return true;
 }
 
-// findIntersectionBisection, RayCastRender.cu:229-271.
-__device__ __forceinline__ bool bisection(const SceneDev& s, float ox, float oy, float oz, float wx, float wy, float wz, float d0,
-                          float r0, float d1, float r1, float& alpha, uint32_t& rgb, TapCache& tc) {
-    float a = r0, ad = d0, b = r1, bd = d1, c = 0.0f;
-#pragma unroll 1
-    for (int i = 0; i < 3; ++i) {
-        c = a + (ad / (ad - bd)) * (b - a);
-        float cd;
-        if (!trilinear(s, ox + c * wx, oy + c * wy, oz + c * wz, cd, true, rgb, tc)) return false;
-        if (ad * cd > 0.0f) {
-            a = c;
-            ad = cd;
-        } else {
-            b = c;
-            bd = cd;
-        }
-    }
-    alpha = c;
-    return true;
-}
-
-__global__ void __launch_bounds__(128) k_render(RenderArgs a) {
+__global__ void __launch_bounds__(128, 1) k_render(RenderArgs a) {
     const SceneDev& s = a.s;
     // numActiveBlocks == 0 leaves the outputs untouched (RayCastRender.cu:552-555)
     if (*(volatile int*)&s.ctr->free_count >= s.num_blocks) return;
@@ -181,86 +224,155 @@ __global__ void __launch_bounds__(128) k_render(RenderArgs a) {
         const float d2r = 1.0f / cdz;
         float rc = d2r * fmaxf(minD, minD);
         const float re = d2r * fminf(maxD, maxD);
-        const float h = v * 0.5f;
-        const float C = (float)kBlock * v;
-        const float invC = 1.0f / C;
-        const bool hx = fabsf(wdx) > 1e-12f, hy = fabsf(wdy) > 1e-12f, hz = fabsf(wdz) > 1e-12f;
-        const float ix = hx ? 1.0f / wdx : 0.0f, iy = hy ? 1.0f / wdy : 0.0f, iz = hz ? 1.0f / wdz : 0.0f;
-        TapCache tc{kKeyEmpty, -1};
-        int guard = 0;
+        const float C = (float)kBlock * v, C2 = 2.0f * v, C8 = 64.0f * v;
+        const float invC2 = 1.0f / C2;
+        RayInv R;
+        R.ox = ox;
+        R.oy = oy;
+        R.oz = oz;
+        R.hx = fabsf(wdx) > 1e-12f;
+        R.hy = fabsf(wdy) > 1e-12f;
+        R.hz = fabsf(wdz) > 1e-12f;
+        R.ix = R.hx ? 1.0f / wdx : 0.0f;
+        R.iy = R.hy ? 1.0f / wdy : 0.0f;
+        R.iz = R.hz ? 1.0f / wdz : 0.0f;
+        TapCache tc;
+        tc.bx = 0x7FFFFFFF;
+        tc.by = tc.bz = tc.span = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) tc.set(i, -1);
+        int steps = 0;  // FP32 chain additions so far (iteration guard)
+        uint32_t n_full = 0u, n_skip = 0u, n_jump = 0u, n_single = 0u;
+        const float m = 1e-4f;  // keep skipped samples this far inside their cell
+        // one loop for the march and the regula-falsi steps, so a single
+        // trilinear evaluation site serves both (mode 0 = march, 1..3 =
+        // step k of findIntersectionBisection, RayCastRender.cu:229-271)
+        int mode = 0;
+        float ba = 0.0f, bad = 0.0f, bb = 0.0f, bbd = 0.0f, bc = 0.0f, mdist = 0.0f;
+        uint32_t rgb = 0u;
 #pragma unroll 1
-        while (rc < re) {
-            if (++guard > kMaxMarch) {
-                atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_MARCH_LIMIT);
-                break;
-            }
-            const float spx = ox + rc * wdx, spy = oy + rc * wdy, spz = oz + rc * wdz;
-            const int cx = __float2int_rd(spx * invC), cy = __float2int_rd(spy * invC),
-                      cz = __float2int_rd(spz * invC);
-            if (!occ_test(s.occ_dil, cx, cy, cz, s.occ_log2)) {
-                // parameter interval of the ray inside cell (cx,cy,cz)
-                float tlo = -3.4e38f, thi = 3.4e38f;
-                if (hx) {
-                    const float t0 = ((float)cx * C - ox) * ix, t1 = ((float)(cx + 1) * C - ox) * ix;
-                    tlo = fmaxf(tlo, fminf(t0, t1));
-                    thi = fminf(thi, fmaxf(t0, t1));
+        while (true) {
+            float st;  // ray parameter of the sample to evaluate
+            if (mode == 0) {
+                if (!(rc < re)) break;
+                if (steps >= kMaxMarch) {
+                    atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_MARCH_LIMIT);
+                    break;
                 }
-                if (hy) {
-                    const float t0 = ((float)cy * C - oy) * iy, t1 = ((float)(cy + 1) * C - oy) * iy;
-                    tlo = fmaxf(tlo, fminf(t0, t1));
-                    thi = fminf(thi, fmaxf(t0, t1));
-                }
-                if (hz) {
-                    const float t0 = ((float)cz * C - oz) * iz, t1 = ((float)(cz + 1) * C - oz) * iz;
-                    tlo = fmaxf(tlo, fminf(t0, t1));
-                    thi = fminf(thi, fmaxf(t0, t1));
-                }
-                const float m = 1e-5f;
-                const float tstop = fminf(thi - m, re);
-                if (rc > tlo + m && rc < tstop) {
-                    lastValid = false;
-                    int n = 0;
-#pragma unroll 1
-                    do {
-                        rc += h;
-                    } while (rc < tstop && ++n < kMaxMarch);
-                    continue;
-                }
-            }
-            float dist;
-            uint32_t rgb_unused = 0;
-            if (trilinear(s, spx, spy, spz, dist, false, rgb_unused, tc)) {
-                if (lastValid && lastSdf < 0.0f && dist > 0.0f) {
-                    float alpha = 0.0f;
-                    uint32_t rgb = 0;
-                    const bool b = bisection(s, ox, oy, oz, wdx, wdy, wdz, lastSdf, lastAlpha, dist, rc, alpha, rgb, tc);
-                    const float isx = ox + alpha * wdx, isy = oy + alpha * wdy, isz = oz + alpha * wdz;
-                    const float th = v * 3;
-                    if (b && fabsf(lastSdf - dist) < th) {
-                        if (fabsf(dist) < th) {
-                            out_depth = alpha / d2r;
-                            out_pos = make_float4(isx, isy, isz, 1.0f);
-                            out_col = make_float4((float)(rgb & 0xFFu) / 255.0f, (float)((rgb >> 8) & 0xFFu) / 255.0f,
-                                                  (float)((rgb >> 16) & 0xFFu) / 255.0f, 1.0f);
-                            hit = true;
-                            break;
-                        }
+                const float spx = ox + rc * wdx, spy = oy + rc * wdy, spz = oz + rc * wdz;
+                // global sub-cube (2 voxels) of the sample, its block cell and super-cell
+                const int qx = __float2int_rd(spx * invC2), qy = __float2int_rd(spy * invC2),
+                          qz = __float2int_rd(spz * invC2);
+                float tlo = 0.0f, thi = 0.0f;
+                bool cell = false;
+                const int k = s.bidx_log2;
+                const uint32_t sb = grid_bit(qx >> 5, qy >> 5, qz >> 5, k - 3);
+                if (!((__ldg(s.sup + (sb >> 5)) >> (sb & 31)) & 1u)) {
+                    cell_interval(R, qx >> 5, qy >> 5, qz >> 5, C8, tlo, thi);  // 64-voxel cell
+                    cell = true;
+                } else {
+                    const unsigned long long w = __ldg(s.dwm + bidx_cell(qx >> 2, qy >> 2, qz >> 2, k));
+                    if (w == 0ull) {
+                        cell_interval(R, qx >> 2, qy >> 2, qz >> 2, C, tlo, thi);  // 8-voxel cell
+                        cell = true;
+                    } else if (!((w >> ((((qz & 3) << 2) | (qy & 3)) << 2 | (qx & 3))) & 1ull)) {
+                        cell_interval(R, qx, qy, qz, C2, tlo, thi);  // 2-voxel cell
+                        cell = true;
                     }
                 }
-                lastSdf = dist;
-                lastAlpha = rc;
-                lastValid = true;
-                rc += v * 0.5f;
+                if (cell) {
+                    if (rc > tlo + m && rc < thi - m) {
+                        const int before = steps;
+                        rc = vsg_chain_advance(rc, v * 0.5f, fminf(thi - m, re), kMaxMarch - steps, &steps);
+                        n_skip += (uint32_t)(steps - before);
+                        ++n_jump;
+                        lastValid = false;
+                        continue;
+                    }
+                    ++n_single;  // too close to the cell boundary to trust the test
+                }
+                st = rc;
             } else {
-                lastValid = false;
+                st = bc;
+            }
+            float dist = 0.0f;
+            ++n_full;
+            const bool ok = trilinear(s, ox + st * wdx, oy + st * wdy, oz + st * wdz, dist, mode != 0, rgb, tc);
+            if (mode == 0) {
+                if (ok && lastValid && lastSdf < 0.0f && dist > 0.0f) {
+                    // zero crossing: a = last sample, b = this one
+                    ba = lastAlpha;
+                    bad = lastSdf;
+                    bb = rc;
+                    bbd = dist;
+                    mdist = dist;
+                    bc = ba + (bad / (bad - bbd)) * (bb - ba);  // findIntersectionLinear
+                    mode = 1;
+                    continue;
+                }
+                if (ok) {
+                    lastSdf = dist;
+                    lastAlpha = rc;
+                }
+                lastValid = ok;
                 rc += v * 0.5f;
+                ++steps;
+            } else {
+                bool finished = !ok, success = false;
+                if (ok) {
+                    if (bad * dist > 0.0f) {
+                        ba = bc;
+                        bad = dist;
+                    } else {
+                        bb = bc;
+                        bbd = dist;
+                    }
+                    if (mode == 3) {
+                        finished = true;
+                        success = true;
+                    } else {
+                        bc = ba + (bad / (bad - bbd)) * (bb - ba);
+                        ++mode;
+                    }
+                }
+                if (finished) {
+                    const float th = v * 3;
+                    if (success && fabsf(lastSdf - mdist) < th && fabsf(mdist) < th) {
+                        const float alpha = bc;
+                        out_depth = alpha / d2r;
+                        out_pos = make_float4(ox + alpha * wdx, oy + alpha * wdy, oz + alpha * wdz, 1.0f);
+                        out_col = make_float4((float)(rgb & 0xFFu) / 255.0f, (float)((rgb >> 8) & 0xFFu) / 255.0f,
+                                              (float)((rgb >> 16) & 0xFFu) / 255.0f, 1.0f);
+                        hit = true;
+                        break;
+                    }
+                    // not accepted: the march continues after the crossing sample
+                    lastSdf = mdist;
+                    lastAlpha = rc;
+                    lastValid = true;
+                    rc += v * 0.5f;
+                    ++steps;
+                    mode = 0;
+                }
             }
         }
-        const unsigned hm = __ballot_sync(__activemask(), hit);
         const unsigned am = __activemask();
+        const unsigned hm = __ballot_sync(am, hit);
+        uint32_t nf = n_full, ns = n_skip, nj = n_jump, n1 = n_single;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            nf += __shfl_xor_sync(am, nf, o);
+            ns += __shfl_xor_sync(am, ns, o);
+            nj += __shfl_xor_sync(am, nj, o);
+            n1 += __shfl_xor_sync(am, n1, o);
+        }
         if ((threadIdx.x & 31) == (__ffs(am) - 1)) {
             atomicAdd(&s.frame->hits, (uint32_t)__popc(hm));
             atomicAdd(&s.frame->misses, (uint32_t)(__popc(am) - __popc(hm)));
+            atomicAdd(&s.frame->samples_full, nf);
+            atomicAdd(&s.frame->samples_skipped, ns);
+            atomicAdd(&s.frame->jumps, nj);
+            atomicAdd(&s.frame->singles, n1);
         }
     }
     a.depth[pi] = out_depth;
@@ -272,6 +384,10 @@ __global__ void __launch_bounds__(128) k_render(RenderArgs a) {
 __global__ void k_render_begin(FrameCounters* f) {
     f->hits = 0u;
     f->misses = 0u;
+    f->samples_full = 0u;
+    f->samples_skipped = 0u;
+    f->jumps = 0u;
+    f->singles = 0u;
 }
 
 int render_launch(Renderer* r, Scene* sc, const float cam[3], const float* pose_dev, const float* pose_host,

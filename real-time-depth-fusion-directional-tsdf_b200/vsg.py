@@ -46,7 +46,8 @@ class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in (
         "allocated_blocks", "free_blocks", "high_water", "chain_nodes_used", "integrated_frames",
         "frame_valid_pixels", "frame_new_blocks", "frame_visible_blocks", "frame_updated_blocks",
-        "frame_updated_voxels", "render_hits", "render_misses", "flags")]
+        "frame_updated_voxels", "render_hits", "render_misses", "render_samples_full",
+        "render_samples_skipped", "render_jumps", "render_singles", "flags")]
 
     def as_dict(self) -> dict:
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
