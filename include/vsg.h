@@ -102,6 +102,9 @@ typedef struct vsg_stats {
     uint32_t render_jumps;           /* last render: O(1) jumps over skipped runs */
     uint32_t render_singles;         /* last render: samples rejected one at a time */
     uint32_t flags;              /* VSG_FLAG_* (sticky since reset) */
+    uint32_t fast_division;      /* 1: the ray caster divides by the voxel size with a
+                                    product + correction verified exhaustively against
+                                    IEEE division at scene creation */
 } vsg_stats;
 
 /* Reference defaults of the knobs used by the tests (README.md:79-83). */

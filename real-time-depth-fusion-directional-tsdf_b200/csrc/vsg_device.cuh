@@ -95,6 +95,7 @@ struct FrameCounters {
     uint32_t samples_skipped;  // march samples skipped as provably invalid
     uint32_t jumps;          // O(1) jumps over runs of skipped samples
     uint32_t singles;        // samples evaluated at a cell boundary (no jump)
+    uint32_t pad2[4];
 };
 
 struct SceneDev {
@@ -120,6 +121,8 @@ struct SceneDev {
     int max_nodes;
     int bidx_log2;  // k: toroidal block grid of 2^k positions per axis
     float voxel;
+    float inv_voxel;  // RN(1 / voxel)
+    bool div_fast;    // fixed-divisor division verified for this voxel size
 };
 
 struct Pose {

@@ -695,6 +695,10 @@ int scene_alloc_device(Scene* sc) {
     d.max_nodes = (int)M;
     d.bidx_log2 = sc->bidx_log2;
     d.voxel = sc->params.voxel_size;
+    d.inv_voxel = 1.0f / d.voxel;
+    bool fast = false;
+    if (verify_fixed_division(d.voxel, &fast) != VSG_OK) fast = false;
+    d.div_fast = fast;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_integrate, 256, 0);
     sc->integ_ctas_per_sm = per_sm > 0 ? per_sm : 2;

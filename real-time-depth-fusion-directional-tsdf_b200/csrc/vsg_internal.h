@@ -51,6 +51,8 @@ int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H
 int render_launch(Renderer* r, Scene* sc, const float cam[3], const float* pose_dev, const float* pose_host,
                   float fx, float fy, float cx, float cy, float min_depth, float max_depth, cudaStream_t st);
 
+int verify_fixed_division(float v, bool* ok);
+
 void timing_begin(Scene* sc, int slot, cudaStream_t st);
 void timing_end(Scene* sc, int slot, cudaStream_t st);
 

@@ -64,12 +64,34 @@ __device__ __forceinline__ int tap_voxel(float q) {
     return __float2int_rz(floorf(q + 0.5f * sg));
 }
 
-__device__ __forceinline__ int vox_to_block(int v) {
-    if (v < 0) v = (int)((unsigned)v - 7u);  // RayCastRender.cu:28-33
-    return v / kBlock;
+// virtualVoxelPosToSDFBlock (RayCastRender.cu:28-33): (v < 0 ? v - 7 : v) / 8
+// in C division is floor(v / 8), an arithmetic shift
+__device__ __forceinline__ int vox_to_block(int v) { return v >> 3; }
+
+// virtualVoxelPosToLocal (RayCastRender.cu:36-42): ((v % 8) + 8) % 8 == v & 7
+__device__ __forceinline__ int vox_local(int v) { return v & 7; }
+
+// Correctly rounded x / v for the fixed divisor v, given y = RN(1/v): one
+// Markstein correction of the product x*y (P. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990): r = x - q v is exact and q + r y rounds to x / v.
+// Used only for 2^-100 <= |x| < kDivRange, and only when k_verify_div found
+// it equal to IEEE division for every float of that range with this v
+// (checked at scene creation); near zero the product underflows and the
+// correction is not exact, so those x use IEEE division.
+constexpr float kDivRange = 1024.0f;
+constexpr float kDivTiny = 0x1p-100f;
+__device__ __forceinline__ float div_fixed(float x, float v, float y) {
+    const float q = __fmul_rn(x, y);
+    const float r = __fmaf_rn(-q, v, x);
+    return __fmaf_rn(r, y, q);
 }
 
-__device__ __forceinline__ int vox_local(int v) { return ((v % kBlock) + kBlock) % kBlock; }
+__device__ __forceinline__ float div_v(float x, float v, float y, bool fast) {
+    const float ax = fabsf(x);
+    if (fast && ax >= kDivTiny && ax < kDivRange) return div_fixed(x, v, y);
+    return x / v;
+}
 
 // getVoxel's block search (RayCastRender.cu:55-121) for the taps' blocks;
 // -1 = block not allocated (the tap reads as weight 0).
@@ -132,10 +154,13 @@ __device__ __forceinline__ bool trilinear(const SceneDev& s, float px, float py,
     const float off = s.voxel;
     const float v = s.voxel;
     const float dx = px - off / 2.0f, dy = py - off / 2.0f, dz = pz - off / 2.0f;
-    const float fx = dx / v, fy = dy / v, fz = dz / v;
+    const bool fast = s.div_fast;
+    const float y = s.inv_voxel;
+    const float fx = div_v(dx, v, y, fast), fy = div_v(dy, v, y, fast), fz = div_v(dz, v, y, fast);
     const float wx = frac01(fx), wy = frac01(fy), wz = frac01(fz);
     const int ax0 = tap_voxel(fx), ay0 = tap_voxel(fy), az0 = tap_voxel(fz);
-    const int ax1 = tap_voxel((dx + off) / v), ay1 = tap_voxel((dy + off) / v), az1 = tap_voxel((dz + off) / v);
+    const int ax1 = tap_voxel(div_v(dx + off, v, y, fast)), ay1 = tap_voxel(div_v(dy + off, v, y, fast)),
+              az1 = tap_voxel(div_v(dz + off, v, y, fast));
     const int bx0 = vox_to_block(ax0), by0 = vox_to_block(ay0), bz0 = vox_to_block(az0);
     const int span = (vox_to_block(ax1) != bx0 ? 1 : 0) | (vox_to_block(ay1) != by0 ? 2 : 0) |
                      (vox_to_block(az1) != bz0 ? 4 : 0);
@@ -176,7 +201,8 @@ __device__ __forceinline__ bool trilinear(const SceneDev& s, float px, float py,
     return true;
 }
 
-__global__ void __launch_bounds__(128, 1) k_render(RenderArgs a) {
+// One thread per pixel; a warp covers an 8x4 pixel tile.
+__global__ void __launch_bounds__(128, 6) k_render(RenderArgs a) {
     const SceneDev& s = a.s;
     // numActiveBlocks == 0 leaves the outputs untouched (RayCastRender.cu:552-555)
     if (*(volatile int*)&s.ctr->free_count >= s.num_blocks) return;
@@ -336,7 +362,7 @@ __global__ void __launch_bounds__(128, 1) k_render(RenderArgs a) {
                     }
                 }
                 if (finished) {
-                    const float th = v * 3;
+                    const float th = v * 3;  // RayCastRender.cu:362-365
                     if (success && fabsf(lastSdf - mdist) < th && fabsf(mdist) < th) {
                         const float alpha = bc;
                         out_depth = alpha / d2r;
@@ -379,6 +405,39 @@ __global__ void __launch_bounds__(128, 1) k_render(RenderArgs a) {
     a.pos[pi] = out_pos;
     a.col[pi] = out_col;
     a.nrm[pi] = make_float4(kMinf, kMinf, kMinf, kMinf);
+}
+
+// Exhaustive check of div_fixed against IEEE division for this voxel size:
+// every float x with kDivTiny <= |x| < kDivRange, both signs.  One thread
+// per bit pattern of |x|.
+__global__ void k_verify_div(float v, float y, unsigned int* mismatches) {
+    const uint32_t first = __float_as_uint(kDivTiny), limit = __float_as_uint(kDivRange);
+    for (uint32_t u = first + blockIdx.x * blockDim.x + threadIdx.x; u < limit; u += gridDim.x * blockDim.x) {
+        const float x = __uint_as_float(u);
+        const float a = x / v, b = div_fixed(x, v, y);
+        const float c = (-x) / v, d = div_fixed(-x, v, y);
+        if (__float_as_uint(a) != __float_as_uint(b) || __float_as_uint(c) != __float_as_uint(d))
+            atomicAdd(mismatches, 1u);
+    }
+}
+
+int verify_fixed_division(float v, bool* ok) {
+    *ok = false;
+    unsigned int* d = nullptr;
+    if (cudaMalloc(&d, sizeof(unsigned int)) != cudaSuccess) return VSG_ERR_OUT_OF_MEMORY;
+    cudaMemset(d, 0, sizeof(unsigned int));
+    const float y = 1.0f / v;
+    int sms = 148;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    k_verify_div<<<sms * 8, 256>>>(v, y, d);
+    unsigned int h = 1u;
+    const cudaError_t e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return VSG_ERR_CUDA;
+    *ok = h == 0u;
+    return VSG_OK;
 }
 
 __global__ void k_render_begin(FrameCounters* f) {

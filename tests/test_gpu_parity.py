@@ -79,6 +79,8 @@ def test_tabletop_small(cuda, oracle_mod, synth_mod, wh, frames):
     # the kernels restate the reference bit for bit
     assert all(r["volume"]["bit_exact"] for r in reports if "volume" in r)
     assert all(r["render"]["bit_exact_all"] for r in reports if "render" in r)
+    # the fixed-divisor division passed its exhaustive check for 4 mm
+    assert reports[-1]["stats"]["fast_division"] == 1
 
 
 def test_tabletop_full_size(cuda, oracle_mod, synth_mod):
