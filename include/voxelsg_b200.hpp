@@ -1,0 +1,280 @@
+/*
+ * voxelsg_b200.hpp -- header-only C++ drop-in for VoxelSG's fusion API over
+ * the C ABI of libvsg.so (vsg.h).
+ *
+ * Keeps the reference names, signatures and error behaviour of
+ *   GlobalParamsConfig   (globalPramasConfig.h:55-187; defaults
+ *                         globalParamasConfig.cpp:8-402; validation :413-417)
+ *   Params               (CUDAHashData.h:9-42, including its swap of the two
+ *                         truncation fields, CUDAHashData.h:27-28)
+ *   VoxelScene           (VoxelScene.h:51-209): constructor, reset,
+ *                         integrateFromScanData, getNumIntegratedFrames,
+ *                         isAllocated, getParams, getHeapFreeCount
+ *   RayCastRender        (RayCastRender.h:20-124): initialize, render,
+ *                         downloadResults, downloadDepthFloat,
+ *                         getOutputDepth/Color/Normal/Positions
+ * so that reference call sites compile unchanged against it.  Like the
+ * reference, the methods print to stderr and return on bad input instead of
+ * throwing; the only throw is GlobalParamsConfig::initialize.
+ *
+ * cv::Mat is not required: integrateFromScanData accepts any 4x4 matrix type
+ * with at<float>(row, col) (cv::Mat, or vsg::Mat4f below).
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+#include <vector_types.h>
+
+#include <cstdint>
+#include <iostream>
+#include <stdexcept>
+#include <vector>
+
+#include "vsg.h"
+
+#ifndef SDF_BLOCK_SIZE
+#define SDF_BLOCK_SIZE 8
+#endif
+#ifndef HASH_BUCKET_SIZE
+#define HASH_BUCKET_SIZE 10
+#endif
+
+namespace vsg {
+
+/* Row-major 4x4 float matrix with the cv::Mat accessor the API uses. */
+struct Mat4f {
+    float m[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+    template <class T>
+    T& at(int r, int c) {
+        return m[r * 4 + c];
+    }
+    template <class T>
+    const T& at(int r, int c) const {
+        return m[r * 4 + c];
+    }
+};
+
+}  // namespace vsg
+
+/* The knobs the fusion path reads, with the reference's code defaults. */
+class GlobalParamsConfig {
+public:
+    float g_SDFVoxelSize = 0.1f;          /* globalParamasConfig.cpp:28 */
+    float g_SDFTruncation = 0.25f;        /* :38 */
+    float g_SDFTruncationScale = 0.01f;   /* :44 */
+    float g_SDFMaxIntegrationDistance = 3.0f;
+    unsigned int g_SDFIntegrationWeightMax = 255;
+    unsigned int g_hashNumSlots = 10000;  /* :61 */
+    unsigned int g_hashNumSDFBlocks = 10000; /* :65 */
+    unsigned int g_hashSlotSize = HASH_BUCKET_SIZE;
+    unsigned int g_hashNumBuckets = 10000; /* = g_hashNumSlots, :74 */
+    float g_SDFRayIncrementFactor = 0.8f;
+    unsigned int g_marchingCubesMaxNumTriangles = 250000; /* :379 */
+    float g_streamingRadius = 4.0f;       /* :136 */
+    bool g_streamingEnabled = false;
+
+    static GlobalParamsConfig& getInstance() {
+        static GlobalParamsConfig s;
+        return s;
+    }
+    static GlobalParamsConfig& get() { return getInstance(); }
+
+    void initialize() {
+        validateParameters();
+        m_bIsInitialized = true;
+    }
+    bool isInitialized() const { return m_bIsInitialized; }
+    void validateParameters() const {
+        if (g_hashNumBuckets == 0) throw std::invalid_argument("Invalid hash buckets");
+        if (g_SDFVoxelSize <= 0.0f) throw std::invalid_argument("Invalid voxel size");
+    }
+
+private:
+    bool m_bIsInitialized = false;
+};
+
+/* Params derived from the knobs (CUDAHashData.h:14-29). */
+struct Params {
+    Params() = default;
+    explicit Params(const GlobalParamsConfig& gpc) {
+        SDFBlockNum = (int)gpc.g_hashNumSDFBlocks;
+        hashSlotNum = (int)gpc.g_hashNumSlots;
+        SDFBlockSize = SDF_BLOCK_SIZE;
+        slotSize = HASH_BUCKET_SIZE;
+        totalHashSize = (int)gpc.g_hashNumSlots * HASH_BUCKET_SIZE;
+        totalBlockSize = (int)gpc.g_hashNumSDFBlocks * SDF_BLOCK_SIZE * SDF_BLOCK_SIZE * SDF_BLOCK_SIZE;
+        voxelSize = gpc.g_SDFVoxelSize;
+        truncationScale = gpc.g_SDFTruncation;   /* the reference swaps these two */
+        truncation = gpc.g_SDFTruncationScale;
+    }
+    int hashSlotNum = 0;
+    int SDFBlockNum = 0;
+    int SDFBlockSize = SDF_BLOCK_SIZE;
+    int totalHashSize = 0;
+    int slotSize = HASH_BUCKET_SIZE;
+    int totalBlockSize = 0;
+    float voxelSize = 0.0f;
+    float truncationScale = 0.0f;
+    float truncation = 0.0f;
+};
+
+class VoxelScene {
+public:
+    explicit VoxelScene(const Params& params) : m_params(params) {
+        vsg_params p;
+        vsg_params_default(&p);
+        p.voxel_size = params.voxelSize;
+        p.truncation = params.truncationScale;
+        p.truncation_scale = params.truncation;
+        p.hash_num_slots = (uint32_t)params.hashSlotNum;
+        p.num_sdf_blocks = (uint32_t)params.SDFBlockNum;
+        const int rc = vsg_scene_create(&p, &m_scene);
+        if (rc != VSG_OK) {
+            std::cerr << "VoxelScene: allocation failed (status " << rc << ")" << std::endl;
+            m_scene = nullptr;
+        }
+    }
+    ~VoxelScene() {
+        if (m_scene) vsg_scene_destroy(m_scene);
+    }
+    VoxelScene(const VoxelScene&) = delete;
+    VoxelScene& operator=(const VoxelScene&) = delete;
+
+    void reset() {
+        if (!m_scene) {
+            std::cerr << "VoxelScene: Not allocated yet!" << std::endl;
+            return;
+        }
+        vsg_scene_reset(m_scene, nullptr);
+        cudaDeviceSynchronize();
+    }
+
+    /* VoxelScene.h:89-91.  depthmap / colormap / normalmap are device maps;
+     * cameraTransform is a host 4x4 camera->world matrix. */
+    template <class Matrix>
+    void integrateFromScanData(const float3* depthmap, const uchar3* colormap, const float3* normalmap, int width,
+                               int height, float truncationDistance, const Matrix& cameraTransform, float fx,
+                               float fy, float cx, float cy) {
+        if (depthmap == nullptr || colormap == nullptr || normalmap == nullptr) {
+            std::cerr << "VoxelScene: Invalid pointers (nullptr)!" << std::endl;
+            return;
+        }
+        if (!m_scene) {
+            std::cerr << "VoxelScene: Not allocated!" << std::endl;
+            return;
+        }
+        float T[16];
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) T[i * 4 + j] = cameraTransform.template at<float>(i, j);
+        const int rc = vsg_integrate(m_scene, reinterpret_cast<const float*>(depthmap),
+                                     reinterpret_cast<const uint8_t*>(colormap),
+                                     reinterpret_cast<const float*>(normalmap), width, height, truncationDistance,
+                                     T, fx, fy, cx, cy, nullptr);
+        if (rc != VSG_OK) std::cerr << "VoxelScene: integration failed (status " << rc << ")" << std::endl;
+    }
+
+    unsigned int getNumIntegratedFrames() const {
+        vsg_stats st{};
+        if (!m_scene || vsg_scene_stats(m_scene, &st) != VSG_OK) return 0;
+        return st.integrated_frames;
+    }
+    /* VoxelScene.cpp:348-354: heap counter + 1 = free blocks */
+    unsigned int getHeapFreeCount() const {
+        vsg_stats st{};
+        if (!m_scene || vsg_scene_stats(m_scene, &st) != VSG_OK) return 0;
+        return st.free_blocks;
+    }
+    bool isAllocated() const { return m_scene != nullptr; }
+    Params& getParams() { return m_params; }
+    const Params& getParams() const { return m_params; }
+    vsg_scene* handle() const { return m_scene; }
+
+private:
+    Params m_params;
+    vsg_scene* m_scene = nullptr;
+};
+
+class RayCastRender {
+public:
+    RayCastRender() = default;
+    ~RayCastRender() {
+        if (m_r) vsg_renderer_destroy(m_r);
+    }
+    RayCastRender(const RayCastRender&) = delete;
+    RayCastRender& operator=(const RayCastRender&) = delete;
+
+    bool initialize(int width, int height) {
+        if (m_r) {
+            std::cerr << "RayCastRender: Already initialized!" << std::endl;
+            return false;
+        }
+        if (vsg_renderer_create(width, height, &m_r) != VSG_OK) {
+            std::cerr << "RayCastRender: Failed to allocate GPU memory!" << std::endl;
+            m_r = nullptr;
+            return false;
+        }
+        m_width = width;
+        m_height = height;
+        return true;
+    }
+
+    /* RayCastRender.h:66-70: cameraTransform is a DEVICE float[16]
+     * (row-major camera->world); cameraPos is the ray origin. */
+    void render(const VoxelScene* voxelScene, float3 cameraPos, float* cameraTransform, float fx, float fy, float cx,
+                float cy, float minDepth, float maxDepth) {
+        if (!m_r) {
+            std::cerr << "RayCastRender: Not initialized!" << std::endl;
+            return;
+        }
+        if (!voxelScene || !voxelScene->isAllocated()) {
+            std::cerr << "RayCastRender: Invalid voxel scene!" << std::endl;
+            return;
+        }
+        const float cam[3] = {cameraPos.x, cameraPos.y, cameraPos.z};
+        const int rc = vsg_render(m_r, voxelScene->handle(), cam, cameraTransform, fx, fy, cx, cy, minDepth,
+                                  maxDepth, nullptr);
+        if (rc != VSG_OK) std::cerr << "RayCastRender: render failed (status " << rc << ")" << std::endl;
+        cudaDeviceSynchronize();
+    }
+
+    /* RayCastRender.cpp:188-212: depth expanded to (d, d, d, 1) */
+    void downloadResults(float4* h_outputDepth, float4* h_outputColor, float4* h_outputNormal) {
+        if (!m_r) {
+            std::cerr << "RayCastRender: Not initialized!" << std::endl;
+            return;
+        }
+        const size_t n = (size_t)m_width * m_height;
+        std::vector<float> d(n);
+        if (vsg_renderer_download(m_r, d.data(), nullptr, reinterpret_cast<float*>(h_outputColor),
+                                  reinterpret_cast<float*>(h_outputNormal)) != VSG_OK) {
+            std::cerr << "RayCastRender: Failed to download results!" << std::endl;
+            return;
+        }
+        for (size_t i = 0; i < n; ++i) h_outputDepth[i] = make_float4(d[i], d[i], d[i], 1.0f);
+    }
+
+    void downloadDepthFloat(float* h_outputDepthFloat) {
+        if (!m_r || h_outputDepthFloat == nullptr) return;
+        vsg_renderer_download(m_r, h_outputDepthFloat, nullptr, nullptr, nullptr);
+    }
+
+    /* the depth buffer holds floats although typed float4*, as in the
+     * reference (RayCastRender.cpp:98, 151) */
+    float4* getOutputDepth() const { return ptr(0); }
+    float4* getOutputColor() const { return ptr(2); }
+    float4* getOutputNormal() const { return ptr(3); }
+    float4* getOutputPositions() const { return ptr(1); }
+    int getWidth() const { return m_width; }
+    int getHeight() const { return m_height; }
+    bool isAllocated() const { return m_r != nullptr; }
+
+private:
+    float4* ptr(int which) const {
+        if (!m_r) return nullptr;
+        float* p[4] = {nullptr, nullptr, nullptr, nullptr};
+        vsg_renderer_outputs(m_r, &p[0], &p[1], &p[2], &p[3]);
+        return reinterpret_cast<float4*>(p[which]);
+    }
+    vsg_renderer* m_r = nullptr;
+    int m_width = 0, m_height = 0;
+};

@@ -1,0 +1,47 @@
+"""The C++ drop-in classes (include/voxelsg_b200.hpp) driven like the
+reference's main loop give the same depths as the Python binding of the C
+ABI (needs a GPU; compiles the harness with g++)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "real-time-depth-fusion-directional-tsdf_b200")
+CUDA = "/usr/local/cuda"
+
+
+def test_cpp_dropin_matches_binding(cuda, synth_mod, tmp_path):
+    import vsg
+
+    W, H, N = 160, 120, 3
+    fr, K = synth_mod.tabletop_stream(2, N, W, H)
+    d = str(tmp_path)
+    for i, f in enumerate(fr):
+        f.pointmap.astype(np.float32).tofile(os.path.join(d, f"pm_{i}.bin"))
+        f.rgb.astype(np.uint8).tofile(os.path.join(d, f"rgb_{i}.bin"))
+        f.normals.astype(np.float32).tofile(os.path.join(d, f"nm_{i}.bin"))
+        f.pose.astype(np.float32).tofile(os.path.join(d, f"pose_{i}.bin"))
+    exe = os.path.join(d, "dropin_frames")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", exe, os.path.join(ROOT, "tests", "cpp", "dropin_frames.cpp"),
+                    "-I", os.path.join(ROOT, "include"), "-I", f"{CUDA}/include", "-L", PKG, "-lvsg",
+                    f"-Wl,-rpath,{PKG}", "-L", f"{CUDA}/lib64", "-lcudart"], check=True)
+    r = subprocess.run([exe, d, str(N), str(W), str(H), str(K.fx), str(K.fy), str(K.cx), str(K.cy), "0.004", "0.02",
+                        "20011", "40000", "0.2", "3.0"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert f"frames={N}" in r.stdout
+    sc = vsg.Scene(voxel_size=0.004, truncation=0.02, hash_num_slots=20011, num_sdf_blocks=40000)
+    rr = vsg.Renderer(W, H)
+    for i, f in enumerate(fr):
+        pm = cuda.from_numpy(f.pointmap).cuda()
+        rgb = cuda.from_numpy(f.rgb).cuda()
+        nm = cuda.from_numpy(f.normals).cuda()
+        sc.integrate(pm, rgb, nm, W, H, 0.02, f.pose, K.fx, K.fy, K.cx, K.cy)
+        rr.render(sc, f.pose, K.fx, K.fy, K.cx, K.cy, 0.2, 3.0)
+        ref = rr.download()["depth"]
+        got = np.fromfile(os.path.join(d, f"depth_{i}.bin"), np.float32).reshape(H, W)
+        assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), i
+        assert (got < 1e9).sum() > 0.5 * W * H
