@@ -125,6 +125,27 @@ VSG_API int vsg_integrate(vsg_scene* s, const float* pointmap, const uint8_t* rg
                   int h, float truncation, const float pose[16], float fx, float fy, float cx, float cy,
                   vsg_stream_t stream);
 
+/* Same integration as vsg_integrate, allocating no device memory.  This entry
+ * point has no counterpart in the reference.  It is for callers that cannot
+ * allocate while integrating: frame loops recorded into a CUDA graph
+ * (cudaMalloc is not allowed during stream capture), real-time loops that
+ * must not stall on cudaMalloc/cudaFree, hosts with a fixed GPU memory
+ * budget.  vsg_integrate grows two per-pixel work buffers with cudaMalloc
+ * when it first sees a larger image; this variant takes them from a fixed
+ * 20 MiB array of device memory inside the library instead.
+ * Limits and rules:
+ *   - at most 1,048,576 pixels (w*h) per frame; larger frames return
+ *     VSG_ERR_TOO_LARGE without doing anything;
+ *   - the first call on each device looks the array's address up
+ *     (cudaGetSymbolAddress) and should come before any stream capture;
+ *   - every call on a device shares the one array, so calls whose work
+ *     overlaps on the GPU (other streams, other scenes) race; serialise them;
+ *   - the scene must live on the current device (else VSG_ERR_INVALID_ARG).
+ * The scene itself is created beforehand with vsg_scene_create. */
+VSG_API int vsg_integrate_noalloc(vsg_scene* s, const float* pointmap, const uint8_t* rgb, const float* normals,
+                                  int w, int h, float truncation, const float pose[16], float fx, float fy,
+                                  float cx, float cy, vsg_stream_t stream);
+
 /* Counters of the scene and of its last frame / render.  Synchronises. */
 VSG_API int vsg_scene_stats(vsg_scene* s, vsg_stats* out);
 

@@ -788,4 +788,42 @@ int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H
     return cudaGetLastError() == cudaSuccess ? VSG_OK : VSG_ERR_CUDA;
 }
 
+// Same launch sequence as scene_integrate, with the per-pixel work buffers
+// supplied by the caller (at least W*H entries each) instead of the scene's
+// own, and without event timing; allocates nothing.
+int scene_integrate_with_pixels(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H, float trunc,
+                                const float* pose, float fx, float fy, float cx, float cy, float4* pix_world,
+                                uint32_t* pix_rgb, cudaStream_t st) {
+    Pose P;
+    memcpy(P.T, pose, sizeof(P.T));
+    SceneDev dev = sc->dev;
+    dev.pix_world = pix_world;
+    dev.pix_rgb = pix_rgb;
+    k_frame_begin<<<1, 1, 0, st>>>(dev.frame);
+    AllocArgs aa;
+    aa.s = dev;
+    aa.pm = pm;
+    aa.rgb = rgb;
+    aa.W = W;
+    aa.H = H;
+    aa.trunc = trunc;
+    aa.pose = P;
+    dim3 grid((W + kTile - 1) / kTile, (H + kTile - 1) / kTile);
+    k_alloc<<<grid, kTile * kTile, 0, st>>>(aa);
+    IntegArgs ia;
+    ia.s = dev;
+    ia.W = W;
+    ia.H = H;
+    ia.trunc = trunc;
+    ia.pose = P;
+    ia.fx = fx;
+    ia.fy = fy;
+    ia.cx = cx;
+    ia.cy = cy;
+    k_select<<<sc->sm_count * 4, 256, 0, st>>>(ia);
+    k_integrate<<<sc->sm_count * sc->integ_ctas_per_sm, 256, 0, st>>>(ia);
+    sc->integrated_frames++;
+    return cudaGetLastError() == cudaSuccess ? VSG_OK : VSG_ERR_CUDA;
+}
+
 }  // namespace vsg

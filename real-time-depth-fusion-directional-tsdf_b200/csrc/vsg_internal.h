@@ -48,6 +48,9 @@ void scene_free_device(Scene* sc);
 int scene_reset_device(Scene* sc, cudaStream_t st);
 int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H, float trunc,
                     const float* pose, float fx, float fy, float cx, float cy, cudaStream_t st);
+int scene_integrate_with_pixels(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H, float trunc,
+                                const float* pose, float fx, float fy, float cx, float cy, float4* pix_world,
+                                uint32_t* pix_rgb, cudaStream_t st);
 int render_launch(Renderer* r, Scene* sc, const float cam[3], const float* pose_dev, const float* pose_host,
                   float fx, float fy, float cx, float cy, float min_depth, float max_depth, cudaStream_t st);
 

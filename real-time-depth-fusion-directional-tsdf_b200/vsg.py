@@ -23,7 +23,7 @@ FLAG_HEAP_EXHAUSTED, FLAG_CHAIN_EXHAUSTED, FLAG_COORD_RANGE, FLAG_INSERT_RETRY, 
 # every symbol include/vsg.h declares
 EXPORTS = [
     "vsg_params_default", "vsg_scene_create", "vsg_scene_destroy", "vsg_scene_reset", "vsg_scene_params",
-    "vsg_integrate", "vsg_scene_stats", "vsg_scene_export", "vsg_renderer_create", "vsg_renderer_destroy",
+    "vsg_integrate", "vsg_integrate_noalloc", "vsg_scene_stats", "vsg_scene_export", "vsg_renderer_create", "vsg_renderer_destroy",
     "vsg_render", "vsg_render_hostpose", "vsg_renderer_outputs", "vsg_renderer_download",
     "vsg_timing_enable", "vsg_timing_read", "vsg_timing_reset", "vsg_version",
 ]
@@ -74,6 +74,7 @@ def lib() -> ctypes.CDLL:
         L.vsg_scene_reset.argtypes = [_P, _P]
         L.vsg_scene_params.argtypes = [_P, ctypes.POINTER(Params)]
         L.vsg_integrate.argtypes = [_P, _P, _P, _P, _I, _I, _F, _P, _F, _F, _F, _F, _P]
+        L.vsg_integrate_noalloc.argtypes = [_P, _P, _P, _P, _I, _I, _F, _P, _F, _F, _F, _F, _P]
         L.vsg_scene_stats.argtypes = [_P, ctypes.POINTER(Stats)]
         L.vsg_scene_export.argtypes = [_P, _P, _P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
         L.vsg_renderer_create.argtypes = [_I, _I, ctypes.POINTER(_P)]
@@ -150,6 +151,15 @@ class Scene:
     def integrate(self, pointmap, rgb, normals, width, height, truncation, pose, fx, fy, cx, cy, stream=None):
         T = np.ascontiguousarray(np.asarray(pose, np.float32).reshape(16))
         check("vsg_integrate", self.L.vsg_integrate(
+            self.h, _dptr(pointmap), _dptr(rgb), _dptr(normals), int(width), int(height), _F(truncation),
+            _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _stream(stream)))
+
+    def integrate_noalloc(self, pointmap, rgb, normals, width, height, truncation, pose, fx, fy, cx, cy,
+                          stream=None):
+        """vsg_integrate_noalloc: the same integration with its per-pixel
+        work buffers in the library's fixed device array (no allocation)."""
+        T = np.ascontiguousarray(np.asarray(pose, np.float32).reshape(16))
+        check("vsg_integrate_noalloc", self.L.vsg_integrate_noalloc(
             self.h, _dptr(pointmap), _dptr(rgb), _dptr(normals), int(width), int(height), _F(truncation),
             _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _stream(stream)))
 
