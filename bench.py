@@ -192,13 +192,17 @@ def run_ours(args):
             sc.integrate(pm, rgb, nm, W, H, TRUNC, T, K.fx, K.fy, K.cx, K.cy)
             rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
 
-    # per-frame statistics (algorithmic bytes), outside the timed region
+    # per-frame statistics (algorithmic bytes), outside the timed region; the
+    # instrumented mode also counts the distinct blocks each render reads
+    sc.timing(True)
     sc.reset()
     per_frame = []
     for pm, rgb, nm, T in dev:
         sc.integrate(pm, rgb, nm, W, H, TRUNC, T, K.fx, K.fy, K.cx, K.cy)
         rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
         per_frame.append(sc.stats())
+    sc.timing(False)
+    sc.timing_reset()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -235,16 +239,23 @@ def run_ours(args):
     vis = np.mean([p["frame_visible_blocks"] for p in per_frame])
     bytes_integ = upd * 512 * 16 + npx * 15
     bytes_alloc = npx * 12 + new * 20 + vis * 16
-    n_ray = vis  # blocks the frame can see (upper estimate of blocks rays read)
+    n_ray = float(np.mean([p["render_blocks_read"] for p in per_frame]))  # distinct blocks the rays read
     bytes_render = n_ray * 512 * 5 + npx * (4 + 16 + 16 + 16)
     kern["alloc"]["alg_bytes"] = bytes_alloc
     kern["integrate"]["alg_bytes"] = bytes_integ
     kern["render"]["alg_bytes"] = bytes_render
+    kern["render"]["blocks_read_per_frame"] = n_ray
     kern["select"]["alg_bytes"] = float(np.mean([p["high_water"] for p in per_frame])) * 9 + vis * 4
     kern["render"]["samples_full_per_frame"] = float(np.mean([p["render_samples_full"] for p in per_frame]))
     for k in ("samples_skipped", "jumps", "singles"):
         kern["render"][k + "_per_frame"] = float(np.mean([p["render_" + k] for p in per_frame]))
     dom = max(kern, key=lambda k: kern[k]["ms_per_launch"])
+    traffic = None
+    try:  # DRAM bytes per launch of the same kernel from one committed ncu capture
+        tr = json.load(open(os.path.join(ROOT, "profiles", "roofline_traffic.json")))
+        traffic = tr.get("k_" + dom, {}).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        pass
     peak, peak_kind = measured_peak_hbm()
     ach = kern[dom]["alg_bytes"] / (kern[dom]["ms_per_launch"] * 1e-3) / 1e9
     total_bytes = bytes_integ + bytes_alloc + bytes_render
@@ -259,7 +270,7 @@ def run_ours(args):
             "kernels": kern,
             "frame_bytes": total_bytes, "frame_gbps": total_bytes * fps / world / 1e9,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
-                         "frac": ach / peak, "traffic": None, "peak_kind": peak_kind},
+                         "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind},
             "clocks": clk.summary()}
     if not args.no_e2e:
         line["e2e"] = e2e(args, frames, K, sc, rr)

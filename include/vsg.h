@@ -100,7 +100,8 @@ typedef struct vsg_stats {
     uint32_t render_samples_full;    /* last render: march samples evaluated */
     uint32_t render_samples_skipped; /* last render: samples skipped as empty */
     uint32_t render_jumps;           /* last render: O(1) jumps over skipped runs */
-    uint32_t render_singles;         /* last render: samples rejected one at a time */
+    uint32_t render_singles;         /* last render: samples evaluated at a skip-cell boundary */
+    uint32_t render_blocks_read;     /* last render with timing enabled: distinct blocks read */
     uint32_t flags;              /* VSG_FLAG_* (sticky since reset) */
     uint32_t fast_division;      /* 1: the ray caster divides by the voxel size with a
                                     product + correction verified exhaustively against
@@ -181,7 +182,9 @@ VSG_API int vsg_renderer_download(const vsg_renderer* r, float* depth, float* po
 
 /* Per-kernel device time (ms) since the last vsg_timing_reset, measured
  * with CUDA events on the launching stream when timing is enabled.
- * Slots: 0 alloc, 1 integrate, 2 render. counts[i] = launches. */
+ * Slots: 0 alloc, 1 integrate, 2 render, 3 select. counts[i] = launches.
+ * With timing enabled renders also count the distinct blocks they read
+ * (vsg_stats.render_blocks_read). */
 VSG_API int vsg_timing_enable(vsg_scene* s, int enable);
 VSG_API int vsg_timing_read(vsg_scene* s, double* ms, uint32_t* counts, int n_slots);
 VSG_API int vsg_timing_reset(vsg_scene* s);

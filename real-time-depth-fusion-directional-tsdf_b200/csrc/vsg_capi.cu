@@ -192,6 +192,7 @@ int vsg_scene_stats(vsg_scene* s, vsg_stats* out) {
     out->render_samples_skipped = f.samples_skipped;
     out->render_jumps = f.jumps;
     out->render_singles = f.singles;
+    out->render_blocks_read = f.blocks_read;
     out->flags = c.flags;
     out->fast_division = s->impl.dev.div_fast ? 1u : 0u;
     return VSG_OK;

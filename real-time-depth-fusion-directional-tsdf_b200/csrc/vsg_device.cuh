@@ -95,7 +95,8 @@ struct FrameCounters {
     uint32_t samples_skipped;  // march samples skipped as provably invalid
     uint32_t jumps;          // O(1) jumps over runs of skipped samples
     uint32_t singles;        // samples evaluated at a cell boundary (no jump)
-    uint32_t pad2[4];
+    uint32_t blocks_read;    // distinct blocks the last render read (instrumented runs)
+    uint32_t pad2[3];
 };
 
 struct SceneDev {
@@ -107,6 +108,7 @@ struct SceneDev {
     int* block_slot;
     uint8_t* block_fresh;
     unsigned long long* block_wmask;  // per block: 2x2x2-voxel sub-cubes holding a weighted voxel
+    uint8_t* block_touched;           // instrumented renders: block read by a ray
     uint32_t* heap;
     unsigned long long* bindex;
     unsigned long long* dwm;

@@ -679,6 +679,7 @@ int scene_alloc_device(Scene* sc) {
     VSG_MALLOC(d.block_slot, B * sizeof(int));
     VSG_MALLOC(d.block_fresh, B);
     VSG_MALLOC(d.block_wmask, B * sizeof(unsigned long long));
+    VSG_MALLOC(d.block_touched, B);
     VSG_MALLOC(d.heap, B * sizeof(uint32_t));
     VSG_MALLOC(d.bindex, sizeof(unsigned long long) << (3 * sc->bidx_log2));
     VSG_MALLOC(d.dwm, sizeof(unsigned long long) << (3 * sc->bidx_log2));
@@ -707,7 +708,7 @@ int scene_alloc_device(Scene* sc) {
 
 void scene_free_device(Scene* sc) {
     SceneDev& d = sc->dev;
-    void* ptrs[] = {d.sup,       d.dwm,     d.bindex,    d.block_wmask, d.buckets,   d.bucket_next,
+    void* ptrs[] = {d.block_touched, d.sup, d.dwm,     d.bindex,    d.block_wmask, d.buckets,   d.bucket_next,
                     d.nodes,     d.voxels,  d.block_key, d.block_slot,  d.block_fresh, d.heap,
                     d.visible,   d.pix_world, d.pix_rgb, d.ctr,         d.frame};
     for (void* p : ptrs)

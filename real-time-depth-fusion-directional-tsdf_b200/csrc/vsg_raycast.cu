@@ -31,6 +31,7 @@ constexpr int kMaxMarch = 1 << 22;  // iteration guard of one ray
 
 struct RenderArgs {
     SceneDev s;
+    uint8_t* touched;  // non-null in instrumented runs: mark every block a tap reads
     int W, H;
     float camx, camy, camz;
     Pose pose;
@@ -95,7 +96,8 @@ __device__ __forceinline__ float div_v(float x, float v, float y, bool fast) {
 
 // getVoxel's block search (RayCastRender.cu:55-121) for the taps' blocks;
 // -1 = block not allocated (the tap reads as weight 0).
-__device__ __forceinline__ void refill_taps(const SceneDev& s, TapCache& tc, int bx0, int by0, int bz0, int span) {
+__device__ __forceinline__ void refill_taps(const SceneDev& s, TapCache& tc, int bx0, int by0, int bz0, int span,
+                                            uint8_t* touched) {
     tc.bx = bx0;
     tc.by = by0;
     tc.bz = bz0;
@@ -105,7 +107,9 @@ __device__ __forceinline__ void refill_taps(const SceneDev& s, TapCache& tc, int
         const int c = i & span;
         if (c == i) {
             const int bx = bx0 + (i & 1), by = by0 + ((i >> 1) & 1), bz = bz0 + ((i >> 2) & 1);
-            tc.set(i, block_ptr(s, bx, by, bz));
+            const int p = block_ptr(s, bx, by, bz);
+            if (touched && p >= 0) touched[p] = 1;
+            tc.set(i, p);
         } else {
             int p = tc.t0;
 #pragma unroll
@@ -150,7 +154,7 @@ __device__ __forceinline__ void cell_interval(const RayInv& R, int cx, int cy, i
 // trilinearInterpolationSimpleFastFast, RayCastRender.cu:127-215.  The
 // colour is only accumulated when asked for (it never steers the march).
 __device__ __forceinline__ bool trilinear(const SceneDev& s, float px, float py, float pz, float& dist,
-                                          bool want_color, uint32_t& rgb, TapCache& tc) {
+                                          bool want_color, uint32_t& rgb, TapCache& tc, uint8_t* touched) {
     const float off = s.voxel;
     const float v = s.voxel;
     const float dx = px - off / 2.0f, dy = py - off / 2.0f, dz = pz - off / 2.0f;
@@ -164,7 +168,7 @@ __device__ __forceinline__ bool trilinear(const SceneDev& s, float px, float py,
     const int bx0 = vox_to_block(ax0), by0 = vox_to_block(ay0), bz0 = vox_to_block(az0);
     const int span = (vox_to_block(ax1) != bx0 ? 1 : 0) | (vox_to_block(ay1) != by0 ? 2 : 0) |
                      (vox_to_block(az1) != bz0 ? 4 : 0);
-    if (!(tc.bx == bx0 && tc.by == by0 && tc.bz == bz0 && tc.span == span)) refill_taps(s, tc, bx0, by0, bz0, span);
+    if (!(tc.bx == bx0 && tc.by == by0 && tc.bz == bz0 && tc.span == span)) refill_taps(s, tc, bx0, by0, bz0, span, touched);
     const int lx0 = vox_local(ax0), ly0 = vox_local(ay0) * kBlock, lz0 = vox_local(az0) * kBlock * kBlock;
     const int lx1 = vox_local(ax1), ly1 = vox_local(ay1) * kBlock, lz1 = vox_local(az1) * kBlock * kBlock;
     uint2 raw[8];
@@ -323,7 +327,7 @@ __global__ void __launch_bounds__(128, 6) k_render(RenderArgs a) {
             }
             float dist = 0.0f;
             ++n_full;
-            const bool ok = trilinear(s, ox + st * wdx, oy + st * wdy, oz + st * wdz, dist, mode != 0, rgb, tc);
+            const bool ok = trilinear(s, ox + st * wdx, oy + st * wdy, oz + st * wdz, dist, mode != 0, rgb, tc, a.touched);
             if (mode == 0) {
                 if (ok && lastValid && lastSdf < 0.0f && dist > 0.0f) {
                     // zero crossing: a = last sample, b = this one
@@ -440,6 +444,15 @@ int verify_fixed_division(float v, bool* ok) {
     return VSG_OK;
 }
 
+__global__ void k_count_touched(const uint8_t* touched, const SceneCounters* ctr, FrameCounters* f) {
+    const uint32_t hw = ctr->high_water;
+    uint32_t c = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < hw; i += gridDim.x * blockDim.x) c += touched[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(&f->blocks_read, c);
+}
+
 __global__ void k_render_begin(FrameCounters* f) {
     f->hits = 0u;
     f->misses = 0u;
@@ -447,6 +460,7 @@ __global__ void k_render_begin(FrameCounters* f) {
     f->samples_skipped = 0u;
     f->jumps = 0u;
     f->singles = 0u;
+    f->blocks_read = 0u;
 }
 
 int render_launch(Renderer* r, Scene* sc, const float cam[3], const float* pose_dev, const float* pose_host,
@@ -473,11 +487,14 @@ int render_launch(Renderer* r, Scene* sc, const float cam[3], const float* pose_
     a.pos = r->position;
     a.col = r->color;
     a.nrm = r->normal;
+    a.touched = sc->timing.enabled ? sc->dev.block_touched : nullptr;
+    if (a.touched) cudaMemsetAsync(a.touched, 0, (size_t)sc->dev.num_blocks, st);
     k_render_begin<<<1, 1, 0, st>>>(sc->dev.frame);
     dim3 grid((r->w + 15) / 16, (r->h + 7) / 8);
     timing_begin(sc, kSlotRender, st);
     k_render<<<grid, 128, 0, st>>>(a);
     timing_end(sc, kSlotRender, st);
+    if (a.touched) k_count_touched<<<sc->sm_count * 2, 256, 0, st>>>(a.touched, sc->dev.ctr, sc->dev.frame);
     return cudaGetLastError() == cudaSuccess ? VSG_OK : VSG_ERR_CUDA;
 }
 

@@ -47,7 +47,8 @@ class Stats(ctypes.Structure):
         "allocated_blocks", "free_blocks", "high_water", "chain_nodes_used", "integrated_frames",
         "frame_valid_pixels", "frame_new_blocks", "frame_visible_blocks", "frame_updated_blocks",
         "frame_updated_voxels", "render_hits", "render_misses", "render_samples_full",
-        "render_samples_skipped", "render_jumps", "render_singles", "flags", "fast_division")]
+        "render_samples_skipped", "render_jumps", "render_singles", "render_blocks_read", "flags",
+        "fast_division")]
 
     def as_dict(self) -> dict:
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
