@@ -180,6 +180,38 @@ VSG_API int vsg_renderer_outputs(const vsg_renderer* r, float** depth, float** p
 VSG_API int vsg_renderer_download(const vsg_renderer* r, float* depth, float* position, float* color,
                           float* normal);
 
+/* ---- batched form: many independent scenes advanced together ----------
+ * No counterpart in the reference (it fuses one scan at a time).  A batch
+ * holds up to 256 scenes (each its own hash table and voxel pool, any
+ * resolution) and optional per-scene renderers.  vsg_batch_step integrates
+ * one frame for each listed scene -- and ray casts it at the same pose when
+ * `render` is set -- with one launch per stage for all of them; the step's
+ * launch sequence is captured into a CUDA graph and replayed while the set
+ * of resolutions stays the same.  Every scene's results are identical to
+ * vsg_integrate followed by vsg_render. */
+typedef struct vsg_batch vsg_batch;
+
+typedef struct vsg_batch_frame {
+    int scene;              /* index into the scenes given to vsg_batch_create */
+    const float* pointmap;  /* device float3[w*h] camera-space points */
+    const uint8_t* rgb;     /* device uchar3[w*h] */
+    const float* normals;   /* device float3[w*h] (not read; must be non-null) */
+    int w, h;
+    float truncation;
+    float pose[16];         /* row-major camera->world (copied at the call) */
+    float fx, fy, cx, cy;
+    float min_depth, max_depth; /* ray cast range */
+    int render;             /* 1: ray cast into the scene's renderer (w x h) */
+} vsg_batch_frame;
+
+VSG_API int vsg_batch_create(vsg_scene* const* scenes, vsg_renderer* const* renderers, int n, vsg_batch** out);
+VSG_API int vsg_batch_destroy(vsg_batch* b);
+/* Each scene at most once per step.  The first step of a new shape runs
+ * eagerly (and, with autotuning on, times three ray-cast launch variants on
+ * its own data) and captures the graph; later steps replay it. */
+VSG_API int vsg_batch_step(vsg_batch* b, const vsg_batch_frame* frames, int n_frames, vsg_stream_t stream);
+VSG_API int vsg_batch_autotune(vsg_batch* b, int enable);
+
 /* Per-kernel device time (ms) since the last vsg_timing_reset, measured
  * with CUDA events on the launching stream when timing is enabled.
  * Slots: 0 alloc, 1 integrate, 2 render, 3 select. counts[i] = launches.

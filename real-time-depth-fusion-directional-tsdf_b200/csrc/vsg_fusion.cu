@@ -27,6 +27,7 @@
 
 #include "../../include/vsg.h"
 #include "vsg_device.cuh"
+#include "vsg_fusion_core.cuh"
 #include "vsg_internal.h"
 
 namespace vsg {
@@ -35,601 +36,13 @@ namespace vsg {
 // allocation
 // ====================================================================
 
-constexpr int kTile = 16;        // pixels per CTA side
-constexpr int kSetCap = 1024;    // shared-memory de-duplication set
-constexpr int kMaxDDA = 1024;    // VoxelScene.cu:417
+__global__ void __launch_bounds__(kTile* kTile) k_alloc(AllocArgs a) { alloc_tile(a, blockIdx.x, blockIdx.y); }
 
-struct AllocArgs {
-    SceneDev s;
-    const float* pm;
-    const uint8_t* rgb;
-    int W, H;
-    float trunc;
-    Pose pose;
-};
-
-// worldToSDFBlock, VoxelScene.cu:74-96 (truncating conversion).
-__device__ __forceinline__ void world_to_block_alloc(float px, float py, float pz, float v, int& bx, int& by,
-                                                     int& bz) {
-    float q[3] = {px / v, py / v, pz / v};
-    int o[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        float sg = (q[a] > 0) ? 1.0f : ((q[a] < 0) ? -1.0f : 0.0f);
-        int iv = __float2int_rz(q[a] + sg * 0.5f);
-        if (iv < 0) iv = (int)((unsigned)iv - 7u);
-        o[a] = iv / kBlock;
-    }
-    bx = o[0];
-    by = o[1];
-    bz = o[2];
-}
-
-__device__ __forceinline__ void xform(const Pose& P, float x, float y, float z, float& ox, float& oy,
-                                      float& oz) {
-    ox = P.T[0] * x + P.T[1] * y + P.T[2] * z + P.T[3];
-    oy = P.T[4] * x + P.T[5] * y + P.T[6] * z + P.T[7];
-    oz = P.T[8] * x + P.T[9] * y + P.T[10] * z + P.T[11];
-}
-
-// Give a freshly inserted key storage.  entry_key / entry_ptr are the
-// fields of the slot (bucket entry or chain node) the caller now owns.
-// Heap pop as consumeHeap in VoxelScene.cu:183-195 (reference pops index
-// heapCounter, we pop free_count - 1: the same stack).
-__device__ __noinline__ bool claim_block(const SceneDev& s, unsigned long long key, unsigned long long* entry_key,
-                            int* entry_ptr, int slot_index) {
-    int old = atomicSub(&s.ctr->free_count, 1);
-    if (old <= 0) {
-        atomicAdd(&s.ctr->free_count, 1);
-        atomicExch(entry_key, kKeyTomb);
-        atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_HEAP_EXHAUSTED);
-        atomicAdd(&s.ctr->alloc_fail, 1u);
-        return false;
-    }
-    const uint32_t blk = s.heap[old - 1];
-    *entry_ptr = (int)blk;
-    s.block_key[blk] = key;
-    s.block_slot[blk] = slot_index;
-    s.block_fresh[blk] = 1;
-    atomicMax(&s.ctr->high_water, blk + 1);
-    int x, y, z;
-    unpack_key(key, x, y, z);
-    // dense index: first block of a cell owns it, a second one marks it shared
-    {
-        unsigned long long* cell = s.bindex + bidx_cell(x, y, z, s.bidx_log2);
-        const unsigned long long mine = blk < kIdxPtrMask - 2u
-                                            ? ((bidx_tag(x, y, z, s.bidx_log2) << 22) | (unsigned long long)blk)
-                                            : kIdxShared;
-        const unsigned long long prev = atomicCAS(cell, kIdxEmpty, mine);
-        if (prev != kIdxEmpty && prev != mine && prev != kIdxShared) atomicExch(cell, kIdxShared);
-    }
-    atomicAdd(&s.frame->n_new, 1u);
-    return true;
-}
-
-// Search the overflow chain of bucket b for key; append it when absent.
-// Lock-free: a node is published by CAS on the tail link.
-__device__ __noinline__ void chain_insert(const SceneDev& s, uint32_t b, unsigned long long key, bool insert) {
-    int* link = s.bucket_next + b;
-    int mine = -1;
-    const int base = (int)s.num_buckets * kBucketSlots;
-    for (int it = 0; it <= s.max_nodes + 1; ++it) {
-        int n = ld_volatile_i32(link);
-        if (n < 0) {
-            if (!insert) return;
-            if (mine < 0) {
-                mine = atomicAdd(&s.ctr->nodes_used, 1);
-                if (mine >= s.max_nodes) {
-                    atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_CHAIN_EXHAUSTED);
-                    atomicAdd(&s.ctr->alloc_fail, 1u);
-                    return;
-                }
-                s.nodes[mine].ptr = -1;
-                s.nodes[mine].next = -1;
-                s.nodes[mine].key = key;
-                __threadfence();
-            }
-            int prev = atomicCAS(link, -1, mine);
-            if (prev == -1) {
-                claim_block(s, key, &s.nodes[mine].key, &s.nodes[mine].ptr, base + mine);
-                return;
-            }
-            n = prev;
-        }
-        if (ld_volatile_u64(&s.nodes[n].key) == key) {
-            if (mine >= 0) s.nodes[mine].key = kKeyTomb;  // unpublished spare
-            return;
-        }
-        link = &s.nodes[n].next;
-    }
-    atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_INSERT_RETRY);
-}
-
-__device__ bool chain_contains(const SceneDev& s, uint32_t b, unsigned long long key) {
-    int n = ld_volatile_i32(s.bucket_next + b);
-    for (int it = 0; n >= 0 && it < s.max_nodes; ++it) {
-        if (ld_volatile_u64(&s.nodes[n].key) == key) return true;
-        n = ld_volatile_i32(&s.nodes[n].next);
-    }
-    return false;
-}
-
-// Single-thread insert (fallback when the shared set overflows).
-__device__ __noinline__ void insert_single(const SceneDev& s, unsigned long long key, int x, int y, int z) {
-    const uint32_t b = bucket_of(x, y, z, s.num_buckets);
-    Entry* bk = s.buckets + (size_t)b * kBucketSlots;
-    for (int it = 0; it < 4 * kBucketSlots; ++it) {
-        int first = -1;
-        unsigned long long seen = 0;
-        bool found = false;
-        for (int j = 0; j < kBucketSlots; ++j) {
-            unsigned long long k = ld_volatile_u64(&bk[j].key);
-            if (k == key) {
-                found = true;
-                break;
-            }
-            if (first < 0 && (k == kKeyEmpty || k == kKeyTomb)) {
-                first = j;
-                seen = k;
-            }
-            if (k == kKeyEmpty) break;
-        }
-        if (found) return;
-        if (first < 0) {
-            chain_insert(s, b, key, true);
-            return;
-        }
-        if (seen == kKeyTomb && chain_contains(s, b, key)) return;
-        unsigned long long prev = atomicCAS(&bk[first].key, seen, key);
-        if (prev == seen) {
-            claim_block(s, key, &bk[first].key, &bk[first].ptr, (int)(b * kBucketSlots + first));
-            return;
-        }
-    }
-    atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_INSERT_RETRY);
-}
-
-// Warp-cooperative insert of up to 4 keys (one per 8-lane group).  Lane j of
-// a group reads slot j of the key's bucket; ballots find a match or the
-// first free slot, whose lane issues the CAS.  A bucket slot only goes from
-// free to used while allocation runs, so everyone racing on one key ends at
-// the same first free slot.  All lanes of the warp must call this.
-__device__ void coop_insert(const SceneDev& s, unsigned long long key, bool active) {
-    const int lane = threadIdx.x & 31;
-    const int g = lane >> 3, sub = lane & 7;
-    int x = 0, y = 0, z = 0;
-    if (active) unpack_key(key, x, y, z);
-    const uint32_t b = active ? bucket_of(x, y, z, s.num_buckets) : 0u;
-    Entry* bk = s.buckets + (size_t)b * kBucketSlots;
-    bool pending = active;
-    for (int it = 0; it < 4 * kBucketSlots; ++it) {
-        if (!__any_sync(0xFFFFFFFFu, pending)) return;
-        unsigned long long cur = pending ? ld_volatile_u64(&bk[sub].key) : 0ull;
-        const unsigned mm = __ballot_sync(0xFFFFFFFFu, pending && cur == key);
-        const unsigned fm = __ballot_sync(0xFFFFFFFFu, pending && (cur == kKeyEmpty || cur == kKeyTomb));
-        const unsigned gm = (mm >> (g * 8)) & 0xFFu;
-        const unsigned gf = (fm >> (g * 8)) & 0xFFu;
-        const int lead = gf ? (__ffs(gf) - 1) : 0;
-        int res = 0;  // 1 = done
-        if (pending) {
-            if (gm) {
-                res = 1;
-            } else if (!gf) {
-                if (sub == 0) chain_insert(s, b, key, true);
-                res = 1;
-            } else if (sub == lead) {
-                if (cur == kKeyTomb && chain_contains(s, b, key)) {
-                    res = 1;
-                } else {
-                    unsigned long long prev = atomicCAS(&bk[lead].key, cur, key);
-                    if (prev == cur) {
-                        claim_block(s, key, &bk[lead].key, &bk[lead].ptr, (int)(b * kBucketSlots + lead));
-                        res = 1;
-                    }
-                }
-            }
-        }
-        const int r = __shfl_sync(0xFFFFFFFFu, res, (g * 8) + lead);
-        if (pending && (gm || !gf || r)) pending = false;
-    }
-    if (pending && sub == 0) atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_INSERT_RETRY);
-}
-
-__device__ __forceinline__ bool set_insert(unsigned long long* set, unsigned long long k) {
-    uint32_t h = (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> 54) & (kSetCap - 1);
-#pragma unroll 1
-    for (int p = 0; p < 32; ++p) {
-        unsigned long long cur = *(volatile unsigned long long*)(set + h);
-        if (cur == k) return true;
-        if (cur == kKeyEmpty) {
-            unsigned long long prev = atomicCAS(set + h, kKeyEmpty, k);
-            if (prev == kKeyEmpty || prev == k) return true;
-        }
-        h = (h + 1) & (kSetCap - 1);
-    }
-    return false;
-}
-
-__global__ void __launch_bounds__(kTile* kTile) k_alloc(AllocArgs a) {
-    __shared__ unsigned long long set[kSetCap];
-    __shared__ unsigned long long list[kSetCap];
-    __shared__ int list_n;
-    __shared__ uint32_t s_zmin, s_zmax, s_nonfinite, s_valid;
-    const int tid = threadIdx.x;
-    const SceneDev& s = a.s;
-    for (int i = tid; i < kSetCap; i += blockDim.x) set[i] = kKeyEmpty;
-    if (tid == 0) {
-        list_n = 0;
-        s_zmin = 0xFFFFFFFFu;
-        s_zmax = 0u;
-        s_nonfinite = 0u;
-        s_valid = 0u;
-    }
-    __syncthreads();
-    const int px = blockIdx.x * kTile + (tid & (kTile - 1));
-    const int py = blockIdx.y * kTile + (tid / kTile);
-    if (px < a.W && py < a.H) {
-        const size_t pi = (size_t)py * a.W + px;
-        const float p0 = __ldg(a.pm + 3 * pi + 0);
-        const float p1 = __ldg(a.pm + 3 * pi + 1);
-        const float p2 = __ldg(a.pm + 3 * pi + 2);
-        // integration validity (VoxelScene.cu:1040-1046) drives the depth band
-        float4 prep = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
-        if (p0 != 0.0f || p1 != 0.0f || p2 != 0.0f) {
-            // depthPos_world and cameraDist, VoxelScene.cu:1052-1062
-            float Px, Py, Pz;
-            xform(a.pose, p0, p1, p2, Px, Py, Pz);
-            const float ex = Px - a.pose.T[3], ey = Py - a.pose.T[7], ez = Pz - a.pose.T[11];
-            prep = make_float4(Px, Py, Pz, sqrtf(ex * ex + ey * ey + ez * ez));
-            atomicAdd(&s_valid, 1u);
-            if (isfinite(p0) && isfinite(p1) && isfinite(p2)) {
-                atomicMin(&s_zmin, f2ord(p2));
-                atomicMax(&s_zmax, f2ord(p2));
-            } else {
-                s_nonfinite = 1u;
-            }
-        }
-        s.pix_world[pi] = prep;
-        s.pix_rgb[pi] = (uint32_t)__ldg(a.rgb + 3 * pi) | ((uint32_t)__ldg(a.rgb + 3 * pi + 1) << 8) |
-                        ((uint32_t)__ldg(a.rgb + 3 * pi + 2) << 16);
-        // allocBlocksFromDepthMapMethod1Kernel, VoxelScene.cu:547-633
-        if (!(p2 <= 1e-6f)) {
-            const float cx = a.pose.T[3], cy = a.pose.T[7], cz = a.pose.T[11];
-            float wx, wy, wz;
-            xform(a.pose, p0, p1, p2, wx, wy, wz);
-            const float rx = wx - cx, ry = wy - cy, rz = wz - cz;
-            const float rl = sqrtf(rx * rx + ry * ry + rz * rz);
-            if (!(rl < 1e-6f)) {
-                float s0, s1, s2, e0, e1, e2;
-                xform(a.pose, p0, p1, p2 - a.trunc, s0, s1, s2);
-                xform(a.pose, p0, p1, p2 + a.trunc, e0, e1, e2);
-                // allocateBlocksAlongRay, VoxelScene.cu:295-481
-                const float v = s.voxel;
-                int c[3], e[3];
-                world_to_block_alloc(s0, s1, s2, v, c[0], c[1], c[2]);
-                world_to_block_alloc(e0, e1, e2, v, e[0], e[1], e[2]);
-                if (!(c[0] == e[0] && c[1] == e[1] && c[2] == e[2])) {
-                    float d[3] = {e0 - s0, e1 - s1, e2 - s2};
-                    const float len = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-                    if (!(len < 1e-6f)) {
-                        d[0] /= len;
-                        d[1] /= len;
-                        d[2] /= len;
-                        const float st[3] = {s0, s1, s2};
-                        const float ext = (float)kBlock * v;
-                        float step[3], tmax[3], tdel[3];
-#pragma unroll
-                        for (int k = 0; k < 3; ++k) {
-                            step[k] = (d[k] > 0) ? 1.0f : -1.0f;
-                            const float sc = (step[k] > 0) ? 1.0f : 0.0f;
-                            const float bnd = ((float)c[k] + sc) * ext - 0.5f * v;
-                            tmax[k] = (bnd - st[k]) / d[k];
-                            tdel[k] = (step[k] * ext) / d[k];
-                            if (d[k] == 0.0f) {
-                                tmax[k] = 1e6f;
-                                tdel[k] = 1e6f;
-                            }
-                        }
-#pragma unroll 1
-                        for (int it = 0; it < kMaxDDA; ++it) {
-                            if (coord_ok(c[0], c[1], c[2])) {
-                                const unsigned long long k = pack_key(c[0], c[1], c[2]);
-                                if (!set_insert(set, k)) insert_single(s, k, c[0], c[1], c[2]);
-                            } else {
-                                atomicAdd(&s.ctr->coord_drops, 1u);
-                                atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_COORD_RANGE);
-                            }
-                            if (c[0] == e[0] && c[1] == e[1] && c[2] == e[2]) break;
-                            if (tmax[0] < tmax[1] && tmax[0] < tmax[2]) {
-                                tmax[0] += tdel[0];
-                                c[0] += (int)step[0];
-                            } else if (tmax[1] < tmax[2]) {
-                                tmax[1] += tdel[1];
-                                c[1] += (int)step[1];
-                            } else {
-                                tmax[2] += tdel[2];
-                                c[2] += (int)step[2];
-                            }
-                        }
-                    }
-                }
-            }
-        }
-    }
-    __syncthreads();
-    for (int i = tid; i < kSetCap; i += blockDim.x) {
-        const unsigned long long k = set[i];
-        if (k != kKeyEmpty) list[atomicAdd(&list_n, 1)] = k;
-    }
-    __syncthreads();
-    const int n = list_n;
-    const int warp = tid >> 5, lane = tid & 31;
-    const int nwarps = blockDim.x >> 5;
-    for (int base = warp * 4; base < n; base += nwarps * 4) {
-        const int i = base + (lane >> 3);
-        coop_insert(s, i < n ? list[i] : 0ull, i < n);
-    }
-    if (tid == 0) {
-        if (s_valid) {
-            atomicAdd(&s.frame->n_valid_px, s_valid);
-            if (s_zmin != 0xFFFFFFFFu) {
-                atomicMin(&s.frame->zmin_ord, s_zmin);
-                atomicMax(&s.frame->zmax_ord, s_zmax);
-            }
-            if (s_nonfinite) atomicOr(&s.frame->nonfinite, 1u);
-        }
-    }
-}
-
-// ====================================================================
-// integration
-// ====================================================================
-
-struct IntegArgs {
-    SceneDev s;
-    int W, H;
-    float trunc;
-    Pose pose;
-    float fx, fy, cx, cy;
-};
-
-// Can any voxel of block (bx,by,bz) be updated this frame?  Conservative:
-// a voxel updates only if its rounded projection lands in the image and the
-// point it meets is within the truncation distance, so its camera z lies in
-// [zmin - t, zmax + t] of the frame's valid points.  Corner projections
-// bound the block's projection when it lies in front of the camera.
-__device__ bool block_maybe_updated(const IntegArgs& a, int bx, int by, int bz, float zlo, float zhi) {
-    const float v = a.s.voxel;
-    const float T3 = a.pose.T[3], T7 = a.pose.T[7], T11 = a.pose.T[11];
-    float zmn = 3.4e38f, zmx = -3.4e38f, umn = 3.4e38f, umx = -3.4e38f, vmn = 3.4e38f, vmx = -3.4e38f;
-    bool front = zlo > 0.0f;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        const float wx = (float)(bx * 8 + ((c & 1) ? 7 : 0)) * v - T3;
-        const float wy = (float)(by * 8 + ((c & 2) ? 7 : 0)) * v - T7;
-        const float wz = (float)(bz * 8 + ((c & 4) ? 7 : 0)) * v - T11;
-        const float x = a.pose.T[0] * wx + a.pose.T[4] * wy + a.pose.T[8] * wz;
-        const float y = a.pose.T[1] * wx + a.pose.T[5] * wy + a.pose.T[9] * wz;
-        const float z = a.pose.T[2] * wx + a.pose.T[6] * wy + a.pose.T[10] * wz;
-        zmn = fminf(zmn, z);
-        zmx = fmaxf(zmx, z);
-        if (z > 0.5f * zlo) {
-            const float iz = 1.0f / z;
-            const float u = x * a.fx * iz + a.cx, w = y * a.fy * iz + a.cy;
-            umn = fminf(umn, u);
-            umx = fmaxf(umx, u);
-            vmn = fminf(vmn, w);
-            vmx = fmaxf(vmx, w);
-        } else {
-            front = false;
-        }
-    }
-    if (zmx < zlo || zmn > zhi) return false;
-    if (!front) return true;
-    const float m = 2.0f;
-    if (umx < -1.5f - m || umn > (float)a.W - 0.5f + m) return false;
-    if (vmx < -1.5f - m || vmn > (float)a.H - 0.5f + m) return false;
-    return true;
-}
-
-// Visible-block compaction: one thread per pool block in [0, high_water),
-// ballot + popc, one atomic per warp.  Stands in for compactifyHashKernel
-// (VoxelScene.cu:1275-1300), which lists every allocated block: blocks the
-// test rejects cannot have a voxel updated this frame, so integrating only
-// the listed ones leaves every voxel as the full pass would.
 __global__ void __launch_bounds__(256) k_select(IntegArgs a) {
-    const SceneDev& s = a.s;
-    const int lane = threadIdx.x & 31;
-    const uint32_t hw = *(volatile uint32_t*)&s.ctr->high_water;
-    const FrameCounters fc = *s.frame;
-    const bool any_valid = fc.n_valid_px > 0;
-    const bool cull = fc.nonfinite == 0u && fc.zmin_ord != 0xFFFFFFFFu;
-    const float eps = 1e-3f + 2.0f * s.voxel;
-    const float zlo = cull ? ord2f(fc.zmin_ord) - a.trunc - eps : 0.0f;
-    const float zhi = cull ? ord2f(fc.zmax_ord) + a.trunc + eps : 0.0f;
-    for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < hw; b0 += gridDim.x * blockDim.x) {
-        const uint32_t b = b0 + threadIdx.x;
-        bool vis = false;
-        if (b < hw) {
-            const unsigned long long key = s.block_key[b];
-            if (key != kKeyEmpty && key != kKeyTomb) {
-                if (s.block_fresh[b]) {
-                    vis = true;
-                } else if (any_valid) {
-                    if (!cull) {
-                        vis = true;
-                    } else {
-                        int bx, by, bz;
-                        unpack_key(key, bx, by, bz);
-                        vis = block_maybe_updated(a, bx, by, bz, zlo, zhi);
-                    }
-                }
-            }
-        }
-        const unsigned mask = __ballot_sync(0xFFFFFFFFu, vis);
-        if (!mask) continue;
-        uint32_t pos = 0;
-        if (lane == 0) pos = atomicAdd(&s.frame->n_visible, (uint32_t)__popc(mask));
-        pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
-        if (vis) s.visible[pos + __popc(mask & ((1u << lane) - 1u))] = b;
-    }
+    select_blocks(a, blockIdx.x * blockDim.x, gridDim.x * blockDim.x);
 }
 
-constexpr int kIntegBatch = 8;  // voxels per lane with loads in flight together
-
-// Per-voxel TSDF update, VoxelScene.cu:954-1126, for the 16 voxels lane
-// `lane` owns in block blk (idx = 32k + lane), in batches of kIntegBatch:
-// projection of the whole batch, then its point gathers, then the SDF
-// decisions, then the voxel / colour loads, then the updates.
-__device__ void integrate_block(const IntegArgs& a, int blk, unsigned long long key, bool fresh, int lane) {
-    const SceneDev& s = a.s;
-    int bx, by, bz;
-    unpack_key(key, bx, by, bz);
-    Voxel* vb = s.voxels + (size_t)blk * kVoxPerBlock;
-    const float v = s.voxel;
-    const float* T = a.pose.T;
-    const float camx = T[3], camy = T[7], camz = T[11];
-    const float t = a.trunc;
-    const int lx = lane & 7;
-    const float wx = (float)(int)((unsigned)bx * 8u + (unsigned)lx) * v;
-    const float rx = wx - T[3];
-    int cnt = 0;
-    unsigned long long wm = 0ull;  // sub-cubes that received a weight this frame
-#pragma unroll 1
-    for (int k0 = 0; k0 < 16; k0 += kIntegBatch) {
-        int pix[kIntegBatch];
-#pragma unroll
-        for (int j = 0; j < kIntegBatch; ++j) {
-            const int k = k0 + j;
-            const int ly = (lane >> 3) + ((k & 1) << 2);
-            const int lz = k >> 1;
-            const float wy = (float)(int)((unsigned)by * 8u + (unsigned)ly) * v;
-            const float wz = (float)(int)((unsigned)bz * 8u + (unsigned)lz) * v;
-            const float ry = wy - T[7], rz = wz - T[11];
-            const float cxp = T[0] * rx + T[4] * ry + T[8] * rz;
-            const float cyp = T[1] * rx + T[5] * ry + T[9] * rz;
-            const float czp = T[2] * rx + T[6] * ry + T[10] * rz;
-            const float sx = cxp * a.fx / czp + a.cx;
-            const float sy = cyp * a.fy / czp + a.cy;
-            const int ix = __float2int_rz(sx + 0.5f), iy = __float2int_rz(sy + 0.5f);
-            pix[j] = (ix >= 0 && ix < a.W && iy >= 0 && iy < a.H) ? iy * a.W + ix : -1;
-        }
-        float4 P[kIntegBatch];
-#pragma unroll
-        for (int j = 0; j < kIntegBatch; ++j)
-            P[j] = pix[j] >= 0 ? __ldg(s.pix_world + pix[j]) : make_float4(0.0f, 0.0f, 0.0f, -1.0f);
-        float sdfv[kIntegBatch];
-        bool upd[kIntegBatch];
-#pragma unroll
-        for (int j = 0; j < kIntegBatch; ++j) {
-            const int k = k0 + j;
-            const int ly = (lane >> 3) + ((k & 1) << 2);
-            const int lz = k >> 1;
-            const float wy = (float)(int)((unsigned)by * 8u + (unsigned)ly) * v;
-            const float wz = (float)(int)((unsigned)bz * 8u + (unsigned)lz) * v;
-            upd[j] = false;
-            sdfv[j] = 0.0f;
-            if (!(P[j].w < 0.0f)) {  // pixel valid: point != (0,0,0)
-                const float dx = wx - P[j].x, dy = wy - P[j].y, dz = wz - P[j].z;
-                float sdf = sqrtf(dx * dx + dy * dy + dz * dz);
-                const float vdist = sqrtf((wx - camx) * (wx - camx) + (wy - camy) * (wy - camy) +
-                                          (wz - camz) * (wz - camz));
-                if (vdist < P[j].w) sdf = -sdf;
-                if (!(sdf < -t || sdf > t)) {
-                    sdfv[j] = fmaxf(-t, fminf(t, sdf));
-                    upd[j] = true;
-                }
-            }
-        }
-        Voxel old[kIntegBatch];
-        uint32_t col[kIntegBatch];
-#pragma unroll
-        for (int j = 0; j < kIntegBatch; ++j) {
-            const int idx = (k0 + j) * 32 + lane;
-            old[j] = Voxel{0.0f, 0u};
-            col[j] = 0u;
-            if (upd[j]) {
-                if (!fresh) old[j] = vb[idx];
-                col[j] = __ldg(s.pix_rgb + pix[j]);
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < kIntegBatch; ++j) {
-            const int idx = (k0 + j) * 32 + lane;
-            if (upd[j]) {
-                const float oldW = (float)(old[j].rgbw >> 24);
-                const float newW = oldW + 1.0f;
-                const float nsdf = (old[j].sdf * oldW + sdfv[j] * 1.0f) / newW;
-                const uint32_t nw = (uint32_t)fminf(255.0f, newW);
-                const float nr = ((float)(old[j].rgbw & 0xFFu) * oldW + (float)(col[j] & 0xFFu) * 1.0f) / newW;
-                const float ng =
-                    ((float)((old[j].rgbw >> 8) & 0xFFu) * oldW + (float)((col[j] >> 8) & 0xFFu) * 1.0f) / newW;
-                const float nb =
-                    ((float)((old[j].rgbw >> 16) & 0xFFu) * oldW + (float)((col[j] >> 16) & 0xFFu) * 1.0f) / newW;
-                Voxel nv;
-                nv.sdf = nsdf;
-                nv.rgbw = pack_rgbw((uint32_t)nr, (uint32_t)ng, (uint32_t)nb, nw);
-                vb[idx] = nv;
-                ++cnt;
-                const int k = k0 + j;
-                const int ly = (lane >> 3) + ((k & 1) << 2), lz = k >> 1;
-                wm |= 1ull << ((((lz >> 1) * 4 + (ly >> 1)) * 4) + (lx >> 1));
-            } else if (fresh) {
-                vb[idx] = Voxel{0.0f, 0u};
-            }
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, o);
-    const unsigned wlo = __reduce_or_sync(0xFFFFFFFFu, (unsigned)wm);
-    const unsigned whi = __reduce_or_sync(0xFFFFFFFFu, (unsigned)(wm >> 32));
-    const unsigned long long old_wm = fresh ? 0ull : s.block_wmask[blk];
-    const unsigned long long newbits = (((unsigned long long)whi << 32) | wlo) & ~old_wm;
-    if (newbits && lane < 27) {
-        // newly weighted sub-cubes: dilate by one sub-cube into this block
-        // position and its 26 neighbours (one lane per neighbour)
-        const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
-        const unsigned long long mk = dil_z(dil_y(dil_x(newbits, dx), dy), dz);
-        if (mk) {
-            const int nx = bx + dx, ny = by + dy, nz = bz + dz;
-            atomicOr(s.dwm + bidx_cell(nx, ny, nz, s.bidx_log2), mk);
-            const uint32_t q = grid_bit(nx >> 3, ny >> 3, nz >> 3, s.bidx_log2 - 3);
-            atomicOr(s.sup + (q >> 5), 1u << (q & 31));
-        }
-    }
-    __syncwarp();
-    if (lane == 0) {
-        if (cnt) {
-            atomicAdd(&s.frame->n_upd_blocks, 1u);
-            atomicAdd(&s.frame->n_upd_voxels, (uint32_t)cnt);
-        }
-        // only this warp touches the block during the launch
-        const unsigned long long nw = ((unsigned long long)whi << 32) | wlo;
-        if (fresh) {
-            s.block_wmask[blk] = nw;
-            s.block_fresh[blk] = 0;
-        } else if (nw) {
-            s.block_wmask[blk] |= nw;
-        }
-    }
-}
-
-// One warp per visible block, taken from a work counter.
-__global__ void __launch_bounds__(256) k_integrate(IntegArgs a) {
-    const SceneDev& s = a.s;
-    const int lane = threadIdx.x & 31;
-    const uint32_t n = *(volatile uint32_t*)&s.frame->n_visible;
-    for (;;) {
-        uint32_t i = 0;
-        if (lane == 0) i = atomicAdd(&s.frame->work, 1u);
-        i = __shfl_sync(0xFFFFFFFFu, i, 0);
-        if (i >= n) break;
-        const uint32_t b = s.visible[i];
-        const unsigned long long key = s.block_key[b];
-        const bool fresh = s.block_fresh[b] != 0;
-        integrate_block(a, (int)b, key, fresh, lane);
-    }
-}
+__global__ void __launch_bounds__(256) k_integrate(IntegArgs a) { integrate_work(a); }
 
 // ====================================================================
 // scene management kernels
@@ -649,11 +62,7 @@ __global__ void k_init_counters(SceneCounters* c, int num_blocks) {
     c->coord_drops = 0u;
 }
 
-__global__ void k_frame_begin(FrameCounters* f) {
-    FrameCounters z = {};
-    z.zmin_ord = 0xFFFFFFFFu;
-    *f = z;
-}
+__global__ void k_frame_begin(FrameCounters* f) { frame_begin(f); }
 
 // ====================================================================
 // host side
@@ -735,7 +144,7 @@ int scene_reset_device(Scene* sc, cudaStream_t st) {
     return cudaGetLastError() == cudaSuccess ? VSG_OK : VSG_ERR_CUDA;
 }
 
-static int ensure_pixel_buffers(Scene* sc, size_t npx) {
+int ensure_pixel_buffers(Scene* sc, size_t npx) {
     if (npx <= sc->pix_capacity) return VSG_OK;
     // grows only: a first frame of a larger resolution allocates (outside
     // any capture), later frames reuse

@@ -26,6 +26,7 @@ EXPORTS = [
     "vsg_integrate", "vsg_integrate_noalloc", "vsg_scene_stats", "vsg_scene_export", "vsg_renderer_create", "vsg_renderer_destroy",
     "vsg_render", "vsg_render_hostpose", "vsg_renderer_outputs", "vsg_renderer_download",
     "vsg_timing_enable", "vsg_timing_read", "vsg_timing_reset", "vsg_version",
+    "vsg_batch_create", "vsg_batch_destroy", "vsg_batch_step", "vsg_batch_autotune",
 ]
 
 
@@ -40,6 +41,14 @@ class Params(ctypes.Structure):
                 ("truncation_scale", ctypes.c_float), ("hash_num_slots", ctypes.c_uint32),
                 ("num_sdf_blocks", ctypes.c_uint32), ("max_chain_nodes", ctypes.c_uint32),
                 ("occupancy_log2", ctypes.c_uint32)]
+
+
+class BatchFrame(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_int), ("pointmap", ctypes.c_void_p), ("rgb", ctypes.c_void_p),
+                ("normals", ctypes.c_void_p), ("w", ctypes.c_int), ("h", ctypes.c_int),
+                ("truncation", ctypes.c_float), ("pose", ctypes.c_float * 16), ("fx", ctypes.c_float),
+                ("fy", ctypes.c_float), ("cx", ctypes.c_float), ("cy", ctypes.c_float),
+                ("min_depth", ctypes.c_float), ("max_depth", ctypes.c_float), ("render", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -87,6 +96,10 @@ def lib() -> ctypes.CDLL:
         L.vsg_timing_enable.argtypes = [_P, _I]
         L.vsg_timing_read.argtypes = [_P, _P, _P, _I]
         L.vsg_timing_reset.argtypes = [_P]
+        L.vsg_batch_create.argtypes = [_P, _P, _I, ctypes.POINTER(_P)]
+        L.vsg_batch_destroy.argtypes = [_P]
+        L.vsg_batch_step.argtypes = [_P, ctypes.POINTER(BatchFrame), _I, _P]
+        L.vsg_batch_autotune.argtypes = [_P, _I]
         _lib = L
     return _lib
 
@@ -244,6 +257,55 @@ class Renderer:
         check("vsg_renderer_download", self.L.vsg_renderer_download(self.h, _hptr(d), _hptr(p), _hptr(c), _hptr(nm)))
         assert n == d.size
         return {"depth": d, "position": p, "color": c, "normal": nm}
+
+
+class Batch:
+    """vsg_batch_*: scenes (and renderers) advanced together, one frame per
+    listed scene per step."""
+
+    def __init__(self, scenes, renderers=None):
+        self.L = lib()
+        n = len(scenes)
+        self._scenes = list(scenes)
+        self._renderers = list(renderers) if renderers is not None else [None] * n
+        sh = (_P * n)(*[s.h.value if isinstance(s.h, _P) else s.h for s in scenes])
+        rh = (_P * n)(*[(r.h.value if isinstance(r.h, _P) else r.h) if r is not None else None
+                        for r in self._renderers])
+        h = _P()
+        check("vsg_batch_create", self.L.vsg_batch_create(sh, rh, n, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.vsg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def autotune(self, enable: bool):
+        check("vsg_batch_autotune", self.L.vsg_batch_autotune(self.h, int(enable)))
+
+    @staticmethod
+    def frame(scene, pointmap, rgb, normals, width, height, truncation, pose, fx, fy, cx, cy,
+              min_depth=0.2, max_depth=3.0, render=True) -> BatchFrame:
+        f = BatchFrame()
+        f.scene = int(scene)
+        f.pointmap, f.rgb, f.normals = _dptr(pointmap), _dptr(rgb), _dptr(normals)
+        f.w, f.h = int(width), int(height)
+        f.truncation = float(truncation)
+        f.pose[:] = [float(x) for x in np.asarray(pose, np.float32).reshape(16)]
+        f.fx, f.fy, f.cx, f.cy = float(fx), float(fy), float(cx), float(cy)
+        f.min_depth, f.max_depth = float(min_depth), float(max_depth)
+        f.render = int(bool(render))
+        return f
+
+    def step(self, frames, stream=None):
+        arr = (BatchFrame * len(frames))(*frames)
+        check("vsg_batch_step", self.L.vsg_batch_step(self.h, arr, len(frames), _stream(stream)))
 
 
 def version() -> str:
