@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-scans", type=int, default=64)
     return ap.parse_args()
 
 
@@ -274,6 +276,8 @@ def run_ours(args):
             "clocks": clk.summary()}
     if not args.no_e2e:
         line["e2e"] = e2e(args, frames, K, sc, rr)
+    if not args.no_batched:
+        line["batched"] = run_batched(args)
     if not args.no_cpu and rank == 0:
         line["cpu_baseline"] = cpu_baseline(frames, K)
     if rank == 0:
@@ -282,6 +286,87 @@ def run_ours(args):
     rr.close()
     if dist:
         dist.destroy_process_group()
+
+
+def run_batched(args) -> dict:
+    """Batched plain method: independent tabletop scans (own seeds; 160x120 /
+    320x240 / 640x480; U[10,200] frames; 50000-400000 buckets) integrated and
+    ray cast frame by frame.  Times the same frames one scan after the other
+    through vsg_integrate + vsg_render ("plain per-scene") and all scans
+    together through vsg_batch_step (graph-replayed steps, autotuned ray
+    cast).  Frames are generated on the GPU and resident before timing."""
+    import torch
+
+    import synth
+    import vsg
+
+    scans = synth.batched_scans(args.batched_scans)
+    scenes, rends, frames = [], [], []
+    for i, sc in enumerate(scans):
+        K = sc["K"]
+        scenes.append(vsg.Scene(voxel_size=VOXEL, truncation=TRUNC, hash_num_slots=sc["buckets"],
+                                num_sdf_blocks=sc["buckets"]))
+        rends.append(vsg.Renderer(K.width, K.height))
+        geo = synth.tabletop_scene(sc["seed"])
+        frames.append([synth.render_frame_torch(geo, K, T, seed=sc["seed"] * 1000 + j) + (T,)
+                       for j, T in enumerate(sc["poses"])])
+    torch.cuda.synchronize()
+    n_frames = sum(len(f) for f in frames)
+    n_pix = sum(len(f) * sc["K"].width * sc["K"].height for f, sc in zip(frames, scans))
+
+    def plain_pass():
+        for i, sc in enumerate(scans):
+            K = sc["K"]
+            for pm, rgb, nm, T in frames[i]:
+                scenes[i].integrate(pm, rgb, nm, K.width, K.height, TRUNC, T, K.fx, K.fy, K.cx, K.cy)
+                rends[i].render(scenes[i], T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
+
+    batch = vsg.Batch(scenes, rends)
+    steps = max(len(f) for f in frames)
+    step_frames = []
+    for t in range(steps):
+        fl = []
+        for i, sc in enumerate(scans):
+            if t < len(frames[i]):
+                K = sc["K"]
+                pm, rgb, nm, T = frames[i][t]
+                fl.append(batch.frame(i, pm, rgb, nm, K.width, K.height, TRUNC, T, K.fx, K.fy, K.cx, K.cy,
+                                      MIN_D, MAX_D, render=True))
+        step_frames.append(fl)
+
+    def batched_pass():
+        for fl in step_frames:
+            batch.step(fl)
+
+    def timed(fn):
+        for s in scenes:
+            s.reset()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3
+
+    timed(batched_pass)  # first pass: eager steps, autotuning, graph captures
+    t_batched = timed(batched_pass)
+    timed(plain_pass)  # warm
+    t_plain = timed(plain_pass)
+    batch.close()
+    res = {"workload": f"{len(scans)} tabletop scans (160x120/320x240/640x480, U[10,200] frames), "
+                       f"{n_frames} frames, voxel 4mm, trunc 0.02m",
+           "frames": n_frames, "steps": steps,
+           "frames_per_s": n_frames / t_batched, "mpix_per_s": n_pix / t_batched / 1e6,
+           "plain_per_scene_frames_per_s": n_frames / t_plain,
+           "speedup_vs_plain": t_plain / t_batched}
+    for s in scenes:
+        s.close()
+    for r in rends:
+        r.close()
+    del frames
+    torch.cuda.empty_cache()
+    return res
 
 
 def e2e(args, frames, K, sc, rr) -> dict:

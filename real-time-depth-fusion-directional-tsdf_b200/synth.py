@@ -254,3 +254,105 @@ def room_stream(seed: int = 1, frames: int = 300, width: int = 1280, height: int
     ids = range(frames) if frame_ids is None else frame_ids
     return [render_frame(scene, K, poses[i], np.random.default_rng([seed, i]), zmin=0.2, zmax=4.0,
                          color_top=2.5) for i in ids], K
+
+
+# ----------------------------------------------------- device-side generation
+
+def render_frame_torch(scene: Scene, K: Intrinsics, pose: np.ndarray, seed: int | None, device="cuda",
+                       zmin: float = 0.2, zmax: float = 3.0, color_top: float = 0.7):
+    """The same ray tracing as render_frame, with torch on a GPU, for
+    workloads of thousands of frames.  Returns device tensors
+    (pointmap (H,W,3) f32, rgb (H,W,3) u8, normals (H,W,3) f32) and the pose.
+    The noise comes from torch's generator, so frames differ from
+    render_frame's bit for bit but follow the same model."""
+    import torch
+
+    W, H = K.width, K.height
+    dt = torch.float64
+    v, u = torch.meshgrid(torch.arange(H, device=device, dtype=dt), torch.arange(W, device=device, dtype=dt),
+                          indexing="ij")
+    dc = torch.stack([(u - K.cx) / K.fx, (v - K.cy) / K.fy, torch.ones_like(u)], -1).reshape(-1, 3)
+    R = torch.as_tensor(pose[:3, :3], dtype=dt, device=device)
+    o = torch.as_tensor(pose[:3, 3], dtype=dt, device=device)
+    dn = dc / dc.norm(dim=1, keepdim=True)
+    dw = dn @ R.T
+    n = dw.shape[0]
+    tbest = torch.full((n,), float("inf"), dtype=dt, device=device)
+    nbest = torch.zeros((n, 3), dtype=dt, device=device)
+    for (p0, nrm) in scene.planes:
+        nr = torch.as_tensor(nrm, dtype=dt, device=device)
+        den = dw @ nr
+        t = ((torch.as_tensor(p0, dtype=dt, device=device) - o) @ nr) / torch.where(den.abs() < 1e-9,
+                                                                                     torch.full_like(den, 1e-9), den)
+        ok = (den < -1e-9) & (t > 0) & (t < tbest)
+        tbest = torch.where(ok, t, tbest)
+        nbest = torch.where(ok[:, None], nr.expand_as(nbest), nbest)
+    for (c, r) in scene.spheres:
+        ct = torch.as_tensor(np.asarray(c), dtype=dt, device=device)
+        oc = o - ct
+        b = dw @ oc
+        disc = b * b - (oc @ oc - r * r)
+        t = -b - torch.sqrt(torch.clamp(disc, min=0.0))
+        ok = (disc > 0) & (t > 0) & (t < tbest)
+        tbest = torch.where(ok, t, tbest)
+        hp = o + dw * t[:, None]
+        nbest = torch.where(ok[:, None], (hp - ct) / r, nbest)
+    for (lo, hi) in scene.boxes:
+        inv = 1.0 / torch.where(dw.abs() < 1e-9, torch.full_like(dw, 1e-9), dw)
+        t0 = (torch.as_tensor(np.asarray(lo), dtype=dt, device=device) - o) * inv
+        t1 = (torch.as_tensor(np.asarray(hi), dtype=dt, device=device) - o) * inv
+        tmin, tmax = torch.minimum(t0, t1), torch.maximum(t0, t1)
+        tn, tf = tmin.max(dim=1).values, tmax.min(dim=1).values
+        ok = (tn <= tf) & (tn > 0) & (tn < tbest)
+        tbest = torch.where(ok, tn, tbest)
+        ax = tmin.argmax(dim=1)
+        nn = torch.zeros_like(nbest)
+        nn.scatter_(1, ax[:, None], -torch.sign(dw.gather(1, ax[:, None])))
+        nbest = torch.where(ok[:, None], nn, nbest)
+    if scene.room is not None:
+        inv = 1.0 / torch.where(dw.abs() < 1e-9, torch.full_like(dw, 1e-9), dw)
+        t0 = (torch.as_tensor(np.asarray(scene.room[0]), dtype=dt, device=device) - o) * inv
+        t1 = (torch.as_tensor(np.asarray(scene.room[1]), dtype=dt, device=device) - o) * inv
+        tmax = torch.maximum(t0, t1)
+        tf = tmax.min(dim=1).values
+        ax = tmax.argmin(dim=1)
+        ok = (tf > 0) & (tf < tbest)
+        tbest = torch.where(ok, tf, tbest)
+        nn = torch.zeros_like(nbest)
+        nn.scatter_(1, ax[:, None], -torch.sign(dw.gather(1, ax[:, None])))
+        nbest = torch.where(ok[:, None], nn, nbest)
+    z = tbest * dn[:, 2]
+    if seed is not None:
+        g = torch.Generator(device=device)
+        g.manual_seed(int(seed))
+        zf = torch.where(torch.isfinite(z), z, torch.zeros_like(z))
+        z = z + torch.randn(z.shape, generator=g, device=device, dtype=dt) * (0.0012 + 0.0019 * (zf - 0.4) ** 2)
+    valid = torch.isfinite(z) & (z >= zmin) & (z <= zmax)
+    zz = torch.where(valid, z, torch.zeros_like(z))
+    pts = dc * zz[:, None]
+    hw = o + dw * torch.where(valid, tbest, torch.zeros_like(tbest))[:, None]
+    t = torch.clamp(hw[:, 1] / color_top, 0.0, 1.0)
+    rgb = torch.stack([255.0 * t, 255.0 * (1.0 - (2.0 * t - 1.0).abs()), 255.0 * (1.0 - t)], -1)
+    rgb = torch.clamp(rgb, 0, 255).to(torch.uint8)
+    rgb[~valid] = 0
+    nc = nbest @ R
+    nc[~valid] = 0
+    return (pts.reshape(H, W, 3).float().contiguous(), rgb.reshape(H, W, 3).contiguous(),
+            nc.reshape(H, W, 3).float().contiguous())
+
+
+def batched_scans(n_scans: int = 64, seed: int = 2, frames_lo: int = 10, frames_hi: int = 200,
+                  resolutions=((160, 120), (320, 240), (640, 480))) -> list:
+    """Batched-plain workload: independent tabletop scans, each its own seed,
+    resolution drawn from `resolutions`, frame count from U[frames_lo,
+    frames_hi], hash size in proportion to the image area (50000-400000
+    buckets).  Returns (scene seed, intrinsics, poses, buckets) per scan."""
+    rng = np.random.default_rng(seed)
+    scans = []
+    for i in range(n_scans):
+        w, h = resolutions[int(rng.integers(len(resolutions)))]
+        nf = int(rng.integers(frames_lo, frames_hi + 1))
+        K = TABLETOP_K if (w, h) == (640, 480) else scaled_intrinsics(TABLETOP_K, w, h)
+        buckets = int(50000 + 350000 * (w * h - 160 * 120) / (640 * 480 - 160 * 120))
+        scans.append({"seed": 1000 + i, "K": K, "poses": orbit_poses(nf), "buckets": buckets})
+    return scans
