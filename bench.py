@@ -249,7 +249,7 @@ def run_ours(args):
     kern["render"]["blocks_read_per_frame"] = n_ray
     kern["select"]["alg_bytes"] = float(np.mean([p["high_water"] for p in per_frame])) * 9 + vis * 4
     kern["render"]["samples_full_per_frame"] = float(np.mean([p["render_samples_full"] for p in per_frame]))
-    for k in ("samples_skipped", "jumps", "singles"):
+    for k in ("samples_skipped", "jumps", "singles", "lane_iters", "warp_iters"):
         kern["render"][k + "_per_frame"] = float(np.mean([p["render_" + k] for p in per_frame]))
     dom = max(kern, key=lambda k: kern[k]["ms_per_launch"])
     traffic = None

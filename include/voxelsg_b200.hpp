@@ -13,6 +13,9 @@
  *   RayCastRender        (RayCastRender.h:20-124): initialize, render,
  *                         downloadResults, downloadDepthFloat,
  *                         getOutputDepth/Color/Normal/Positions
+ *   MarchingCubesParams, MarchingCubesOutput, allocateMarchingCubesOutput,
+ *   freeMarchingCubesOutput, runMarchingCubesCUDA,
+ *   copyMarchingCubesTriangleCount (MarchingCubes.h:7-58)
  * so that reference call sites compile unchanged against it.  Like the
  * reference, the methods print to stderr and return on bad input instead of
  * throwing; the only throw is GlobalParamsConfig::initialize.
@@ -118,6 +121,14 @@ struct Params {
     float truncation = 0.0f;
 };
 
+class VoxelScene;
+
+/* What VoxelScene::getHashData hands to the marching-cubes launcher: here a
+ * view of the scene's handle (the reference exposes its raw hash arrays). */
+struct CUDAHashRef {
+    vsg_scene* scene = nullptr;
+};
+
 class VoxelScene {
 public:
     explicit VoxelScene(const Params& params) : m_params(params) {
@@ -188,10 +199,16 @@ public:
     Params& getParams() { return m_params; }
     const Params& getParams() const { return m_params; }
     vsg_scene* handle() const { return m_scene; }
+    /* VoxelScene.h:129 */
+    CUDAHashRef& getHashData() {
+        m_hashRef.scene = m_scene;
+        return m_hashRef;
+    }
 
 private:
     Params m_params;
     vsg_scene* m_scene = nullptr;
+    CUDAHashRef m_hashRef;
 };
 
 class RayCastRender {
@@ -278,3 +295,68 @@ private:
     vsg_renderer* m_r = nullptr;
     int m_width = 0, m_height = 0;
 };
+
+/* MarchingCubes.h:7-17 */
+struct MarchingCubesParams {
+    float isoValue = 0.0f;
+    float voxelSize = 1.0f; /* > 0 overrides the scene's voxel size, as in the reference */
+    int maxTriangles = 0;
+};
+
+/* MarchingCubes.h:19-31: device triangle soup (3 vertices / normals each). */
+struct MarchingCubesOutput {
+    float3* d_vertices = nullptr;
+    float3* d_normals = nullptr;
+    int* d_triangleCount = nullptr;
+    int maxTriangles = 0;
+    vsg_mc_output* handle = nullptr;
+};
+
+inline void freeMarchingCubesOutput(MarchingCubesOutput& output) {
+    if (output.handle) vsg_mc_output_destroy(output.handle);
+    output = MarchingCubesOutput();
+}
+
+inline void allocateMarchingCubesOutput(MarchingCubesOutput& output, int maxTriangles) {
+    if (maxTriangles <= 0) {
+        std::cerr << "allocateMarchingCubesOutput: maxTriangles must be positive." << std::endl;
+        return;
+    }
+    freeMarchingCubesOutput(output);
+    if (vsg_mc_output_create(maxTriangles, &output.handle) != VSG_OK) {
+        std::cerr << "allocateMarchingCubesOutput: allocation failed" << std::endl;
+        output.handle = nullptr;
+        return;
+    }
+    float *v = nullptr, *n = nullptr;
+    vsg_mc_output_buffers(output.handle, &v, &n, &output.d_triangleCount, &output.maxTriangles);
+    output.d_vertices = reinterpret_cast<float3*>(v);
+    output.d_normals = reinterpret_cast<float3*>(n);
+}
+
+/* The reference synchronises the stream before returning; so does this. */
+inline void runMarchingCubesCUDA(const CUDAHashRef& hashData, const Params& params,
+                                 const MarchingCubesParams& paramsMC, MarchingCubesOutput& output,
+                                 cudaStream_t stream = nullptr) {
+    (void)params; /* the scene carries its own voxel size */
+    if (hashData.scene == nullptr) {
+        std::cerr << "runMarchingCubesCUDA: Hash data not initialized." << std::endl;
+        return;
+    }
+    if (output.handle == nullptr) {
+        std::cerr << "runMarchingCubesCUDA: Output buffers not allocated." << std::endl;
+        return;
+    }
+    if (vsg_mc_run(hashData.scene, output.handle, paramsMC.isoValue, paramsMC.voxelSize, stream) != VSG_OK) {
+        std::cerr << "runMarchingCubesCUDA: kernel launch failed" << std::endl;
+        return;
+    }
+    if (cudaStreamSynchronize(stream) != cudaSuccess)
+        std::cerr << "runMarchingCubesCUDA: stream sync failed" << std::endl;
+}
+
+inline int copyMarchingCubesTriangleCount(const MarchingCubesOutput& output) {
+    int64_t n = 0;
+    if (!output.handle || vsg_mc_triangle_count(output.handle, &n) != VSG_OK) return 0;
+    return n > 2147483647 ? 2147483647 : (int)n;
+}

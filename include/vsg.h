@@ -102,6 +102,8 @@ typedef struct vsg_stats {
     uint32_t render_jumps;           /* last render: O(1) jumps over skipped runs */
     uint32_t render_singles;         /* last render: samples evaluated at a skip-cell boundary */
     uint32_t render_blocks_read;     /* last render with timing enabled: distinct blocks read */
+    uint32_t render_lane_iters;      /* last render: march iterations summed over rays */
+    uint32_t render_warp_iters;      /* last render: per-warp maximum iterations, summed */
     uint32_t flags;              /* VSG_FLAG_* (sticky since reset) */
     uint32_t fast_division;      /* 1: the ray caster divides by the voxel size with a
                                     product + correction verified exhaustively against
@@ -180,6 +182,38 @@ VSG_API int vsg_renderer_outputs(const vsg_renderer* r, float** depth, float** p
 VSG_API int vsg_renderer_download(const vsg_renderer* r, float* depth, float* position, float* color,
                           float* normal);
 
+/* ---- marching cubes -----------------------------------------------------
+ * Replaces allocateMarchingCubesOutput / freeMarchingCubesOutput /
+ * runMarchingCubesCUDA / copyMarchingCubesTriangleCount (MarchingCubes.h:
+ * 34-58, MarchingCubes.cu:472-571).  Triangle soup over every allocated
+ * block, cubes inside one block only, vertices float3[3 * max_triangles] and
+ * per-vertex face normals float3[3 * max_triangles] on the device. */
+typedef struct vsg_mc_output vsg_mc_output;
+
+/* allocateMarchingCubesOutput: buffers for max_triangles triangles, on the
+ * current device. */
+VSG_API int vsg_mc_output_create(int max_triangles, vsg_mc_output** out);
+/* freeMarchingCubesOutput */
+VSG_API int vsg_mc_output_destroy(vsg_mc_output* m);
+/* runMarchingCubesCUDA: extract the iso surface (iso: SDF level, 0 for the
+ * surface; voxel_size <= 0 takes the scene's, as MarchingCubesParams'
+ * voxelSize does).  Triangles go out in an unspecified order, each block's
+ * as one range; the first max_triangles of them are written.
+ * Stream-ordered; does not synchronise (the reference does). */
+VSG_API int vsg_mc_run(vsg_scene* s, vsg_mc_output* m, float iso, float voxel_size, vsg_stream_t stream);
+/* copyMarchingCubesTriangleCount: the surface's triangle count, which may
+ * exceed the capacity (then only max_triangles were written).  Synchronises. */
+VSG_API int vsg_mc_triangle_count(const vsg_mc_output* m, int64_t* count);
+/* Device buffers (MarchingCubesOutput's d_vertices / d_normals /
+ * d_triangleCount, the count as int clamped to INT_MAX); any pointer may be
+ * NULL. */
+VSG_API int vsg_mc_output_buffers(const vsg_mc_output* m, float** vertices, float** normals, int** count_dev,
+                                  int* max_triangles);
+/* Copy the written triangles to host memory: vertices / normals float[9 *
+ * min(count, max_triangles)] (either may be NULL); count as in
+ * vsg_mc_triangle_count.  Synchronises. */
+VSG_API int vsg_mc_download(const vsg_mc_output* m, float* vertices, float* normals, int64_t* count);
+
 /* ---- batched form: many independent scenes advanced together ----------
  * No counterpart in the reference (it fuses one scan at a time).  A batch
  * holds up to 256 scenes (each its own hash table and voxel pool, any
@@ -214,7 +248,8 @@ VSG_API int vsg_batch_autotune(vsg_batch* b, int enable);
 
 /* Per-kernel device time (ms) since the last vsg_timing_reset, measured
  * with CUDA events on the launching stream when timing is enabled.
- * Slots: 0 alloc, 1 integrate, 2 render, 3 select. counts[i] = launches.
+ * Slots: 0 alloc, 1 integrate, 2 render, 3 select, 4 marching cubes.
+ * counts[i] = launches.
  * With timing enabled renders also count the distinct blocks they read
  * (vsg_stats.render_blocks_read). */
 VSG_API int vsg_timing_enable(vsg_scene* s, int enable);

@@ -57,6 +57,8 @@ def lib():
                                       _p, _p]
         L.orc_render_touched_blocks.restype = _i64
         L.orc_render_touched_blocks.argtypes = [_p, _i, _i, _p, _p, _f, _f, _f, _f, _f, _f]
+        L.orc_marching_cubes.restype = _i64
+        L.orc_marching_cubes.argtypes = [_p, _p, _f, _f, _i64, _p, _p]
         L.orc_export.argtypes = [_p, _p, _p]
         L.orc_import.argtypes = [_p, _i64, _p, _p]
         L.orc_bucket_hash.restype = ctypes.c_uint32
@@ -137,6 +139,18 @@ class OracleScene:
         cam = np.array([T[3], T[7], T[11]], np.float32)
         return int(self.L.orc_render_touched_blocks(self.h, W, H, _ptr(cam), _ptr(T), _f(fx), _f(fy),
                                                     _f(cx), _f(cy), _f(min_depth), _f(max_depth)))
+
+    def marching_cubes(self, table, iso: float, voxel: float, max_tris: int):
+        """Triangle soup of MarchingCubes.cu:354-467 with the given 256x16 case
+        table: (total count, vertices (m,3,3) f32, normals (m,3,3) f32),
+        m = min(total, max_tris)."""
+        tab = np.ascontiguousarray(table, dtype=np.uint8).reshape(256, 16)
+        v = np.zeros((max(max_tris, 1), 3, 3), np.float32)
+        n = np.zeros((max(max_tris, 1), 3, 3), np.float32)
+        total = int(self.L.orc_marching_cubes(self.h, _ptr(tab), _f(iso), _f(voxel), int(max_tris), _ptr(v),
+                                              _ptr(n)))
+        m = min(total, max_tris)
+        return total, v[:m].copy(), n[:m].copy()
 
     def export(self, with_voxels: bool = True):
         """(coords (n,3) int32 sorted by x,y,z; voxels (n,512) structured)."""

@@ -635,6 +635,100 @@ int64_t orc_render_touched_blocks(const orc_scene* s, int W, int H, const float*
     return n;
 }
 
+/* --------------------------------------------------------- marching cubes */
+
+/* Corner k of a cube at offset ((k ^ k>>1) & 1, k>>1 & 1, k>>2) and edge e
+ * from corner MC_EDGE[e][0] to MC_EDGE[e][1]: the numbering of
+ * MarchingCubes.cu:264-285 (MC_CORNER_OFFSET_HOST, MC_EDGE_CONNECTION_HOST). */
+static const int MC_EDGE[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                   {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+
+/* vertexInterp, MarchingCubes.cu:313-327 */
+static void mc_interp(float iso, const float* p1, const float* p2, float v1, float v2, float* o) {
+    const float denom = v2 - v1;
+    if (fabsf(denom) < 1e-6f) {
+        for (int i = 0; i < 3; i++) o[i] = 0.5f * (p1[i] + p2[i]);
+        return;
+    }
+    float mu = (iso - v1) / denom;
+    mu = fminf(fmaxf(mu, 0.0f), 1.0f);
+    for (int i = 0; i < 3; i++) o[i] = p1[i] + mu * (p2[i] - p1[i]);
+}
+
+/* computeNormal, MarchingCubes.cu:329-350 */
+static void mc_normal(const float* v0, const float* v1, const float* v2, float* n) {
+    const float a[3] = {v1[0] - v0[0], v1[1] - v0[1], v1[2] - v0[2]};
+    const float b[3] = {v2[0] - v0[0], v2[1] - v0[1], v2[2] - v0[2]};
+    n[0] = a[1] * b[2] - a[2] * b[1];
+    n[1] = a[2] * b[0] - a[0] * b[2];
+    n[2] = a[0] * b[1] - a[1] * b[0];
+    const float len = sqrtf(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    if (len > 1e-6f) {
+        const float inv = 1.0f / len;
+        n[0] *= inv;
+        n[1] *= inv;
+        n[2] *= inv;
+    } else {
+        n[0] = n[1] = n[2] = 0.0f;
+    }
+}
+
+/* marchingCubesKernel (MarchingCubes.cu:354-467) over every allocated block
+ * (the reference's compact list holds all of them, VoxelScene.cu:1275-1300),
+ * cubes with local x, y, z < 7 only (:379).  `tab` is a 256 x 16 case table
+ * (triangle edge indices, count in entry 15).  Triangles go out in block
+ * order, cube order (z, y, x), table order: 9 floats of vertices and 9 of
+ * normals (the face normal three times) each, the first max_tris of them
+ * written.  Returns the total triangle count, like the reference's counter. */
+int64_t orc_marching_cubes(const orc_scene* s, const uint8_t* tab, float iso, float voxel, int64_t max_tris,
+                           float* verts, float* norms) {
+    int64_t total = 0;
+    const float extent = (float)BS * voxel;
+    for (int64_t b = 0; b < s->n; b++) {
+        int32_t bc[3];
+        unpack_key(s->keys[b], bc);
+        const float base[3] = {(float)bc[0] * extent, (float)bc[1] * extent, (float)bc[2] * extent};
+        const ovox* vb = s->vox + b * VPB;
+        for (int lz = 0; lz < BS - 1; lz++)
+            for (int ly = 0; ly < BS - 1; ly++)
+                for (int lx = 0; lx < BS - 1; lx++) {
+                    float val[8], pos[8][3];
+                    int ci = 0;
+                    for (int k = 0; k < 8; k++) {
+                        const int v[3] = {lx + ((k ^ (k >> 1)) & 1), ly + ((k >> 1) & 1), lz + (k >> 2)};
+                        val[k] = vb[(v[2] * BS + v[1]) * BS + v[0]].sdf;
+                        for (int i = 0; i < 3; i++) pos[k][i] = base[i] + ((float)v[i] + 0.5f) * voxel;
+                        if (val[k] < iso) ci |= 1 << k;
+                    }
+                    if (ci == 0 || ci == 255) continue; /* empty edge mask */
+                    float vl[12][3];
+                    for (int e = 0; e < 12; e++) {
+                        const int c0 = MC_EDGE[e][0], c1 = MC_EDGE[e][1];
+                        if (((ci >> c0) & 1) != ((ci >> c1) & 1))
+                            mc_interp(iso, pos[c0], pos[c1], val[c0], val[c1], vl[e]);
+                    }
+                    const uint8_t* row = tab + ci * 16;
+                    for (int t = 0; t < row[15]; t++, total++) {
+                        if (total >= max_tris) continue;
+                        const float* p0 = vl[row[3 * t]];
+                        const float* p1 = vl[row[3 * t + 1]];
+                        const float* p2 = vl[row[3 * t + 2]];
+                        float n[3];
+                        mc_normal(p0, p1, p2, n);
+                        float* ov = verts + total * 9;
+                        float* on = norms + total * 9;
+                        for (int i = 0; i < 3; i++) {
+                            ov[i] = p0[i];
+                            ov[3 + i] = p1[i];
+                            ov[6 + i] = p2[i];
+                            on[i] = on[3 + i] = on[6 + i] = n[i];
+                        }
+                    }
+                }
+    }
+    return total;
+}
+
 /* ------------------------------------------------------- export / import */
 
 static int cmp_key3(const void* a, const void* b) {

@@ -193,6 +193,8 @@ int vsg_scene_stats(vsg_scene* s, vsg_stats* out) {
     out->render_jumps = f.jumps;
     out->render_singles = f.singles;
     out->render_blocks_read = f.blocks_read;
+    out->render_lane_iters = f.lane_iters;
+    out->render_warp_iters = f.warp_iters;
     out->flags = c.flags;
     out->fast_division = s->impl.dev.div_fast ? 1u : 0u;
     return VSG_OK;

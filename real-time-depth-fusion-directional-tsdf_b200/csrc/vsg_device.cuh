@@ -96,7 +96,9 @@ struct FrameCounters {
     uint32_t jumps;          // O(1) jumps over runs of skipped samples
     uint32_t singles;        // samples evaluated at a cell boundary (no jump)
     uint32_t blocks_read;    // distinct blocks the last render read (instrumented runs)
-    uint32_t pad2[3];
+    uint32_t lane_iters;     // march loop iterations summed over rays (x1/32 per warp)
+    uint32_t warp_iters;     // per-warp maximum iterations summed over warps
+    uint32_t pad2;
 };
 
 struct SceneDev {

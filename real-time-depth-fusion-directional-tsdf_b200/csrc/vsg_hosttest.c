@@ -17,3 +17,8 @@ float vsg_test_chain_serial(float r, float h, float target, int max_steps, int* 
     *steps = n;
     return r;
 }
+
+#include "vsg_mc_table.h"
+
+/* the generated marching-cubes table, 256 x 16 bytes */
+void vsg_test_mc_table(unsigned char* out) { vsg_mc_build_table((unsigned char(*)[16])out); }

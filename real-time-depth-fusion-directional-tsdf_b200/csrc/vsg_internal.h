@@ -8,7 +8,14 @@
 
 namespace vsg {
 
-enum TimingSlot { kSlotAlloc = 0, kSlotIntegrate = 1, kSlotRender = 2, kSlotSelect = 3, kNumSlots = 8 };
+enum TimingSlot {
+    kSlotAlloc = 0,
+    kSlotIntegrate = 1,
+    kSlotRender = 2,
+    kSlotSelect = 3,
+    kSlotMarchingCubes = 4,
+    kNumSlots = 8
+};
 
 struct Timing {
     bool enabled = false;

@@ -368,13 +368,16 @@ static __device__ __forceinline__ void render_pixel(const RenderArgs& a, int x, 
         }
         const unsigned am = __activemask();
         const unsigned hm = __ballot_sync(am, hit);
-        uint32_t nf = n_full, ns = n_skip, nj = n_jump, n1 = n_single;
+        const uint32_t it = n_full + n_jump;
+        const uint32_t it_max = __reduce_max_sync(am, it);
+        uint32_t nf = n_full, ns = n_skip, nj = n_jump, n1 = n_single, ni = it;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             nf += __shfl_xor_sync(am, nf, o);
             ns += __shfl_xor_sync(am, ns, o);
             nj += __shfl_xor_sync(am, nj, o);
             n1 += __shfl_xor_sync(am, n1, o);
+            ni += __shfl_xor_sync(am, ni, o);
         }
         if ((threadIdx.x & 31) == (__ffs(am) - 1)) {
             atomicAdd(&s.frame->hits, (uint32_t)__popc(hm));
@@ -383,6 +386,8 @@ static __device__ __forceinline__ void render_pixel(const RenderArgs& a, int x, 
             atomicAdd(&s.frame->samples_skipped, ns);
             atomicAdd(&s.frame->jumps, nj);
             atomicAdd(&s.frame->singles, n1);
+            atomicAdd(&s.frame->lane_iters, ni);
+            atomicAdd(&s.frame->warp_iters, it_max);
         }
     }
     a.depth[pi] = out_depth;
@@ -399,6 +404,8 @@ static __device__ __forceinline__ void render_begin(FrameCounters* f) {
     f->jumps = 0u;
     f->singles = 0u;
     f->blocks_read = 0u;
+    f->lane_iters = 0u;
+    f->warp_iters = 0u;
 }
 
 }  // namespace vsg

@@ -27,6 +27,8 @@ EXPORTS = [
     "vsg_render", "vsg_render_hostpose", "vsg_renderer_outputs", "vsg_renderer_download",
     "vsg_timing_enable", "vsg_timing_read", "vsg_timing_reset", "vsg_version",
     "vsg_batch_create", "vsg_batch_destroy", "vsg_batch_step", "vsg_batch_autotune",
+    "vsg_mc_output_create", "vsg_mc_output_destroy", "vsg_mc_run", "vsg_mc_triangle_count",
+    "vsg_mc_output_buffers", "vsg_mc_download",
 ]
 
 
@@ -56,7 +58,8 @@ class Stats(ctypes.Structure):
         "allocated_blocks", "free_blocks", "high_water", "chain_nodes_used", "integrated_frames",
         "frame_valid_pixels", "frame_new_blocks", "frame_visible_blocks", "frame_updated_blocks",
         "frame_updated_voxels", "render_hits", "render_misses", "render_samples_full",
-        "render_samples_skipped", "render_jumps", "render_singles", "render_blocks_read", "flags",
+        "render_samples_skipped", "render_jumps", "render_singles", "render_blocks_read",
+        "render_lane_iters", "render_warp_iters", "flags",
         "fast_division")]
 
     def as_dict(self) -> dict:
@@ -100,6 +103,13 @@ def lib() -> ctypes.CDLL:
         L.vsg_batch_destroy.argtypes = [_P]
         L.vsg_batch_step.argtypes = [_P, ctypes.POINTER(BatchFrame), _I, _P]
         L.vsg_batch_autotune.argtypes = [_P, _I]
+        L.vsg_mc_output_create.argtypes = [_I, ctypes.POINTER(_P)]
+        L.vsg_mc_output_destroy.argtypes = [_P]
+        L.vsg_mc_run.argtypes = [_P, _P, _F, _F, _P]
+        L.vsg_mc_triangle_count.argtypes = [_P, ctypes.POINTER(ctypes.c_int64)]
+        L.vsg_mc_output_buffers.argtypes = [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
+                                            ctypes.POINTER(_I)]
+        L.vsg_mc_download.argtypes = [_P, _P, _P, ctypes.POINTER(ctypes.c_int64)]
         _lib = L
     return _lib
 
@@ -257,6 +267,53 @@ class Renderer:
         check("vsg_renderer_download", self.L.vsg_renderer_download(self.h, _hptr(d), _hptr(p), _hptr(c), _hptr(nm)))
         assert n == d.size
         return {"depth": d, "position": p, "color": c, "normal": nm}
+
+
+class MarchingCubes:
+    """MarchingCubesOutput + runMarchingCubesCUDA over the C ABI (vsg_mc_*)."""
+
+    def __init__(self, max_triangles: int):
+        self.L = lib()
+        h = _P()
+        check("vsg_mc_output_create", self.L.vsg_mc_output_create(int(max_triangles), ctypes.byref(h)))
+        self.h = h
+        self.max_triangles = int(max_triangles)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.vsg_mc_output_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, scene: "Scene", iso: float = 0.0, voxel_size: float = 0.0, stream=None):
+        check("vsg_mc_run", self.L.vsg_mc_run(scene.h, self.h, _F(iso), _F(voxel_size), _stream(stream)))
+
+    def count(self) -> int:
+        n = ctypes.c_int64()
+        check("vsg_mc_triangle_count", self.L.vsg_mc_triangle_count(self.h, ctypes.byref(n)))
+        return int(n.value)
+
+    def buffers(self) -> dict:
+        v, nm, c, m = _P(), _P(), _P(), _I()
+        check("vsg_mc_output_buffers", self.L.vsg_mc_output_buffers(self.h, ctypes.byref(v), ctypes.byref(nm),
+                                                                    ctypes.byref(c), ctypes.byref(m)))
+        return {"vertices": int(v.value or 0), "normals": int(nm.value or 0), "count": int(c.value or 0),
+                "max_triangles": int(m.value)}
+
+    def download(self):
+        """(total count, vertices (m,3,3) f32, normals (m,3,3) f32), m = min(count, capacity)."""
+        n = self.count()
+        m = min(n, self.max_triangles)
+        v = np.zeros((max(m, 1), 3, 3), np.float32)
+        nm = np.zeros((max(m, 1), 3, 3), np.float32)
+        c = ctypes.c_int64()
+        check("vsg_mc_download", self.L.vsg_mc_download(self.h, _hptr(v), _hptr(nm), ctypes.byref(c)))
+        return int(c.value), v[:m], nm[:m]
 
 
 class Batch:

@@ -32,6 +32,18 @@ def synth_mod():
 
 
 @pytest.fixture(scope="session")
+def hosttest_lib(tmp_path_factory):
+    """Host (gcc) build of the library's header-only helpers, for CPU tests."""
+    import ctypes
+    import subprocess
+
+    out = str(tmp_path_factory.mktemp("hosttest") / "libvsg_hosttest.so")
+    subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", out,
+                    os.path.join(PKG, "csrc", "vsg_hosttest.c"), "-lm"], check=True)
+    return ctypes.CDLL(out)
+
+
+@pytest.fixture(scope="session")
 def cuda():
     import torch
 

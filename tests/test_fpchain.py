@@ -2,22 +2,14 @@
 against serial additions: it must land on the identical float after the
 identical number of steps.  Host build of the same header; no GPU."""
 import ctypes
-import os
-import subprocess
 
 import numpy as np
 import pytest
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-CSRC = os.path.join(ROOT, "real-time-depth-fusion-directional-tsdf_b200", "csrc")
-
 
 @pytest.fixture(scope="module")
-def L(tmp_path_factory):
-    out = str(tmp_path_factory.mktemp("hosttest") / "libvsg_hosttest.so")
-    subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", out,
-                    os.path.join(CSRC, "vsg_hosttest.c"), "-lm"], check=True)
-    lib = ctypes.CDLL(out)
+def L(hosttest_lib):
+    lib = hosttest_lib
     for f in (lib.vsg_test_chain_advance, lib.vsg_test_chain_serial):
         f.restype = ctypes.c_float
         f.argtypes = [ctypes.c_float] * 3 + [ctypes.c_int, ctypes.POINTER(ctypes.c_int)]

@@ -1,0 +1,177 @@
+"""Marching-cubes case table (no GPU).
+
+- The library's generator (csrc/vsg_mc_table.h, host build) and the
+  independent numpy restatement (mc_cases.py) give the same table.
+- Every case crosses exactly the edges whose corners differ (the edge table
+  the reference indexes, MarchingCubes.cu:13-45), uses at most 5 triangles,
+  and its triangles' face normals point towards the inside corners.
+- The surface is closed: on random sign grids every directed segment between
+  edge vertices is matched by as many reversed ones, except on the border.
+- Against the reference's own table (read as text when the reference source
+  tree is present; skipped otherwise): its edge table equals the computed
+  one; its triangle table is malformed (209 of 256 rows; rows whose edges are
+  not the crossed edges of their case); every well-formed row has the same
+  face segments, with the same orientation, as the generated table.
+"""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import mc_cases
+
+REF_MC = "/root/reference/VoxelSG/src/MarchingCubes.cu"
+
+
+@pytest.fixture(scope="module")
+def c_table(hosttest_lib):
+    out = np.zeros((256, 16), np.uint8)
+    hosttest_lib.vsg_test_mc_table.argtypes = [ctypes.c_void_p]
+    hosttest_lib.vsg_test_mc_table(out.ctypes.data)
+    return out
+
+
+def test_c_generator_matches_independent_restatement(c_table):
+    assert np.array_equal(c_table, mc_cases.table())
+
+
+def test_cases_cross_exactly_the_sign_change_edges(c_table):
+    for c in range(256):
+        n = int(c_table[c, 15])
+        assert n <= 5
+        es = set(int(e) for e in c_table[c, :3 * n])
+        want = {e for e in range(12) if (mc_cases.edge_mask(c) >> e) & 1}
+        assert es == want, c
+        assert all(v == 0xFF for v in c_table[c, 3 * n:15])
+    assert c_table[0, 15] == 0 and c_table[255, 15] == 0
+
+
+def _edge_point(e, vals):
+    a, b = mc_cases.EDGES[e]
+    pa, pb = np.array(mc_cases.CORNERS[a], float), np.array(mc_cases.CORNERS[b], float)
+    mu = (0.0 - vals[a]) / (vals[b] - vals[a])
+    return pa + mu * (pb - pa)
+
+
+def _newell(pts):
+    n = np.zeros(3)
+    for i in range(len(pts)):
+        p, q = pts[i], pts[(i + 1) % len(pts)]
+        n += np.cross(p, q)
+    return 0.5 * n
+
+
+def test_normals_point_inside(c_table):
+    """The region where the field is below the iso value is closed off by the
+    triangles and the inside parts of the cube faces; with triangle normals
+    pointing inside, the triangles' area vectors sum to the outward area
+    vectors of those face parts (divergence theorem, exact for planar
+    pieces)."""
+    rng = np.random.default_rng(3)
+    for c in range(1, 255):
+        vals = np.where([(c >> k) & 1 for k in range(8)], -1.0, 1.0) * rng.uniform(0.2, 1.0, 8)
+        tri_sum = np.zeros(3)
+        for t in range(int(c_table[c, 15])):
+            p = [_edge_point(int(x), vals) for x in c_table[c, 3 * t:3 * t + 3]]
+            tri_sum += 0.5 * np.cross(p[1] - p[0], p[2] - p[0])
+        face_sum = np.zeros(3)
+        for cyc in mc_cases.FACES:
+            ins = [(c >> k) & 1 for k in cyc]
+            P = [np.array(mc_cases.CORNERS[k], float) for k in cyc]
+            if all(ins):
+                face_sum += _newell(P)
+                continue
+            for i in range(4):
+                if ins[i] and not ins[i - 1]:
+                    j = i
+                    pts = [_edge_point(mc_cases._EID[(cyc[i - 1], cyc[i])], vals)]
+                    while True:
+                        pts.append(P[j])
+                        if not ins[(j + 1) % 4]:
+                            break
+                        j = (j + 1) % 4
+                    pts.append(_edge_point(mc_cases._EID[(cyc[j], cyc[(j + 1) % 4])], vals))
+                    face_sum += _newell(pts)
+        assert np.allclose(tri_sum, face_sum, atol=1e-9), c
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_surface_is_closed_across_cubes(c_table, seed):
+    rng = np.random.default_rng(seed)
+    N = 6
+    inside = rng.random((N + 1, N + 1, N + 1)) < 0.5
+    seg = {}
+    for z in range(N):
+        for y in range(N):
+            for x in range(N):
+                c = 0
+                for k, (ox, oy, oz) in enumerate(mc_cases.CORNERS):
+                    c |= int(inside[x + ox, y + oy, z + oz]) << k
+
+                def gid(e):  # global id of the grid edge under cube edge e
+                    a, b = mc_cases.EDGES[e]
+                    pa = (x + mc_cases.CORNERS[a][0], y + mc_cases.CORNERS[a][1], z + mc_cases.CORNERS[a][2])
+                    pb = (x + mc_cases.CORNERS[b][0], y + mc_cases.CORNERS[b][1], z + mc_cases.CORNERS[b][2])
+                    return tuple(sorted((pa, pb)))
+
+                for t in range(int(c_table[c, 15])):
+                    tri = [gid(int(e)) for e in c_table[c, 3 * t:3 * t + 3]]
+                    for i in range(3):
+                        d = (tri[i], tri[(i + 1) % 3])
+                        seg[d] = seg.get(d, 0) + 1
+
+    def on_border(g):
+        return any(all(p[i] == v for p in g) for i in range(3) for v in (0, N))
+
+    # closed and consistently oriented: every directed segment is matched by
+    # as many reversed ones (chords that two cubes both lay in their shared
+    # face plane appear twice each way), except on the grid's border
+    for (a, b), n in seg.items():
+        if on_border(a) and on_border(b):
+            continue
+        assert n == seg.get((b, a), 0), (a, b)
+
+
+def _reference_tables():
+    if not os.path.exists(REF_MC):
+        pytest.skip("reference source tree not present")
+    src = open(REF_MC).read()
+    et = src[src.index("MC_EDGE_TABLE_HOST[256]"):]
+    et = et[et.index("{") + 1:et.index("};")]
+    edge = [int(x, 16) for x in re.findall(r"0x[0-9a-fA-F]+", et)]
+    tt = src[src.index("MC_TRI_TABLE_HOST"):]
+    tt = tt[tt.index("{") + 1:]
+    tt = tt[:tt.index("};")]
+    rows = [[int(v) for v in r.split(",") if v.strip()] for r in re.findall(r"\{([^{}]*)\}", tt)]
+    return edge, rows
+
+
+def test_reference_edge_table_equals_computed():
+    edge, _ = _reference_tables()
+    assert len(edge) == 256
+    assert edge == [mc_cases.edge_mask(c) for c in range(256)]
+
+
+def test_reference_triangle_table_well_formed_rows_agree(c_table):
+    _, rows = _reference_tables()
+    assert len(rows) == 209  # MC_TRI_TABLE_HOST[256][16]: rows 209..255 are zero-filled
+    good, bad = [], []
+    for c, r in enumerate(rows):
+        k = r.index(-1) if -1 in r else len(r)
+        es = r[:k]
+        if k % 3 == 0 and set(es) == {e for e in range(12) if (mc_cases.edge_mask(c) >> e) & 1}:
+            good.append(c)
+        else:
+            bad.append(c)
+    assert len(good) == 186 and bad[0] == 140, bad
+    same_tris = 0
+    for c in good:
+        r = rows[c]
+        ref = [tuple(r[i:i + 3]) for i in range(0, r.index(-1), 3)]
+        mine = [tuple(int(e) for e in c_table[c, 3 * t:3 * t + 3]) for t in range(int(c_table[c, 15]))]
+        assert mc_cases.boundary(mine) == mc_cases.boundary(ref), c
+        canon = lambda t: min(t[i:] + t[:i] for i in range(3))
+        same_tris += sorted(map(canon, mine)) == sorted(map(canon, ref))
+    assert same_tris == 85
