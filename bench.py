@@ -274,6 +274,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind},
             "clocks": clk.summary()}
+    line["marching_cubes"] = mc_measure(sc, peak)
     if not args.no_e2e:
         line["e2e"] = e2e(args, frames, K, sc, rr)
     if not args.no_batched:
@@ -286,6 +287,33 @@ def run_ours(args):
     rr.close()
     if dist:
         dist.destroy_process_group()
+
+
+def mc_measure(sc, peak: float, reps: int = 10) -> dict:
+    """Marching cubes over the scene as the timed step left it (the 30-frame
+    volume): device time per launch from the library's event ring, triangle
+    count, and algorithmic bytes = SDF of every block holding a weighted voxel
+    (4 B x 512) + 72 B per triangle written (3 vertices + 3 normals, float3)."""
+    import vsg
+
+    mc = vsg.MarchingCubes(4_000_000)
+    mc.run(sc)
+    sc.timing(True)
+    sc.timing_reset()
+    for _ in range(reps):
+        mc.run(sc)
+    kms, kcnt = sc.timing_read()
+    sc.timing(False)
+    sc.timing_reset()
+    n = mc.count()
+    _, vox = sc.export()
+    weighted = int((vox.reshape(-1, 512, 8)[:, :, 7] > 0).any(1).sum())
+    mc.close()
+    ms = float(kms[4] / max(kcnt[4], 1))
+    alg = weighted * 512 * 4 + min(n, 4_000_000) * 72
+    gbs = alg / (ms * 1e-3) / 1e9
+    return {"triangles": n, "blocks_with_weight": weighted, "ms_per_launch": ms, "alg_bytes": alg,
+            "achieved_gbs": gbs, "frac_of_peak": gbs / peak, "launches_timed": int(kcnt[4])}
 
 
 def run_batched(args) -> dict:

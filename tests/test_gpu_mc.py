@@ -39,12 +39,16 @@ def test_mc_matches_oracle(cuda, synth_mod, oracle_mod, iso, voxel_override):
     import vsg
 
     sc = _scene(vsg, cuda, synth_mod, 21, 160, 120, 4)
-    mc = vsg.MarchingCubes(400000)
+    probe = vsg.MarchingCubes(1)  # learn the count, then size the output to it
+    probe.run(sc, iso=iso, voxel_size=voxel_override)
+    need = probe.count()
+    probe.close()
+    mc = vsg.MarchingCubes(need)
     mc.run(sc, iso=iso, voxel_size=voxel_override)
     n, v, nrm = mc.download()
     o = _oracle_of(oracle_mod, sc, 0.004)
-    on, ov, onrm = o.marching_cubes(mc_cases.table(), iso, voxel_override if voxel_override > 0 else 0.004, 400000)
-    assert n == on > 1000
+    on, ov, onrm = o.marching_cubes(mc_cases.table(), iso, voxel_override if voxel_override > 0 else 0.004, need)
+    assert n == on == need == v.shape[0] > 1000
     assert np.array_equal(_rows(v, nrm), _rows(ov, onrm))
     # every normal is unit length or zero
     ln = np.linalg.norm(nrm[:, 0].astype(np.float64), axis=1)
@@ -66,7 +70,7 @@ def test_mc_capacity_and_empty(cuda, synth_mod, oracle_mod):
     mc.run(sc)
     n, v, nrm = mc.download()
     o = _oracle_of(oracle_mod, sc, 0.004)
-    on, ov, onrm = o.marching_cubes(mc_cases.table(), 0.0, 0.004, 400000)
+    on, ov, onrm = o.marching_cubes(mc_cases.table(), 0.0, 0.004, n)
     assert n == on > 64 and v.shape[0] == 64
     full = {r.tobytes() for r in _rows(ov, onrm)}
     assert all(r.tobytes() in full for r in _rows(v, nrm))  # the written ones are genuine
