@@ -214,6 +214,45 @@ VSG_API int vsg_mc_output_buffers(const vsg_mc_output* m, float** vertices, floa
  * vsg_mc_triangle_count.  Synchronises. */
 VSG_API int vsg_mc_download(const vsg_mc_output* m, float* vertices, float* normals, int64_t* count);
 
+/* ---- streaming between the scene and host memory -------------------------
+ * Replaces VoxelStreamingManager (VoxelStreamingManager.h:140-301): the
+ * host-side chunk grid (m_grid, :246) is a vsg_block_store; stream out =
+ * streamOutFindBlocksOnGPU + streamOutCopyToChunkGrid (VoxelStreamingManager.
+ * cpp:303-527), stream in = streamInCopyToGPUBuffer + streamInInsertToHashTable
+ * (:530-834).  Both synchronise.  Differences: stream-in really inserts (the
+ * reference's insertion is switched off), a block that is resident or stored
+ * twice is merged voxel by voxel (weights add, capped at 255; SDF and colour
+ * weight-averaged), no per-call cap and no chunk-grid bounds. */
+typedef struct vsg_block_store vsg_block_store;
+
+/* chunk_extent: g_streamingVoxelExtents (m, NULL = 1 m cubes). */
+VSG_API int vsg_store_create(const float chunk_extent[3], vsg_block_store** out);
+VSG_API int vsg_store_destroy(vsg_block_store* st);
+VSG_API int vsg_store_info(const vsg_block_store* st, uint64_t* n_blocks, uint64_t* n_chunks);
+/* Stored blocks as vsg_scene_export lays them out (sorted coords, 8-byte
+ * voxels; voxels may be NULL).  VSG_ERR_TOO_LARGE when more than max_blocks. */
+VSG_API int vsg_store_export(const vsg_block_store* st, int32_t* coords, uint8_t* voxels, uint64_t max_blocks,
+                             uint64_t* n_out);
+/* Checkpoint file of the stored blocks in the reference's streaming record
+ * layout (SDFBlockInfo + SDFBlock of 12-byte VoxelData, VoxelStreamingManager.h:
+ * 30-76) after a 32-byte header; load merges the file into the store. */
+VSG_API int vsg_store_save(const vsg_block_store* st, const char* path);
+VSG_API int vsg_store_load(vsg_block_store* st, const char* path);
+/* Move every block whose corner lies at distance >= radius from center into
+ * the store (deleted from the scene, pool blocks freed). */
+VSG_API int vsg_stream_out(vsg_scene* s, vsg_block_store* st, const float center[3], float radius, uint32_t* n_out,
+                           vsg_stream_t stream);
+/* Move the stored chunks that intersect the sphere back into the scene
+ * (radius < 0: every stored block).  VSG_ERR_TOO_LARGE, with nothing moved,
+ * when the free pool cannot hold them. */
+VSG_API int vsg_stream_in(vsg_scene* s, vsg_block_store* st, const float center[3], float radius, uint32_t* n_in,
+                          uint32_t* n_merged, vsg_stream_t stream);
+/* Whole-scene checkpoint in the same file format (no counterpart in the
+ * reference): save writes every allocated block; load inserts the file's
+ * blocks (merging into resident ones). */
+VSG_API int vsg_scene_save(vsg_scene* s, const char* path);
+VSG_API int vsg_scene_load(vsg_scene* s, const char* path, vsg_stream_t stream);
+
 /* ---- batched form: many independent scenes advanced together ----------
  * No counterpart in the reference (it fuses one scan at a time).  A batch
  * holds up to 256 scenes (each its own hash table and voxel pool, any

@@ -59,6 +59,10 @@ def lib():
         L.orc_render_touched_blocks.argtypes = [_p, _i, _i, _p, _p, _f, _f, _f, _f, _f, _f]
         L.orc_marching_cubes.restype = _i64
         L.orc_marching_cubes.argtypes = [_p, _p, _f, _f, _i64, _p, _p]
+        L.orc_stream_out.restype = _i64
+        L.orc_stream_out.argtypes = [_p, _p, _f, _p, _p]
+        L.orc_stream_in.argtypes = [_p, _i64, _p, _p]
+        L.orc_merge_voxels.argtypes = [_i64, _p, _p, _p]
         L.orc_export.argtypes = [_p, _p, _p]
         L.orc_import.argtypes = [_p, _i64, _p, _p]
         L.orc_bucket_hash.restype = ctypes.c_uint32
@@ -152,6 +156,22 @@ class OracleScene:
         m = min(total, max_tris)
         return total, v[:m].copy(), n[:m].copy()
 
+    def stream_out(self, center, radius: float):
+        """Remove the blocks whose corner is >= radius from center:
+        (coords (m,3) int32 sorted, voxel bytes (m, 4096) uint8)."""
+        n = self.num_blocks
+        c = _f32(center)
+        coords = np.zeros((max(n, 1), 3), np.int32)
+        vox = np.zeros((max(n, 1), 512 * 8), np.uint8)
+        m = int(self.L.orc_stream_out(self.h, _ptr(c), _f(radius), _ptr(coords), _ptr(vox)))
+        order = np.lexsort((coords[:m, 2], coords[:m, 1], coords[:m, 0]))
+        return coords[:m][order].copy(), vox[:m][order].copy()
+
+    def stream_in(self, coords, voxel_bytes):
+        coords = np.ascontiguousarray(coords, dtype=np.int32)
+        vb = np.ascontiguousarray(voxel_bytes, dtype=np.uint8)
+        self.L.orc_stream_in(self.h, coords.shape[0], _ptr(coords), _ptr(vb))
+
     def export(self, with_voxels: bool = True):
         """(coords (n,3) int32 sorted by x,y,z; voxels (n,512) structured)."""
         n = self.num_blocks
@@ -171,6 +191,76 @@ def split_voxels(vox_bytes: np.ndarray) -> dict:
     v = vox_bytes.reshape(-1, 512, 8)
     sdf = np.ascontiguousarray(v[:, :, :4]).view(np.float32).reshape(-1, 512)
     return {"sdf": sdf, "rgb": v[:, :, 4:7].copy(), "weight": v[:, :, 7].copy(), "raw": vox_bytes}
+
+
+def merge_voxels(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Voxel-by-voxel weighted merge of two blocks' 8-byte voxel records."""
+    a = np.ascontiguousarray(a, dtype=np.uint8)
+    b = np.ascontiguousarray(b, dtype=np.uint8)
+    out = np.zeros_like(a)
+    lib().orc_merge_voxels(a.size // 8, _ptr(a), _ptr(b), _ptr(out))
+    return out
+
+
+class ChunkStore:
+    """Host chunk grid of streamed-out blocks, restating VoxelStreamingManager
+    (VoxelStreamingManager.cpp:836-1140) in FP32: a block is filed under the
+    chunk of its corner (worldToChunks, :905-922); stream-in takes every
+    stored chunk in the box of ceil(r / extent) chunks around the centre's
+    chunk that passes isChunkInSphere (:962-991).  A block stored twice is
+    merged (merge_voxels)."""
+
+    def __init__(self, voxel: float, extent=(1.0, 1.0, 1.0)):
+        self.v = np.float32(voxel)
+        self.ext = [np.float32(e) for e in extent]
+        self.chunks = {}  # chunk -> {block coord: voxel bytes}
+
+    def chunk_of_world(self, p):
+        out = []
+        for i in range(3):
+            q = np.float32(np.float32(p[i]) / self.ext[i])
+            sg = np.float32(1.0) if q > 0 else (np.float32(-1.0) if q < 0 else np.float32(0.0))
+            out.append(int(np.float32(q + np.float32(sg * np.float32(0.5)))))  # truncation toward zero
+        return tuple(out)
+
+    def chunk_of_block(self, b):
+        return self.chunk_of_world([np.float32(np.float32(int(b[i]) * 8) * self.v) for i in range(3)])
+
+    def add(self, coords, vox):
+        for c, v in zip(coords, vox):
+            ch = self.chunks.setdefault(self.chunk_of_block(c), {})
+            k = tuple(int(x) for x in c)
+            ch[k] = merge_voxels(ch[k], v) if k in ch else np.array(v, np.uint8)
+
+    def in_sphere(self, c, center, radius):
+        f32 = np.float32
+        w = [f32(f32(c[i]) * self.ext[i]) for i in range(3)]
+        ce = max(self.ext)
+        cr = f32(f32(f32(0.5) * ce) * f32(np.sqrt(f32(3.0))))
+        d = [f32(w[i] - f32(center[i])) for i in range(3)]
+        dist = f32(np.sqrt(f32(f32(f32(d[0] * d[0]) + f32(d[1] * d[1])) + f32(d[2] * d[2]))))
+        return bool(f32(dist - cr) <= f32(radius))
+
+    def take(self, center, radius):
+        """Remove and return (coords, voxels) of the chunks a stream-in takes."""
+        if radius < 0:
+            keys = sorted(self.chunks)
+        else:
+            cc = self.chunk_of_world(center)
+            cr = [int(np.ceil(np.float32(np.float32(radius) / self.ext[i]))) for i in range(3)]
+            keys = sorted(k for k in self.chunks
+                          if all(abs(k[i] - cc[i]) <= cr[i] for i in range(3)) and self.in_sphere(k, center, radius))
+        coords, vox = [], []
+        for k in keys:
+            for c, v in self.chunks.pop(k).items():
+                coords.append(c)
+                vox.append(v)
+        return (np.array(coords, np.int32).reshape(-1, 3), np.array(vox, np.uint8).reshape(-1, 4096))
+
+    def export(self):
+        items = sorted((c, v) for ch in self.chunks.values() for c, v in ch.items())
+        return (np.array([c for c, _ in items], np.int32).reshape(-1, 3),
+                np.array([v for _, v in items], np.uint8).reshape(-1, 4096))
 
 
 def dda_blocks(start, end, voxel) -> np.ndarray:

@@ -729,6 +729,97 @@ int64_t orc_marching_cubes(const orc_scene* s, const uint8_t* tab, float iso, fl
     return total;
 }
 
+/* -------------------------------------------------------------- streaming */
+
+/* Weighted merge of two partial averages of one voxel (the library's rule
+ * for a block streamed in while resident, or stored twice; the reference
+ * has none): weights add (cap 255), SDF and colour are weight-averaged,
+ * colour truncated to 8 bits. */
+static ovox merge_vox(ovox a, ovox b) {
+    if (b.w == 0) return a;
+    if (a.w == 0) return b;
+    const float fa = (float)a.w, fb = (float)b.w, fw = (float)(a.w + b.w);
+    ovox o;
+    o.sdf = (a.sdf * fa + b.sdf * fb) / fw;
+    o.r = (uint8_t)(uint32_t)(((float)a.r * fa + (float)b.r * fb) / fw);
+    o.g = (uint8_t)(uint32_t)(((float)a.g * fa + (float)b.g * fb) / fw);
+    o.b = (uint8_t)(uint32_t)(((float)a.b * fa + (float)b.b * fb) / fw);
+    o.w = (uint8_t)(a.w + b.w > 255 ? 255 : a.w + b.w);
+    return o;
+}
+
+void orc_merge_voxels(int64_t n, const uint8_t* a, const uint8_t* b, uint8_t* out) {
+    for (int64_t i = 0; i < n; i++) {
+        ovox x, y;
+        memcpy(&x, a + 8 * i, 8);
+        memcpy(&y, b + 8 * i, 8);
+        const ovox o = merge_vox(x, y);
+        memcpy(out + 8 * i, &o, 8);
+    }
+}
+
+static void rebuild_map(orc_scene* s) {
+    for (int64_t i = 0; i < s->mcap; i++) s->mkeys[i] = KEY_EMPTY;
+    for (int64_t i = 0; i < s->n; i++) map_put_raw(s->mkeys, s->mvals, s->mcap, s->keys[i], (int32_t)i);
+}
+
+/* streamOutFindBlocksKernel_OPTIMIZED + streamOutCopyBlocksKernel
+ * (VoxelStreamingManager.cu:36-84, 258-355): every block whose corner
+ * (SDFBlockToWorld, :22-28: int coordinate * 8, then times the voxel size)
+ * lies at distance >= radius from c leaves the scene; its coordinates and
+ * voxels go to the output (scene order).  Returns how many. */
+int64_t orc_stream_out(orc_scene* s, const float* c, float radius, int32_t* coords, uint8_t* voxels) {
+    int64_t keep = 0, out = 0;
+    for (int64_t i = 0; i < s->n; i++) {
+        int32_t b[3];
+        unpack_key(s->keys[i], b);
+        const float dx = (float)(b[0] * BS) * s->voxel - c[0];
+        const float dy = (float)(b[1] * BS) * s->voxel - c[1];
+        const float dz = (float)(b[2] * BS) * s->voxel - c[2];
+        const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+        if (dist >= radius) {
+            memcpy(coords + 3 * out, b, sizeof(b));
+            memcpy(voxels + out * VPB * 8, s->vox + i * VPB, VPB * 8);
+            out++;
+        } else {
+            if (keep != i) {
+                s->keys[keep] = s->keys[i];
+                memcpy(s->vox + keep * VPB, s->vox + i * VPB, sizeof(ovox) * VPB);
+            }
+            keep++;
+        }
+    }
+    s->n = keep;
+    if (out) rebuild_map(s);
+    return out;
+}
+
+/* Stream-in insertion (streamInHashAllocKernel + streamInHashInitKernel,
+ * VoxelStreamingManager.cu:443-714): new positions get the stored voxels,
+ * resident ones merge them voxel by voxel. */
+void orc_stream_in(orc_scene* s, int64_t n, const int32_t* coords, const uint8_t* voxels) {
+    for (int64_t i = 0; i < n; i++) {
+        const int32_t* b = coords + 3 * i;
+        if (!in_range(b)) {
+            s->coord_range_drops++;
+            continue;
+        }
+        const uint64_t k = pack_key(b[0], b[1], b[2]);
+        const int64_t at = map_find(s, k);
+        if (at < 0) {
+            scene_add(s, k);
+            memcpy(s->vox + (s->n - 1) * VPB, voxels + i * VPB * 8, VPB * 8);
+        } else {
+            ovox* dst = s->vox + at * VPB;
+            for (int v = 0; v < VPB; v++) {
+                ovox x;
+                memcpy(&x, voxels + (i * VPB + v) * 8, 8);
+                dst[v] = merge_vox(dst[v], x);
+            }
+        }
+    }
+}
+
 /* ------------------------------------------------------- export / import */
 
 static int cmp_key3(const void* a, const void* b) {

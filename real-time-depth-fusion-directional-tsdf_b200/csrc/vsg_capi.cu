@@ -141,6 +141,7 @@ int vsg_scene_destroy(vsg_scene* s) {
     if (!s) return VSG_ERR_INVALID_ARG;
     cudaDeviceSynchronize();
     vsg::timing_destroy(&s->impl);
+    vsg::stream_stage_free(&s->impl);
     vsg::scene_free_device(&s->impl);
     delete s;
     return VSG_OK;

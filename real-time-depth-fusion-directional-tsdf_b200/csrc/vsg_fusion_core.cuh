@@ -53,9 +53,11 @@ static __device__ __forceinline__ void xform(const Pose& P, float x, float y, fl
 // Give a freshly inserted key storage.  entry_key / entry_ptr are the
 // fields of the slot (bucket entry or chain node) the caller now owns.
 // Heap pop as consumeHeap in VoxelScene.cu:183-195 (reference pops index
-// heapCounter, we pop free_count - 1: the same stack).
+// heapCounter, we pop free_count - 1: the same stack).  from_frame: the
+// block comes from a frame's allocation (counted as new this frame);
+// blocks streamed back in from host memory are not.
 static __device__ __noinline__ bool claim_block(const SceneDev& s, unsigned long long key, unsigned long long* entry_key,
-                            int* entry_ptr, int slot_index) {
+                            int* entry_ptr, int slot_index, bool from_frame = true) {
     int old = atomicSub(&s.ctr->free_count, 1);
     if (old <= 0) {
         atomicAdd(&s.ctr->free_count, 1);
@@ -81,13 +83,14 @@ static __device__ __noinline__ bool claim_block(const SceneDev& s, unsigned long
         const unsigned long long prev = atomicCAS(cell, kIdxEmpty, mine);
         if (prev != kIdxEmpty && prev != mine && prev != kIdxShared) atomicExch(cell, kIdxShared);
     }
-    atomicAdd(&s.frame->n_new, 1u);
+    if (from_frame) atomicAdd(&s.frame->n_new, 1u);
     return true;
 }
 
 // Search the overflow chain of bucket b for key; append it when absent.
 // Lock-free: a node is published by CAS on the tail link.
-static __device__ __noinline__ void chain_insert(const SceneDev& s, uint32_t b, unsigned long long key, bool insert) {
+static __device__ __noinline__ void chain_insert(const SceneDev& s, uint32_t b, unsigned long long key, bool insert,
+                                                 bool from_frame = true) {
     int* link = s.bucket_next + b;
     int mine = -1;
     const int base = (int)s.num_buckets * kBucketSlots;
@@ -109,7 +112,7 @@ static __device__ __noinline__ void chain_insert(const SceneDev& s, uint32_t b, 
             }
             int prev = atomicCAS(link, -1, mine);
             if (prev == -1) {
-                claim_block(s, key, &s.nodes[mine].key, &s.nodes[mine].ptr, base + mine);
+                claim_block(s, key, &s.nodes[mine].key, &s.nodes[mine].ptr, base + mine, from_frame);
                 return;
             }
             n = prev;
@@ -133,7 +136,8 @@ static __device__ bool chain_contains(const SceneDev& s, uint32_t b, unsigned lo
 }
 
 // Single-thread insert (fallback when the shared set overflows).
-static __device__ __noinline__ void insert_single(const SceneDev& s, unsigned long long key, int x, int y, int z) {
+static __device__ __noinline__ void insert_single(const SceneDev& s, unsigned long long key, int x, int y, int z,
+                                                  bool from_frame = true) {
     const uint32_t b = bucket_of(x, y, z, s.num_buckets);
     Entry* bk = s.buckets + (size_t)b * kBucketSlots;
     for (int it = 0; it < 4 * kBucketSlots; ++it) {
@@ -154,13 +158,13 @@ static __device__ __noinline__ void insert_single(const SceneDev& s, unsigned lo
         }
         if (found) return;
         if (first < 0) {
-            chain_insert(s, b, key, true);
+            chain_insert(s, b, key, true, from_frame);
             return;
         }
         if (seen == kKeyTomb && chain_contains(s, b, key)) return;
         unsigned long long prev = atomicCAS(&bk[first].key, seen, key);
         if (prev == seen) {
-            claim_block(s, key, &bk[first].key, &bk[first].ptr, (int)(b * kBucketSlots + first));
+            claim_block(s, key, &bk[first].key, &bk[first].ptr, (int)(b * kBucketSlots + first), from_frame);
             return;
         }
     }

@@ -38,6 +38,7 @@ struct Scene {
     int integ_ctas_per_sm = 2;
     uint32_t integrated_frames = 0;
     Timing timing;
+    void* stream_stage = nullptr;  // staging buffers of vsg_stream_* (created on first use)
 };
 
 struct Renderer {
@@ -63,6 +64,8 @@ int render_launch(Renderer* r, Scene* sc, const float cam[3], const float* pose_
                   float fx, float fy, float cx, float cy, float min_depth, float max_depth, cudaStream_t st);
 
 int verify_fixed_division(float v, bool* ok);
+
+void stream_stage_free(Scene* sc);
 
 void timing_begin(Scene* sc, int slot, cudaStream_t st);
 void timing_end(Scene* sc, int slot, cudaStream_t st);

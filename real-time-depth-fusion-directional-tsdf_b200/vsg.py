@@ -29,6 +29,8 @@ EXPORTS = [
     "vsg_batch_create", "vsg_batch_destroy", "vsg_batch_step", "vsg_batch_autotune",
     "vsg_mc_output_create", "vsg_mc_output_destroy", "vsg_mc_run", "vsg_mc_triangle_count",
     "vsg_mc_output_buffers", "vsg_mc_download",
+    "vsg_store_create", "vsg_store_destroy", "vsg_store_info", "vsg_store_export", "vsg_store_save",
+    "vsg_store_load", "vsg_stream_out", "vsg_stream_in", "vsg_scene_save", "vsg_scene_load",
 ]
 
 
@@ -110,6 +112,18 @@ def lib() -> ctypes.CDLL:
         L.vsg_mc_output_buffers.argtypes = [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
                                             ctypes.POINTER(_I)]
         L.vsg_mc_download.argtypes = [_P, _P, _P, ctypes.POINTER(ctypes.c_int64)]
+        _u64p = ctypes.POINTER(ctypes.c_uint64)
+        _u32p = ctypes.POINTER(ctypes.c_uint32)
+        L.vsg_store_create.argtypes = [_P, ctypes.POINTER(_P)]
+        L.vsg_store_destroy.argtypes = [_P]
+        L.vsg_store_info.argtypes = [_P, _u64p, _u64p]
+        L.vsg_store_export.argtypes = [_P, _P, _P, ctypes.c_uint64, _u64p]
+        L.vsg_store_save.argtypes = [_P, ctypes.c_char_p]
+        L.vsg_store_load.argtypes = [_P, ctypes.c_char_p]
+        L.vsg_stream_out.argtypes = [_P, _P, _P, _F, _u32p, _P]
+        L.vsg_stream_in.argtypes = [_P, _P, _P, _F, _u32p, _u32p, _P]
+        L.vsg_scene_save.argtypes = [_P, ctypes.c_char_p]
+        L.vsg_scene_load.argtypes = [_P, ctypes.c_char_p, _P]
         _lib = L
     return _lib
 
@@ -206,6 +220,26 @@ class Scene:
             self.h, _hptr(coords), _hptr(vox) if with_voxels else None, cnt, ctypes.byref(n)))
         return coords[:cnt], (vox[:cnt] if with_voxels else None)
 
+    def stream_out(self, store: "Store", center, radius: float, stream=None) -> int:
+        c = np.ascontiguousarray(np.asarray(center, np.float32).reshape(3))
+        n = ctypes.c_uint32()
+        check("vsg_stream_out", self.L.vsg_stream_out(self.h, store.h, _hptr(c), _F(radius), ctypes.byref(n),
+                                                      _stream(stream)))
+        return int(n.value)
+
+    def stream_in(self, store: "Store", center=None, radius: float = -1.0, stream=None) -> tuple[int, int]:
+        c = np.ascontiguousarray(np.asarray(center if center is not None else (0, 0, 0), np.float32).reshape(3))
+        n, m = ctypes.c_uint32(), ctypes.c_uint32()
+        check("vsg_stream_in", self.L.vsg_stream_in(self.h, store.h, _hptr(c), _F(radius), ctypes.byref(n),
+                                                    ctypes.byref(m), _stream(stream)))
+        return int(n.value), int(m.value)
+
+    def save(self, path: str):
+        check("vsg_scene_save", self.L.vsg_scene_save(self.h, str(path).encode()))
+
+    def load(self, path: str, stream=None):
+        check("vsg_scene_load", self.L.vsg_scene_load(self.h, str(path).encode(), _stream(stream)))
+
     def timing(self, enable: bool):
         check("vsg_timing_enable", self.L.vsg_timing_enable(self.h, int(enable)))
 
@@ -267,6 +301,48 @@ class Renderer:
         check("vsg_renderer_download", self.L.vsg_renderer_download(self.h, _hptr(d), _hptr(p), _hptr(c), _hptr(nm)))
         assert n == d.size
         return {"depth": d, "position": p, "color": c, "normal": nm}
+
+
+class Store:
+    """Host chunk grid of streamed-out blocks (vsg_block_store)."""
+
+    def __init__(self, chunk_extent=(1.0, 1.0, 1.0)):
+        self.L = lib()
+        h = _P()
+        e = np.ascontiguousarray(np.asarray(chunk_extent, np.float32).reshape(3))
+        check("vsg_store_create", self.L.vsg_store_create(_hptr(e), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.vsg_store_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> tuple[int, int]:
+        nb, nc = ctypes.c_uint64(), ctypes.c_uint64()
+        check("vsg_store_info", self.L.vsg_store_info(self.h, ctypes.byref(nb), ctypes.byref(nc)))
+        return int(nb.value), int(nc.value)
+
+    def export(self):
+        """(coords (n,3) int32 sorted, voxel bytes (n, 4096) uint8)."""
+        n = self.info()[0]
+        coords = np.zeros((max(n, 1), 3), np.int32)
+        vox = np.zeros((max(n, 1), 4096), np.uint8)
+        out = ctypes.c_uint64()
+        check("vsg_store_export", self.L.vsg_store_export(self.h, _hptr(coords), _hptr(vox), n, ctypes.byref(out)))
+        return coords[:n], vox[:n]
+
+    def save(self, path: str):
+        check("vsg_store_save", self.L.vsg_store_save(self.h, str(path).encode()))
+
+    def load(self, path: str):
+        check("vsg_store_load", self.L.vsg_store_load(self.h, str(path).encode()))
 
 
 class MarchingCubes:

@@ -1,0 +1,110 @@
+"""Host side of streaming, no GPU: the block store (vsg_store_*) reads and
+writes checkpoint files in the reference's streaming record layout
+(SDFBlockInfo {int3 pos, int ptr} + SDFBlock of 512 12-byte VoxelData
+{uchar3 color, uchar weight, float sdf, 2 flag bytes, 2 pad},
+VoxelStreamingManager.h:30-76, CUDAHashRef.h:22-45) and merges blocks stored
+twice with the oracle's rule."""
+import struct
+
+import numpy as np
+import pytest
+
+
+def _file(path, coords, vox8, voxel):
+    n = len(coords)
+    with open(path, "wb") as f:
+        f.write(b"VSGBLK01" + struct.pack("<IIQfI", 16, 12, n, voxel, 0))
+        for c in coords:
+            f.write(struct.pack("<4i", int(c[0]), int(c[1]), int(c[2]), -1))
+        for b in vox8:
+            v = b.reshape(512, 8)
+            rec = np.zeros((512, 12), np.uint8)
+            rec[:, 0:3] = v[:, 4:7]   # colour
+            rec[:, 3] = v[:, 7]       # weight
+            rec[:, 4:8] = v[:, 0:4]   # sdf
+            f.write(rec.tobytes())
+
+
+def _blocks(rng, n):
+    coords = rng.integers(-300, 300, size=(n, 3)).astype(np.int32)
+    coords = np.unique(coords, axis=0)
+    vox = np.zeros((len(coords), 512, 8), np.uint8)
+    sdf = rng.uniform(-0.02, 0.02, (len(coords), 512)).astype(np.float32)
+    vox[:, :, 0:4] = sdf.view(np.uint8).reshape(len(coords), 512, 4)
+    vox[:, :, 4:7] = rng.integers(0, 256, (len(coords), 512, 3))
+    w = rng.integers(0, 30, (len(coords), 512))
+    w[rng.random((len(coords), 512)) < 0.3] = 0
+    vox[:, :, 7] = w
+    vox[w == 0, 0:4] = 0  # unobserved voxels hold sdf 0, as in a scene
+    return coords, vox.reshape(len(coords), 4096)
+
+
+def test_store_reads_reference_records_and_writes_them_back(tmp_path, oracle_mod):
+    import vsg
+
+    rng = np.random.default_rng(5)
+    coords, vox = _blocks(rng, 200)
+    p = str(tmp_path / "a.vsgb")
+    _file(p, coords, vox, 0.004)
+    st = vsg.Store((0.5, 0.5, 0.5))
+    st.load(p)
+    gc, gv = st.export()
+    order = np.lexsort((coords[:, 2], coords[:, 1], coords[:, 0]))
+    assert np.array_equal(gc, coords[order]) and np.array_equal(gv, vox[order])
+    # and the library writes the same record layout
+    q = str(tmp_path / "b.vsgb")
+    st.save(q)
+    st2 = vsg.Store((0.5, 0.5, 0.5))
+    st2.load(q)
+    c2, v2 = st2.export()
+    assert np.array_equal(c2, gc) and np.array_equal(v2, gv)
+    raw = open(q, "rb").read()
+    assert raw[:8] == b"VSGBLK01" and len(raw) == 32 + len(coords) * (16 + 512 * 12)
+
+
+def test_store_merges_blocks_stored_twice(tmp_path, oracle_mod):
+    import vsg
+
+    rng = np.random.default_rng(6)
+    coords, vox_a = _blocks(rng, 50)
+    _, vox_b = _blocks(np.random.default_rng(7), 50)
+    vox_b = vox_b[:len(coords)]
+    pa, pb = str(tmp_path / "a.vsgb"), str(tmp_path / "b.vsgb")
+    _file(pa, coords, vox_a, 0.004)
+    _file(pb, coords, vox_b, 0.004)
+    st = vsg.Store()
+    st.load(pa)
+    st.load(pb)
+    assert st.info()[0] == len(coords)
+    gc, gv = st.export()
+    order = np.lexsort((coords[:, 2], coords[:, 1], coords[:, 0]))
+    want = np.stack([oracle_mod.merge_voxels(vox_a[i], vox_b[i]) for i in order])
+    assert np.array_equal(gv, want)
+
+
+def test_chunk_assignment_matches_oracle_store(tmp_path, oracle_mod):
+    import vsg
+
+    rng = np.random.default_rng(8)
+    coords, vox = _blocks(rng, 300)
+    p = str(tmp_path / "c.vsgb")
+    _file(p, coords, vox, 0.004)
+    st = vsg.Store((0.3, 0.2, 0.5))
+    st.load(p)
+    o = oracle_mod.ChunkStore(0.004, (0.3, 0.2, 0.5))
+    o.add(coords, vox)
+    assert st.info() == (len(coords), len(o.chunks))
+
+
+def test_store_rejects_bad_files(tmp_path):
+    import vsg
+
+    p = str(tmp_path / "bad.vsgb")
+    open(p, "wb").write(b"NOTVSG00" + bytes(24))
+    st = vsg.Store()
+    with pytest.raises(vsg.VsgError):
+        st.load(p)
+    with pytest.raises(vsg.VsgError):
+        st.load(str(tmp_path / "missing.vsgb"))
+    with pytest.raises(vsg.VsgError):
+        vsg.Store((0.0, 1.0, 1.0))
