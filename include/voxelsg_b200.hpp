@@ -16,6 +16,10 @@
  *   MarchingCubesParams, MarchingCubesOutput, allocateMarchingCubesOutput,
  *   freeMarchingCubesOutput, runMarchingCubesCUDA,
  *   copyMarchingCubesTriangleCount (MarchingCubes.h:7-58)
+ *   VoxelStreamingManager (VoxelStreamingManager.h:140-301): constructor,
+ *                         streamOut / streamIn, streamOutFindBlocksOnGPU,
+ *                         streamOutCopyToChunkGrid, streamInCopyToGPUBuffer,
+ *                         streamInInsertToHashTable
  * so that reference call sites compile unchanged against it.  Like the
  * reference, the methods print to stderr and return on bad input instead of
  * throwing; the only throw is GlobalParamsConfig::initialize.
@@ -360,3 +364,116 @@ inline int copyMarchingCubesTriangleCount(const MarchingCubesOutput& output) {
     if (!output.handle || vsg_mc_triangle_count(output.handle, &n) != VSG_OK) return 0;
     return n > 2147483647 ? 2147483647 : (int)n;
 }
+
+/* The reference's small vector types (its utils.h); define VSG_HAVE_VEC3
+ * before including this header to use your own. */
+#ifndef VSG_HAVE_VEC3
+struct vec3f {
+    float x = 0.0f, y = 0.0f, z = 0.0f;
+    vec3f() = default;
+    vec3f(float a, float b, float c) : x(a), y(b), z(c) {}
+};
+struct vec3i {
+    int x = 0, y = 0, z = 0;
+    vec3i() = default;
+    vec3i(int a, int b, int c) : x(a), y(b), z(c) {}
+};
+#endif
+
+/* VoxelStreamingManager.h:140-301 over vsg_stream_* and a vsg_block_store.
+ * Single host thread: the reference's auxiliary thread and its Win32 event
+ * handshakes are not reproduced (the multiThreaded flags are accepted and
+ * ignored), streamOutFindBlocksOnGPU already files the blocks in the host
+ * chunk grid (streamOutCopyToChunkGrid has nothing left to do), and
+ * streamInCopyToGPUBuffer only records the sphere that
+ * streamInInsertToHashTable then brings back.  The chunk grid has no bounds
+ * (gridDimensions / minGridPos are accepted, not enforced). */
+class VoxelStreamingManager {
+public:
+    VoxelStreamingManager(VoxelScene& sceneHashRef, Params& params, const vec3f& voxelExtends,
+                          const vec3i& gridDimensions, const vec3i& minGridPos, unsigned int initialChunkListSize,
+                          bool streamingEnabled)
+        : m_scene(&sceneHashRef), m_params(params) {
+        (void)gridDimensions;
+        (void)minGridPos;
+        (void)initialChunkListSize;
+        (void)streamingEnabled;
+        const float e[3] = {voxelExtends.x, voxelExtends.y, voxelExtends.z};
+        if (vsg_store_create(e, &m_store) != VSG_OK) {
+            std::cerr << "VoxelStreamingManager: invalid chunk extents" << std::endl;
+            m_store = nullptr;
+        }
+    }
+    ~VoxelStreamingManager() {
+        if (m_store) vsg_store_destroy(m_store);
+    }
+    VoxelStreamingManager(const VoxelStreamingManager&) = delete;
+    VoxelStreamingManager& operator=(const VoxelStreamingManager&) = delete;
+
+    void startMultiThreading() {}
+    void stopMultiThreading() {}
+
+    void streamOut(VoxelScene& scene, const float3& cameraPos, float radius) {
+        m_scene = &scene;
+        streamOutFindBlocksOnGPU(vec3f(cameraPos.x, cameraPos.y, cameraPos.z), radius, false, false);
+    }
+    void streamIn(VoxelScene& scene, const float3& cameraPos, float radius) {
+        m_scene = &scene;
+        streamInCopyToGPUBuffer(vec3f(cameraPos.x, cameraPos.y, cameraPos.z), radius, false, false);
+        streamInInsertToHashTable(false);
+    }
+
+    /* blocks at distance >= radius from sphereCenter leave the GPU */
+    void streamOutFindBlocksOnGPU(const vec3f& sphereCenter, float radius, bool useParts, bool multiThreaded) {
+        (void)useParts;
+        (void)multiThreaded;
+        if (!ready()) return;
+        const float c[3] = {sphereCenter.x, sphereCenter.y, sphereCenter.z};
+        uint32_t n = 0;
+        if (vsg_stream_out(m_scene->handle(), m_store, c, radius, &n, nullptr) != VSG_OK)
+            std::cerr << "[STREAM OUT] failed" << std::endl;
+        m_out = n;
+    }
+    void streamOutCopyToChunkGrid(bool multiThreaded) { (void)multiThreaded; }
+
+    void streamInCopyToGPUBuffer(const vec3f& sphereCenter, float radius, bool useParts, bool multiThreaded) {
+        (void)useParts;
+        (void)multiThreaded;
+        m_inCenter = sphereCenter;
+        m_inRadius = radius;
+        m_inPending = true;
+    }
+    void streamInInsertToHashTable(bool multiThreaded) {
+        (void)multiThreaded;
+        if (!ready() || !m_inPending) return;
+        m_inPending = false;
+        const float c[3] = {m_inCenter.x, m_inCenter.y, m_inCenter.z};
+        uint32_t n = 0, merged = 0;
+        const int rc = vsg_stream_in(m_scene->handle(), m_store, c, m_inRadius, &n, &merged, nullptr);
+        if (rc == VSG_ERR_TOO_LARGE)
+            std::cerr << "[ERROR] Not enough free blocks in heap for stream-in" << std::endl;
+        else if (rc != VSG_OK)
+            std::cerr << "[STREAM IN] failed" << std::endl;
+        m_in = n;
+    }
+
+    unsigned int getNumStreamedOut() const { return m_out; }
+    unsigned int getNumStreamedIn() const { return m_in; }
+    vsg_block_store* store() const { return m_store; }
+
+private:
+    bool ready() const {
+        if (!m_store || !m_scene || !m_scene->isAllocated()) {
+            std::cerr << "VoxelStreamingManager: scene or store not allocated" << std::endl;
+            return false;
+        }
+        return true;
+    }
+    VoxelScene* m_scene;
+    Params m_params;
+    vsg_block_store* m_store = nullptr;
+    vec3f m_inCenter;
+    float m_inRadius = 0.0f;
+    bool m_inPending = false;
+    unsigned int m_out = 0, m_in = 0;
+};

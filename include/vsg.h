@@ -130,10 +130,10 @@ VSG_API int vsg_integrate(vsg_scene* s, const float* pointmap, const uint8_t* rg
 
 /* Same integration as vsg_integrate, allocating no device memory.  This entry
  * point has no counterpart in the reference.  It is for callers that cannot
- * allocate while integrating: frame loops recorded into a CUDA graph
- * (cudaMalloc is not allowed during stream capture), real-time loops that
- * must not stall on cudaMalloc/cudaFree, hosts with a fixed GPU memory
- * budget.  vsg_integrate grows two per-pixel work buffers with cudaMalloc
+ * allocate while integrating: real-time loops that must not stall on
+ * cudaMalloc/cudaFree (both can synchronise the whole device), hosts that
+ * hand the library a fixed GPU memory budget at start-up, and plug-in hosts
+ * whose own allocator owns all device memory.  vsg_integrate grows two per-pixel work buffers with cudaMalloc
  * when it first sees a larger image; this variant takes them from a fixed
  * 20 MiB array of device memory inside the library instead.
  * Limits and rules:

@@ -4,8 +4,8 @@
 // pixel's world point with its camera distance, and its packed colour) and
 // grows them with cudaMalloc the first time it sees a larger image.  Some
 // callers cannot let that happen:
-//   - code that records its frame loop into a CUDA graph: cudaMalloc is not
-//     permitted while a stream is being captured;
+//   - plug-in hosts whose own allocator owns all device memory and forbids
+//     the libraries it loads from calling cudaMalloc;
 //   - real-time loops that must never stall on cudaMalloc / cudaFree, which
 //     can synchronise the whole device;
 //   - hosts that hand the library a fixed GPU memory budget at start-up and

@@ -2,8 +2,11 @@
 // reference's main loop does (voxelSG.cpp:392-618): configure the knobs,
 // build a VoxelScene, and per frame upload the maps, integrateFromScanData,
 // construct a RayCastRender, render at the frame's pose from a device
-// matrix, download the depth.  Test harness: frames come from binary files
-// written by the Python test, depths are written back for comparison.
+// matrix, download the depth.  After the frames it extracts the surface with
+// the marching-cubes launchers (MarchingCubes.h:34-58) and streams blocks
+// out to host memory and back with VoxelStreamingManager, then renders the
+// last pose again.  Test harness: frames come from binary files written by
+// the Python test, depths are written back for comparison.
 //
 //   dropin_frames DIR NFRAMES W H FX FY CX CY VOXEL TRUNC SLOTS BLOCKS MIND MAXD
 #include <cstdio>
@@ -78,6 +81,34 @@ int main(int argc, char** argv) {
         if (!write_file(dir + "/depth_" + id + ".bin", depth.data(), n * 4)) return 6;
     }
     std::printf("frames=%u free=%u\n", scene.getNumIntegratedFrames(), scene.getHeapFreeCount());
+    // marching cubes as the reference's launchers are called
+    MarchingCubesParams mcParams;
+    mcParams.voxelSize = g.g_SDFVoxelSize;
+    MarchingCubesOutput mcOut;
+    allocateMarchingCubesOutput(mcOut, (int)g.g_marchingCubesMaxNumTriangles);
+    runMarchingCubesCUDA(scene.getHashData(), scene.getParams(), mcParams, mcOut);
+    std::printf("triangles=%d\n", copyMarchingCubesTriangleCount(mcOut));
+    freeMarchingCubesOutput(mcOut);
+    // stream far blocks out, then everything back in, and render the last pose again
+    VoxelStreamingManager streaming(scene, params, vec3f(0.1f, 0.1f, 0.1f), vec3i(513, 513, 513),
+                                    vec3i(-256, -256, -256), 2000, false);
+    streaming.streamOutFindBlocksOnGPU(vec3f(0.0f, 0.1f, 0.0f), 0.25f, false, false);
+    streaming.streamOutCopyToChunkGrid(false);
+    std::printf("streamed_out=%u free=%u\n", streaming.getNumStreamedOut(), scene.getHeapFreeCount());
+    streaming.streamInCopyToGPUBuffer(vec3f(0.0f, 0.1f, 0.0f), 100.0f, false, false);
+    streaming.streamInInsertToHashTable(false);
+    std::printf("streamed_in=%u free=%u\n", streaming.getNumStreamedIn(), scene.getHeapFreeCount());
+    {
+        vsg::Mat4f T;
+        if (!read_file(dir + "/pose_" + std::to_string(nframes - 1) + ".bin", T.m, sizeof(T.m))) return 4;
+        RayCastRender renderer;
+        if (!renderer.initialize(W, H)) return 5;
+        const float3 cam = make_float3(T.at<float>(0, 3), T.at<float>(1, 3), T.at<float>(2, 3));
+        cudaMemcpy(d_T, T.m, sizeof(T.m), cudaMemcpyHostToDevice);
+        renderer.render(&scene, cam, d_T, fx, fy, cx, cy, minD, maxD);
+        renderer.downloadDepthFloat(depth.data());
+        if (!write_file(dir + "/depth_after_stream.bin", depth.data(), n * 4)) return 6;
+    }
     cudaFree(d_pm);
     cudaFree(d_nm);
     cudaFree(d_rgb);

@@ -1,6 +1,8 @@
 """The C++ drop-in classes (include/voxelsg_b200.hpp) driven like the
 reference's main loop give the same depths as the Python binding of the C
-ABI (needs a GPU; compiles the harness with g++)."""
+ABI, the same marching-cubes triangle count and the same stream-out set, and
+a stream-out / stream-in round trip leaves the rendered depth unchanged
+(needs a GPU; compiles the harness with g++)."""
 import os
 import subprocess
 
@@ -45,3 +47,11 @@ def test_cpp_dropin_matches_binding(cuda, synth_mod, tmp_path):
         got = np.fromfile(os.path.join(d, f"depth_{i}.bin"), np.float32).reshape(H, W)
         assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), i
         assert (got < 1e9).sum() > 0.5 * W * H
+    mc = vsg.MarchingCubes(250000)
+    mc.run(sc, voxel_size=0.004)
+    assert f"triangles={min(mc.count(), 2**31 - 1)}" in r.stdout
+    n_out = sc.stream_out(vsg.Store((0.1, 0.1, 0.1)), (0.0, 0.1, 0.0), 0.25)
+    assert n_out > 0 and f"streamed_out={n_out} " in r.stdout
+    assert f"streamed_in={n_out} " in r.stdout
+    after = np.fromfile(os.path.join(d, "depth_after_stream.bin"), np.float32).reshape(H, W)
+    assert np.array_equal(after.view(np.uint32), ref.view(np.uint32))

@@ -1,6 +1,6 @@
 """vsg_integrate_noalloc -- integration for callers that cannot allocate
-device memory (frame loops recorded into CUDA graphs, real-time loops that
-must not stall on cudaMalloc, fixed memory budgets).  Its per-pixel work
+device memory (real-time loops that must not stall on cudaMalloc, hosts with
+a fixed memory budget, plug-in hosts whose allocator owns device memory).  Its per-pixel work
 buffers live in a fixed device array inside the library instead of buffers
 the scene grows with cudaMalloc.
 
