@@ -275,6 +275,7 @@ def run_ours(args):
                          "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind},
             "clocks": clk.summary()}
     line["marching_cubes"] = mc_measure(sc, peak)
+    line["streaming"] = stream_measure(sc)
     if not args.no_e2e:
         line["e2e"] = e2e(args, frames, K, sc, rr)
     if not args.no_batched:
@@ -314,6 +315,29 @@ def mc_measure(sc, peak: float, reps: int = 10) -> dict:
     gbs = alg / (ms * 1e-3) / 1e9
     return {"triangles": n, "blocks_with_weight": weighted, "ms_per_launch": ms, "alg_bytes": alg,
             "achieved_gbs": gbs, "frac_of_peak": gbs / peak, "launches_timed": int(kcnt[4])}
+
+
+def stream_measure(sc) -> dict:
+    """Streaming over the scene as the timed step left it: every block out to
+    host memory and back (wall clock around each synchronous call; the calls
+    copy through pinned staging, so PCIe bounds them).  Bytes = 4096 + 16 per
+    block each way."""
+    import time
+
+    import vsg
+
+    n0 = sc.stats()["allocated_blocks"]
+    store = vsg.Store()
+    t0 = time.perf_counter()
+    n_out = sc.stream_out(store, (0.0, 0.0, 0.0), 0.0)
+    t1 = time.perf_counter()
+    n_in, _ = sc.stream_in(store)
+    t2 = time.perf_counter()
+    store.close()
+    nb = 4096 + 16
+    return {"blocks": n0, "out_blocks": n_out, "in_blocks": n_in, "out_ms": (t1 - t0) * 1e3,
+            "in_ms": (t2 - t1) * 1e3, "out_gbs": n_out * nb / max(t1 - t0, 1e-9) / 1e9,
+            "in_gbs": n_in * nb / max(t2 - t1, 1e-9) / 1e9}
 
 
 def run_batched(args) -> dict:

@@ -63,6 +63,21 @@ struct Mat4f {
 
 }  // namespace vsg
 
+/* The reference's small vector types (its utils.h); define VSG_HAVE_VEC3
+ * before including this header to use your own. */
+#ifndef VSG_HAVE_VEC3
+struct vec3f {
+    float x = 0.0f, y = 0.0f, z = 0.0f;
+    vec3f() = default;
+    vec3f(float a, float b, float c) : x(a), y(b), z(c) {}
+};
+struct vec3i {
+    int x = 0, y = 0, z = 0;
+    vec3i() = default;
+    vec3i(int a, int b, int c) : x(a), y(b), z(c) {}
+};
+#endif
+
 /* The knobs the fusion path reads, with the reference's code defaults. */
 class GlobalParamsConfig {
 public:
@@ -78,7 +93,11 @@ public:
     float g_SDFRayIncrementFactor = 0.8f;
     unsigned int g_marchingCubesMaxNumTriangles = 250000; /* :379 */
     float g_streamingRadius = 4.0f;       /* :136 */
-    bool g_streamingEnabled = false;
+    bool g_streamingEnabled = true;       /* :119 */
+    vec3f g_streamingVoxelExtents = vec3f(1.0f, 1.0f, 1.0f);        /* :124 */
+    vec3i g_streamingGridDimensions = vec3i(513, 513, 513);         /* :127 */
+    vec3i g_streamingMinGridPos = vec3i(-256, -256, -256);          /* :130 */
+    unsigned int g_streamingInitialChunkListSize = 2000;            /* :133 */
 
     static GlobalParamsConfig& getInstance() {
         static GlobalParamsConfig s;
@@ -364,21 +383,6 @@ inline int copyMarchingCubesTriangleCount(const MarchingCubesOutput& output) {
     if (!output.handle || vsg_mc_triangle_count(output.handle, &n) != VSG_OK) return 0;
     return n > 2147483647 ? 2147483647 : (int)n;
 }
-
-/* The reference's small vector types (its utils.h); define VSG_HAVE_VEC3
- * before including this header to use your own. */
-#ifndef VSG_HAVE_VEC3
-struct vec3f {
-    float x = 0.0f, y = 0.0f, z = 0.0f;
-    vec3f() = default;
-    vec3f(float a, float b, float c) : x(a), y(b), z(c) {}
-};
-struct vec3i {
-    int x = 0, y = 0, z = 0;
-    vec3i() = default;
-    vec3i(int a, int b, int c) : x(a), y(b), z(c) {}
-};
-#endif
 
 /* VoxelStreamingManager.h:140-301 over vsg_stream_* and a vsg_block_store.
  * Single host thread: the reference's auxiliary thread and its Win32 event
