@@ -12,7 +12,8 @@
  *                         isAllocated, getParams, getHeapFreeCount
  *   RayCastRender        (RayCastRender.h:20-124): initialize, render,
  *                         downloadResults, downloadDepthFloat,
- *                         getOutputDepth/Color/Normal/Positions
+ *                         getOutputDepth/Color/Normal/Positions,
+ *                         extractSurfacePoints, saveExtractedSurfacePointsPLY
  *   MarchingCubesParams, MarchingCubesOutput, allocateMarchingCubesOutput,
  *   freeMarchingCubesOutput, runMarchingCubesCUDA,
  *   copyMarchingCubesTriangleCount (MarchingCubes.h:7-58)
@@ -35,6 +36,7 @@
 #include <cstdint>
 #include <iostream>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 #include "vsg.h"
@@ -239,6 +241,7 @@ public:
     RayCastRender() = default;
     ~RayCastRender() {
         if (m_r) vsg_renderer_destroy(m_r);
+        if (m_points) vsg_points_destroy(m_points);
     }
     RayCastRender(const RayCastRender&) = delete;
     RayCastRender& operator=(const RayCastRender&) = delete;
@@ -308,6 +311,38 @@ public:
     int getHeight() const { return m_height; }
     bool isAllocated() const { return m_r != nullptr; }
 
+    /* RayCastRender.cpp:307-360: point buffers (10,000,000 points, as the
+     * reference) are created on the first call; returns the number found. */
+    int extractSurfacePoints(const VoxelScene* voxelScene, float minSDF = -0.01f, float maxSDF = 0.01f,
+                             unsigned int minWeight = 1) {
+        if (!voxelScene || !voxelScene->isAllocated()) {
+            std::cerr << "RayCastRender::extractSurfacePoints: Invalid voxelScene!" << std::endl;
+            return 0;
+        }
+        if (!m_points && vsg_points_create(m_maxExtractedPoints, &m_points) != VSG_OK) {
+            std::cerr << "RayCastRender::extractSurfacePoints: Failed to allocate GPU memory!" << std::endl;
+            m_points = nullptr;
+            return 0;
+        }
+        int64_t n = 0;
+        if (vsg_extract_points(voxelScene->handle(), m_points, minSDF, maxSDF, minWeight, nullptr) != VSG_OK ||
+            vsg_points_count(m_points, &n) != VSG_OK)
+            return 0;
+        m_numExtractedPoints = n > m_maxExtractedPoints ? m_maxExtractedPoints : (int)n;
+        return m_numExtractedPoints;
+    }
+    bool saveExtractedSurfacePointsPLY(const std::string& filePath) {
+        if (!m_points || m_numExtractedPoints == 0) {
+            std::cerr << "RayCastRender::saveExtractedSurfacePointsPLY: No points to save!" << std::endl;
+            return false;
+        }
+        return vsg_points_save_ply(m_points, filePath.c_str()) == VSG_OK;
+    }
+    float4* getExtractedPositions() const { return pts(0); }
+    float4* getExtractedColors() const { return pts(1); }
+    float4* getExtractedNormals() const { return pts(2); }
+    int getNumExtractedPoints() const { return m_numExtractedPoints; }
+
 private:
     float4* ptr(int which) const {
         if (!m_r) return nullptr;
@@ -315,8 +350,17 @@ private:
         vsg_renderer_outputs(m_r, &p[0], &p[1], &p[2], &p[3]);
         return reinterpret_cast<float4*>(p[which]);
     }
+    float4* pts(int which) const {
+        if (!m_points) return nullptr;
+        float* p[3] = {nullptr, nullptr, nullptr};
+        vsg_points_buffers(m_points, &p[0], &p[1], &p[2], nullptr, nullptr);
+        return reinterpret_cast<float4*>(p[which]);
+    }
     vsg_renderer* m_r = nullptr;
     int m_width = 0, m_height = 0;
+    vsg_points* m_points = nullptr;
+    int m_maxExtractedPoints = 10000000;
+    int m_numExtractedPoints = 0;
 };
 
 /* MarchingCubes.h:7-17 */

@@ -214,6 +214,34 @@ VSG_API int vsg_mc_output_buffers(const vsg_mc_output* m, float** vertices, floa
  * vsg_mc_triangle_count.  Synchronises. */
 VSG_API int vsg_mc_download(const vsg_mc_output* m, float* vertices, float* normals, int64_t* count);
 
+/* ---- voxel-wise surface-point extraction ---------------------------------
+ * Replaces RayCastRender::extractSurfacePoints / extractSurfacePointsCUDA /
+ * saveExtractedSurfacePointsPLY (RayCastRender.h:91-109, RayCastRender.cu:
+ * 683-910, RayCastRender.cpp:307-446).  One point per voxel with weight
+ * >= max(1, min_weight) and SDF in [min_sdf, max_sdf] that has a zero
+ * crossing towards a neighbour (or |sdf| < 0.001): float4 position (w = 1),
+ * colour / 255 (w = 1) and SDF-gradient normal (w = 0), unspecified order. */
+typedef struct vsg_points vsg_points;
+
+/* buffers for max_points points on the current device (the reference
+ * allocates 10,000,000) */
+VSG_API int vsg_points_create(int max_points, vsg_points** out);
+VSG_API int vsg_points_destroy(vsg_points* m);
+/* Stream-ordered; does not synchronise. */
+VSG_API int vsg_extract_points(vsg_scene* s, vsg_points* m, float min_sdf, float max_sdf, uint32_t min_weight,
+                               vsg_stream_t stream);
+/* The number of points found, which may exceed the capacity (then only
+ * max_points were written).  Synchronises. */
+VSG_API int vsg_points_count(const vsg_points* m, int64_t* count);
+/* Device buffers (float4 each; the count as int clamped to INT_MAX). */
+VSG_API int vsg_points_buffers(const vsg_points* m, float** positions, float** colors, float** normals,
+                               int** count_dev, int* max_points);
+/* Copy the written points to host float4 arrays (any may be NULL). */
+VSG_API int vsg_points_download(const vsg_points* m, float* positions, float* colors, float* normals,
+                                int64_t* count);
+/* ASCII PLY as saveExtractedSurfacePointsPLY writes it. */
+VSG_API int vsg_points_save_ply(const vsg_points* m, const char* path);
+
 /* ---- streaming between the scene and host memory -------------------------
  * Replaces VoxelStreamingManager (VoxelStreamingManager.h:140-301): the
  * host-side chunk grid (m_grid, :246) is a vsg_block_store; stream out =
@@ -287,7 +315,8 @@ VSG_API int vsg_batch_autotune(vsg_batch* b, int enable);
 
 /* Per-kernel device time (ms) since the last vsg_timing_reset, measured
  * with CUDA events on the launching stream when timing is enabled.
- * Slots: 0 alloc, 1 integrate, 2 render, 3 select, 4 marching cubes.
+ * Slots: 0 alloc, 1 integrate, 2 render, 3 select, 4 marching cubes,
+ * 5 surface-point extraction.
  * counts[i] = launches.
  * With timing enabled renders also count the distinct blocks they read
  * (vsg_stats.render_blocks_read). */

@@ -59,6 +59,8 @@ def lib():
         L.orc_render_touched_blocks.argtypes = [_p, _i, _i, _p, _p, _f, _f, _f, _f, _f, _f]
         L.orc_marching_cubes.restype = _i64
         L.orc_marching_cubes.argtypes = [_p, _p, _f, _f, _i64, _p, _p]
+        L.orc_extract_points.restype = _i64
+        L.orc_extract_points.argtypes = [_p, _f, _f, ctypes.c_uint32, _i64, _p, _p, _p]
         L.orc_stream_out.restype = _i64
         L.orc_stream_out.argtypes = [_p, _p, _f, _p, _p]
         L.orc_stream_in.argtypes = [_p, _i64, _p, _p]
@@ -155,6 +157,18 @@ class OracleScene:
                                               _ptr(n)))
         m = min(total, max_tris)
         return total, v[:m].copy(), n[:m].copy()
+
+    def extract_points(self, min_sdf: float, max_sdf: float, min_weight: int, max_points: int):
+        """kernelExtractSurfacePoints (RayCastRender.cu:683-868): (total count,
+        positions (m,4), colours (m,4), normals (m,4)), m = min(total, max)."""
+        m = max(int(max_points), 1)
+        P = np.zeros((m, 4), np.float32)
+        C = np.zeros((m, 4), np.float32)
+        N = np.zeros((m, 4), np.float32)
+        total = int(self.L.orc_extract_points(self.h, _f(min_sdf), _f(max_sdf), int(min_weight), int(max_points),
+                                              _ptr(P), _ptr(C), _ptr(N)))
+        k = min(total, int(max_points))
+        return total, P[:k].copy(), C[:k].copy(), N[:k].copy()
 
     def stream_out(self, center, radius: float):
         """Remove the blocks whose corner is >= radius from center:

@@ -729,6 +729,112 @@ int64_t orc_marching_cubes(const orc_scene* s, const uint8_t* tab, float iso, fl
     return total;
 }
 
+/* ------------------------------------------------ surface-point extraction */
+
+static ovox voxel_at(const orc_scene* s, const float* p) {
+    const ovox* v = get_voxel(s, p, NULL);
+    ovox e = {0.0f, 0, 0, 0, 0};
+    return v ? *v : e;
+}
+
+/* computeNormalFromSDF, RayCastRender.cu:629-677 */
+static void sdf_normal(const orc_scene* s, const float* p, float* g) {
+    const float eps = s->voxel * 0.5f;
+    for (int a = 0; a < 3; a++) {
+        float q1[3] = {p[0], p[1], p[2]}, q0[3] = {p[0], p[1], p[2]};
+        q1[a] = p[a] + eps;
+        q0[a] = p[a] - eps;
+        const ovox v1 = voxel_at(s, q1), v0 = voxel_at(s, q0);
+        g[a] = (v1.w > 0 && v0.w > 0) ? (v1.sdf - v0.sdf) / (2.0f * eps) : 0.0f;
+    }
+    const float len = sqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+    if (len > 1e-6f) {
+        g[0] /= len;
+        g[1] /= len;
+        g[2] /= len;
+    }
+}
+
+/* kernelExtractSurfacePoints (RayCastRender.cu:683-868) over every allocated
+ * block, voxels in (z, y, x) order: a voxel with weight >= max(1, minW) and
+ * SDF in [minSDF, maxSDF] yields the mean of the zero crossings towards its
+ * six neighbours (x+, x-, y+, y-, z+, z-; neighbours inside the block by
+ * index, outside through getVoxel at centre +- one voxel), or its centre when
+ * there is none and |sdf| < 0.001; colour / 255 and the SDF-gradient normal.
+ * Writes float4 records in block order, the first max_pts of them; returns
+ * the total count. */
+int64_t orc_extract_points(const orc_scene* s, float min_sdf, float max_sdf, uint32_t min_w, int64_t max_pts,
+                           float* pos, float* col, float* nrm) {
+    static const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    const float v = s->voxel;
+    int64_t total = 0;
+    for (int64_t b = 0; b < s->n; b++) {
+        int32_t bc[3];
+        unpack_key(s->keys[b], bc);
+        const float base[3] = {(float)(bc[0] * BS) * v, (float)(bc[1] * BS) * v, (float)(bc[2] * BS) * v};
+        const ovox* vb = s->vox + b * VPB;
+        for (int z = 0; z < BS; z++)
+            for (int y = 0; y < BS; y++)
+                for (int x = 0; x < BS; x++) {
+                    const ovox me = vb[x + y * BS + z * BS * BS];
+                    if (me.w == 0 || me.w < min_w) continue;
+                    if (me.sdf < min_sdf || me.sdf > max_sdf) continue;
+                    const int l[3] = {x, y, z};
+                    float c[3];
+                    for (int a = 0; a < 3; a++) c[a] = base[a] + ((float)l[a] + 0.5f) * v;
+                    float acc[3] = {0.0f, 0.0f, 0.0f};
+                    int nv = 0;
+                    for (int d = 0; d < 6; d++) {
+                        const int nl[3] = {x + off[d][0], y + off[d][1], z + off[d][2]};
+                        ovox nb;
+                        if (nl[0] < 0 || nl[0] >= BS || nl[1] < 0 || nl[1] >= BS || nl[2] < 0 || nl[2] >= BS) {
+                            float q[3];
+                            for (int a = 0; a < 3; a++) q[a] = c[a] + (float)off[d][a] * v;
+                            nb = voxel_at(s, q);
+                        } else {
+                            nb = vb[nl[0] + nl[1] * BS + nl[2] * BS * BS];
+                        }
+                        if (nb.w == 0) continue;
+                        if ((me.sdf < 0.0f && nb.sdf > 0.0f) || (me.sdf > 0.0f && nb.sdf < 0.0f)) {
+                            const float t = me.sdf / (me.sdf - nb.sdf);
+                            for (int a = 0; a < 3; a++) acc[a] += c[a] + (float)off[d][a] * v * t;
+                            nv++;
+                        }
+                    }
+                    float iso[3];
+                    if (nv == 0) {
+                        if (!(fabsf(me.sdf) < 0.001f)) continue;
+                        iso[0] = c[0];
+                        iso[1] = c[1];
+                        iso[2] = c[2];
+                    } else {
+                        for (int a = 0; a < 3; a++) iso[a] = acc[a] / (float)nv;
+                    }
+                    float g[3];
+                    sdf_normal(s, iso, g);
+                    if (total < max_pts) {
+                        float* P = pos + 4 * total;
+                        float* C = col + 4 * total;
+                        float* N = nrm + 4 * total;
+                        P[0] = iso[0];
+                        P[1] = iso[1];
+                        P[2] = iso[2];
+                        P[3] = 1.0f;
+                        C[0] = (float)me.r / 255.0f;
+                        C[1] = (float)me.g / 255.0f;
+                        C[2] = (float)me.b / 255.0f;
+                        C[3] = 1.0f;
+                        N[0] = g[0];
+                        N[1] = g[1];
+                        N[2] = g[2];
+                        N[3] = 0.0f;
+                    }
+                    total++;
+                }
+    }
+    return total;
+}
+
 /* -------------------------------------------------------------- streaming */
 
 /* Weighted merge of two partial averages of one voxel (the library's rule

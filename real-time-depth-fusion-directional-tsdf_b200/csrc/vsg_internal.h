@@ -14,6 +14,7 @@ enum TimingSlot {
     kSlotRender = 2,
     kSlotSelect = 3,
     kSlotMarchingCubes = 4,
+    kSlotExtractPoints = 5,
     kNumSlots = 8
 };
 

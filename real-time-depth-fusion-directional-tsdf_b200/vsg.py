@@ -31,6 +31,8 @@ EXPORTS = [
     "vsg_mc_output_buffers", "vsg_mc_download",
     "vsg_store_create", "vsg_store_destroy", "vsg_store_info", "vsg_store_export", "vsg_store_save",
     "vsg_store_load", "vsg_stream_out", "vsg_stream_in", "vsg_scene_save", "vsg_scene_load",
+    "vsg_points_create", "vsg_points_destroy", "vsg_extract_points", "vsg_points_count", "vsg_points_buffers",
+    "vsg_points_download", "vsg_points_save_ply",
 ]
 
 
@@ -124,6 +126,13 @@ def lib() -> ctypes.CDLL:
         L.vsg_stream_in.argtypes = [_P, _P, _P, _F, _u32p, _u32p, _P]
         L.vsg_scene_save.argtypes = [_P, ctypes.c_char_p]
         L.vsg_scene_load.argtypes = [_P, ctypes.c_char_p, _P]
+        L.vsg_points_create.argtypes = [_I, ctypes.POINTER(_P)]
+        L.vsg_points_destroy.argtypes = [_P]
+        L.vsg_extract_points.argtypes = [_P, _P, _F, _F, ctypes.c_uint32, _P]
+        L.vsg_points_count.argtypes = [_P, ctypes.POINTER(ctypes.c_int64)]
+        L.vsg_points_buffers.argtypes = [_P] + [ctypes.POINTER(_P)] * 4 + [ctypes.POINTER(_I)]
+        L.vsg_points_download.argtypes = [_P, _P, _P, _P, ctypes.POINTER(ctypes.c_int64)]
+        L.vsg_points_save_ply.argtypes = [_P, ctypes.c_char_p]
         _lib = L
     return _lib
 
@@ -343,6 +352,60 @@ class Store:
 
     def load(self, path: str):
         check("vsg_store_load", self.L.vsg_store_load(self.h, str(path).encode()))
+
+
+class SurfacePoints:
+    """RayCastRender::extractSurfacePoints over the C ABI (vsg_points_*)."""
+
+    def __init__(self, max_points: int):
+        self.L = lib()
+        h = _P()
+        check("vsg_points_create", self.L.vsg_points_create(int(max_points), ctypes.byref(h)))
+        self.h = h
+        self.max_points = int(max_points)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.vsg_points_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def extract(self, scene: "Scene", min_sdf: float = -0.1, max_sdf: float = 0.1, min_weight: int = 1,
+                stream=None):
+        check("vsg_extract_points", self.L.vsg_extract_points(scene.h, self.h, _F(min_sdf), _F(max_sdf),
+                                                              int(min_weight), _stream(stream)))
+
+    def count(self) -> int:
+        n = ctypes.c_int64()
+        check("vsg_points_count", self.L.vsg_points_count(self.h, ctypes.byref(n)))
+        return int(n.value)
+
+    def buffers(self) -> dict:
+        ps = [_P() for _ in range(4)]
+        m = _I()
+        check("vsg_points_buffers", self.L.vsg_points_buffers(self.h, *[ctypes.byref(p) for p in ps],
+                                                              ctypes.byref(m)))
+        d = {k: int(p.value or 0) for k, p in zip(("positions", "colors", "normals", "count"), ps)}
+        d["max_points"] = int(m.value)
+        return d
+
+    def download(self):
+        """(total count, positions (m,4), colours (m,4), normals (m,4)), m = min(count, capacity)."""
+        n = self.count()
+        m = min(n, self.max_points)
+        P, C, N = (np.zeros((max(m, 1), 4), np.float32) for _ in range(3))
+        c = ctypes.c_int64()
+        check("vsg_points_download", self.L.vsg_points_download(self.h, _hptr(P), _hptr(C), _hptr(N),
+                                                                ctypes.byref(c)))
+        return int(c.value), P[:m], C[:m], N[:m]
+
+    def save_ply(self, path: str):
+        check("vsg_points_save_ply", self.L.vsg_points_save_ply(self.h, str(path).encode()))
 
 
 class MarchingCubes:
