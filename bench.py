@@ -275,6 +275,7 @@ def run_ours(args):
                          "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind},
             "clocks": clk.summary()}
     line["marching_cubes"] = mc_measure(sc, peak)
+    line["surface_points"] = points_measure(sc, peak)
     line["streaming"] = stream_measure(sc)
     if not args.no_e2e:
         line["e2e"] = e2e(args, frames, K, sc, rr)
@@ -315,6 +316,34 @@ def mc_measure(sc, peak: float, reps: int = 10) -> dict:
     gbs = alg / (ms * 1e-3) / 1e9
     return {"triangles": n, "blocks_with_weight": weighted, "ms_per_launch": ms, "alg_bytes": alg,
             "achieved_gbs": gbs, "frac_of_peak": gbs / peak, "launches_timed": int(kcnt[4])}
+
+
+def points_measure(sc, peak: float, reps: int = 10) -> dict:
+    """Surface-point extraction over the scene as the timed step left it, with
+    the reference main loop's arguments (-0.1, 0.1, weight >= 5,
+    voxelSG.cpp:661): device time per launch from the event ring.  Bytes =
+    voxels of every block holding a weighted voxel (8 B x 512) + 48 B per
+    point written (three float4)."""
+    import vsg
+
+    pts = vsg.SurfacePoints(4_000_000)
+    pts.extract(sc, -0.1, 0.1, 5)
+    sc.timing(True)
+    sc.timing_reset()
+    for _ in range(reps):
+        pts.extract(sc, -0.1, 0.1, 5)
+    kms, kcnt = sc.timing_read()
+    sc.timing(False)
+    sc.timing_reset()
+    n = pts.count()
+    pts.close()
+    _, vox = sc.export()
+    weighted = int((vox.reshape(-1, 512, 8)[:, :, 7] > 0).any(1).sum())
+    ms = float(kms[5] / max(kcnt[5], 1))
+    alg = weighted * 512 * 8 + min(n, 4_000_000) * 48
+    gbs = alg / (ms * 1e-3) / 1e9
+    return {"points": n, "ms_per_launch": ms, "alg_bytes": alg, "achieved_gbs": gbs, "frac_of_peak": gbs / peak,
+            "launches_timed": int(kcnt[5])}
 
 
 def stream_measure(sc) -> dict:
