@@ -74,6 +74,6 @@ def test_points_capacity_empty_and_ply(cuda, synth_mod, oracle_mod, tmp_path):
     path = str(tmp_path / "pts.ply")
     pts.save_ply(path)
     lines = open(path).read().splitlines()
-    assert lines[0] == "ply" and "element vertex 100" in lines and lines.index("end_header") == 12
-    body = np.array([[float(x) for x in ln.split()] for ln in lines[13:]])
+    assert lines[0] == "ply" and "element vertex 100" in lines and lines.index("end_header") == 13
+    body = np.array([[float(x) for x in ln.split()] for ln in lines[14:]])
     assert body.shape == (100, 9) and np.all((body[:, 6:] >= 0) & (body[:, 6:] <= 255))
