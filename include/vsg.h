@@ -182,6 +182,40 @@ VSG_API int vsg_renderer_outputs(const vsg_renderer* r, float** depth, float** p
 VSG_API int vsg_renderer_download(const vsg_renderer* r, float* depth, float* position, float* color,
                           float* normal);
 
+/* ---- adjoint of the ray cast (no counterpart in the reference) ----------
+ * A hit pixel's depth and position are smooth functions of the camera pose
+ * and of the voxel SDF values once the march's discrete decisions are fixed
+ * (the zero-crossing bracket, each sample's tap voxels and their weights, the
+ * side each regula-falsi step keeps).  vsg_renderer_record makes the
+ * following renders keep each pixel's bracket (8 bytes per pixel, allocated
+ * on the first enable); vsg_render_backward then recomputes the crossing
+ * with the forward's exact arithmetic and runs reverse mode through it.
+ * The render must have used the same scene, unchanged since, and the pose's
+ * translation as ray origin (vsg_render_hostpose does). */
+VSG_API int vsg_renderer_record(vsg_renderer* r, int enable);
+/* grad_depth: device float[w*h] dL/d depth (NULL = 0); grad_position: device
+ * float4[w*h] dL/d position (NULL = 0).  grad_pose: DEVICE double[12]
+ * receiving dL/dT for the row-major 3x4 camera->world matrix (written;
+ * rotation entries 0-2, 4-6, 8-10, translation 3, 7, 11).  grad_sdf: device
+ * float[num_sdf_blocks * 512] indexed like the voxel pool (pool block * 512 +
+ * x + 8y + 64z), ACCUMULATED with atomics (NULL = skip).  n_skipped: if not
+ * NULL, the call synchronises and stores the number of hit pixels whose
+ * recomputation did not reproduce the rendered depth (0 when the
+ * preconditions hold). */
+VSG_API int vsg_render_backward(const vsg_renderer* r, const vsg_scene* s, const float pose[16], float fx, float fy,
+                                float cx, float cy, const float* grad_depth, const float* grad_position,
+                                double* grad_pose, float* grad_sdf, uint32_t* n_skipped, vsg_stream_t stream);
+/* Pool indices of the given blocks (host int32 coords[n*3] -> host int32
+ * ptrs[n], -1 = not allocated): the row of grad_sdf, or of the voxel pool,
+ * that holds each block.  Synchronises. */
+VSG_API int vsg_scene_lookup_blocks(const vsg_scene* s, const int32_t* coords, uint32_t n, int32_t* ptrs);
+/* Normals of the last recorded render (the reference never writes its normal
+ * output): the normalised trilinear SDF gradient at each hit point, pointing
+ * towards increasing SDF like computeNormalFromSDF (RayCastRender.cu:629-677);
+ * misses get 1e10.  normals: device float4[w*h]. */
+VSG_API int vsg_render_normals(const vsg_renderer* r, const vsg_scene* s, const float pose[16], float fx, float fy,
+                               float cx, float cy, float* normals, uint32_t* n_skipped, vsg_stream_t stream);
+
 /* ---- marching cubes -----------------------------------------------------
  * Replaces allocateMarchingCubesOutput / freeMarchingCubesOutput /
  * runMarchingCubesCUDA / copyMarchingCubesTriangleCount (MarchingCubes.h:

@@ -59,6 +59,7 @@ def lib():
         L.orc_render_touched_blocks.argtypes = [_p, _i, _i, _p, _p, _f, _f, _f, _f, _f, _f]
         L.orc_marching_cubes.restype = _i64
         L.orc_marching_cubes.argtypes = [_p, _p, _f, _f, _i64, _p, _p]
+        L.orc_render_brackets.argtypes = [_p, _i, _i, _p, _p, _f, _f, _f, _f, _f, _f, _p]
         L.orc_extract_points.restype = _i64
         L.orc_extract_points.argtypes = [_p, _f, _f, ctypes.c_uint32, _i64, _p, _p, _p]
         L.orc_stream_out.restype = _i64
@@ -139,6 +140,15 @@ class OracleScene:
                                    _ptr(col), _ptr(nrm), _ptr(st))
         return {"depth": depth, "position": pos, "color": col, "normal": nrm, "hits": int(st[0]),
                 "misses": int(st[1]), "samples": int(st[2])}
+
+    def brackets(self, W, H, pose, fx, fy, cx, cy, min_depth, max_depth) -> np.ndarray:
+        """(H, W, 2) float32: the march bracket of each hit pixel's crossing."""
+        T = _f32(pose).reshape(16)
+        cam = np.array([T[3], T[7], T[11]], np.float32)
+        out = np.full((H, W, 2), np.nan, np.float32)
+        self.L.orc_render_brackets(self.h, W, H, _ptr(cam), _ptr(T), _f(fx), _f(fy), _f(cx), _f(cy),
+                                   _f(min_depth), _f(max_depth), _ptr(out))
+        return out
 
     def touched_blocks(self, W, H, pose, fx, fy, cx, cy, min_depth, max_depth) -> int:
         T = _f32(pose).reshape(16)

@@ -502,7 +502,7 @@ static int bisection(const orc_scene* s, const float* o, const float* dir, float
  * 276-398.  One pixel.  Returns 1 on a hit. steps_out counts samples. */
 static int render_pixel(const orc_scene* s, int x, int y, const float* cam, const float* T, float fx,
                         float fy, float cx, float cy, float minD, float maxD, float* depth, float* pos4,
-                        float* col4, float* nrm4, int64_t* steps_out, uint8_t* mark) {
+                        float* col4, float* nrm4, int64_t* steps_out, uint8_t* mark, float* bracket) {
     *depth = MINF;
     for (int k = 0; k < 4; k++) pos4[k] = col4[k] = nrm4[k] = MINF;
     float cd[3] = {((float)x - cx) / fx, ((float)y - cy) / fy, 1.0f};
@@ -534,6 +534,10 @@ static int render_pixel(const orc_scene* s, int x, int y, const float* cam, cons
         steps++;
         if (trilinear(s, p, &dist, NULL, mark)) {
             if (lastW > 0 && lastSdf < 0.0f && dist > 0.0f) {
+                if (bracket) {
+                    bracket[0] = lastAlpha;
+                    bracket[1] = rc;
+                }
                 float alpha = 0.0f;
                 uint8_t c2[3] = {0, 0, 0};
                 int b = bisection(s, cam, wd, lastSdf, lastAlpha, dist, rc, &alpha, c2, mark);
@@ -583,7 +587,7 @@ void orc_render(const orc_scene* s, int W, int H, const float* cam, const float*
     for (int64_t i = 0; i < (int64_t)W * H; i++) {
         int x = (int)(i % W), y = (int)(i / W);
         int h = render_pixel(s, x, y, cam, T, fx, fy, cx, cy, minD, maxD, depth + i, pos4 + 4 * i,
-                             col4 + 4 * i, nrm4 + 4 * i, &steps, NULL);
+                             col4 + 4 * i, nrm4 + 4 * i, &steps, NULL, NULL);
         hits += h;
         miss += !h;
     }
@@ -606,7 +610,7 @@ void orc_render_rows(const orc_scene* s, int W, int H, int y0, int y1, const flo
     for (int64_t i = (int64_t)y0 * W; i < (int64_t)y1 * W; i++) {
         int x = (int)(i % W), y = (int)(i / W);
         int h = render_pixel(s, x, y, cam, T, fx, fy, cx, cy, minD, maxD, depth + i, pos4 + 4 * i,
-                             col4 + 4 * i, nrm4 + 4 * i, &steps, NULL);
+                             col4 + 4 * i, nrm4 + 4 * i, &steps, NULL, NULL);
         hits += h;
         miss += !h;
     }
@@ -627,7 +631,7 @@ int64_t orc_render_touched_blocks(const orc_scene* s, int W, int H, const float*
     for (int64_t i = 0; i < (int64_t)W * H; i++) {
         float d, p4[4], c4[4], n4[4];
         render_pixel(s, (int)(i % W), (int)(i / W), cam, T, fx, fy, cx, cy, minD, maxD, &d, p4, c4, n4,
-                     &steps, mark);
+                     &steps, mark, NULL);
     }
     int64_t n = 0;
     for (int64_t b = 0; b < s->n; b++) n += mark[b];
@@ -922,6 +926,24 @@ void orc_stream_in(orc_scene* s, int64_t n, const int32_t* coords, const uint8_t
                 memcpy(&x, voxels + (i * VPB + v) * 8, 8);
                 dst[v] = merge_vox(dst[v], x);
             }
+        }
+    }
+}
+
+/* March bracket [lastAlpha, rc] of each hit pixel's zero crossing (float2
+ * per pixel; misses untouched): the discrete decision the ray-cast adjoint
+ * holds fixed.  Test support, not part of the reference. */
+void orc_render_brackets(const orc_scene* s, int W, int H, const float* cam, const float* T, float fx, float fy,
+                         float cx, float cy, float minD, float maxD, float* bracket) {
+    if (s->n == 0) return;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < (int64_t)W * H; i++) {
+        float d, p4[4], c4[4], n4[4], br[2];
+        int64_t steps = 0;
+        if (render_pixel(s, (int)(i % W), (int)(i / W), cam, T, fx, fy, cx, cy, minD, maxD, &d, p4, c4, n4, &steps,
+                         NULL, br)) {
+            bracket[2 * i] = br[0];
+            bracket[2 * i + 1] = br[1];
         }
     }
 }

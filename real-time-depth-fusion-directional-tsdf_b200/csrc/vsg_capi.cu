@@ -271,6 +271,9 @@ int vsg_renderer_destroy(vsg_renderer* r) {
     cudaFree(r->impl.position);
     cudaFree(r->impl.color);
     cudaFree(r->impl.normal);
+    cudaFree(r->impl.bracket);
+    cudaFree(r->impl.partials);
+    cudaFree(r->impl.skipped);
     delete r;
     return VSG_OK;
 }

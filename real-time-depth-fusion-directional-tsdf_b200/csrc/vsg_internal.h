@@ -50,6 +50,12 @@ struct Renderer {
     float4* color = nullptr;
     float4* normal = nullptr;
     int sm_count = 148;
+    // adjoint support (vsg_renderer_record): march brackets, per-CTA pose
+    // gradient partials, skipped-pixel counter
+    bool record = false;
+    float2* bracket = nullptr;
+    float* partials = nullptr;
+    unsigned int* skipped = nullptr;
 };
 
 int scene_alloc_device(Scene* sc);

@@ -104,6 +104,7 @@ int render_launch(Renderer* r, Scene* sc, const float cam[3], const float* pose_
     a.pos = r->position;
     a.col = r->color;
     a.nrm = r->normal;
+    a.rec = r->record ? r->bracket : nullptr;
     a.touched = sc->timing.enabled ? sc->dev.block_touched : nullptr;
     if (a.touched) cudaMemsetAsync(a.touched, 0, (size_t)sc->dev.num_blocks, st);
     k_render_begin<<<1, 1, 0, st>>>(sc->dev.frame);

@@ -24,6 +24,7 @@ struct RenderArgs {
     float4* pos;
     float4* col;
     float4* nrm;
+    float2* rec;  // non-null when recording: per pixel the march bracket of its last zero crossing
 };
 
 // Pool indices of the blocks holding a sample's 8 trilinear taps.  The taps
@@ -311,6 +312,7 @@ static __device__ __forceinline__ void render_pixel(const RenderArgs& a, int x, 
             if (mode == 0) {
                 if (ok && lastValid && lastSdf < 0.0f && dist > 0.0f) {
                     // zero crossing: a = last sample, b = this one
+                    if (a.rec) a.rec[pi] = make_float2(lastAlpha, rc);
                     ba = lastAlpha;
                     bad = lastSdf;
                     bb = rc;

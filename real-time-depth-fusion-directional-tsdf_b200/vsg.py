@@ -33,6 +33,7 @@ EXPORTS = [
     "vsg_store_load", "vsg_stream_out", "vsg_stream_in", "vsg_scene_save", "vsg_scene_load",
     "vsg_points_create", "vsg_points_destroy", "vsg_extract_points", "vsg_points_count", "vsg_points_buffers",
     "vsg_points_download", "vsg_points_save_ply",
+    "vsg_renderer_record", "vsg_render_backward", "vsg_render_normals", "vsg_scene_lookup_blocks",
 ]
 
 
@@ -133,6 +134,11 @@ def lib() -> ctypes.CDLL:
         L.vsg_points_buffers.argtypes = [_P] + [ctypes.POINTER(_P)] * 4 + [ctypes.POINTER(_I)]
         L.vsg_points_download.argtypes = [_P, _P, _P, _P, ctypes.POINTER(ctypes.c_int64)]
         L.vsg_points_save_ply.argtypes = [_P, ctypes.c_char_p]
+        L.vsg_renderer_record.argtypes = [_P, _I]
+        L.vsg_scene_lookup_blocks.argtypes = [_P, _P, ctypes.c_uint32, _P]
+        L.vsg_render_backward.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, _P, _P, _P,
+                                          ctypes.POINTER(ctypes.c_uint32), _P]
+        L.vsg_render_normals.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, ctypes.POINTER(ctypes.c_uint32), _P]
         _lib = L
     return _lib
 
@@ -169,6 +175,42 @@ def default_params(**kw) -> Params:
     for k, v in kw.items():
         setattr(p, k, v)
     return p
+
+
+class _DeviceArray:
+    """__cuda_array_interface__ view of a raw device pointer."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3}
+
+
+def render_depth(scene, renderer, pose, fx, fy, cx, cy, min_depth, max_depth):
+    """Differentiable ray cast (torch autograd): depth (H,W) of `scene` seen
+    from `pose` (a (4,4) float32 torch tensor, camera->world; may require
+    grad).  The backward pass returns dL/dpose (rows 0-2; row 3 zero) through
+    vsg_render_backward.  Misses hold 1e10 and carry no gradient."""
+    import torch
+
+    class _Render(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, T):
+            Th = T.detach().to("cpu", torch.float32).numpy().reshape(16)
+            renderer.record(True)
+            renderer.render(scene, Th, fx, fy, cx, cy, min_depth, max_depth)
+            ctx.Th = Th
+            ctx.dev, ctx.dtype = T.device, T.dtype
+            return renderer.depth_tensor().clone()
+
+        @staticmethod
+        def backward(ctx, g):
+            g = g.contiguous().to(torch.float32)
+            gT, skipped = renderer.backward(scene, ctx.Th, fx, fy, cx, cy, grad_depth=g)
+            out = torch.zeros((4, 4), dtype=torch.float64)
+            out[:3] = torch.from_numpy(gT)
+            return out.to(device=ctx.dev, dtype=ctx.dtype)
+
+    return _Render.apply(pose)
 
 
 class Scene:
@@ -228,6 +270,13 @@ class Scene:
         check("vsg_scene_export", self.L.vsg_scene_export(
             self.h, _hptr(coords), _hptr(vox) if with_voxels else None, cnt, ctypes.byref(n)))
         return coords[:cnt], (vox[:cnt] if with_voxels else None)
+
+    def lookup_blocks(self, coords) -> np.ndarray:
+        """Pool index of each block coordinate (-1 = not allocated)."""
+        c = np.ascontiguousarray(np.asarray(coords, np.int32).reshape(-1, 3))
+        out = np.zeros(max(len(c), 1), np.int32)
+        check("vsg_scene_lookup_blocks", self.L.vsg_scene_lookup_blocks(self.h, _hptr(c), len(c), _hptr(out)))
+        return out[:len(c)]
 
     def stream_out(self, store: "Store", center, radius: float, stream=None) -> int:
         c = np.ascontiguousarray(np.asarray(center, np.float32).reshape(3))
@@ -295,6 +344,49 @@ class Renderer:
             check("vsg_render_hostpose", self.L.vsg_render_hostpose(
                 self.h, scene.h, _hptr(cam), _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _F(min_depth),
                 _F(max_depth), _stream(stream)))
+
+    def record(self, enable: bool = True):
+        """Keep each pixel's march bracket in the following renders (needed
+        by backward() and normals())."""
+        check("vsg_renderer_record", self.L.vsg_renderer_record(self.h, int(enable)))
+
+    def backward(self, scene: "Scene", pose, fx, fy, cx, cy, grad_depth=None, grad_position=None, grad_sdf=None,
+                 stream=None):
+        """Reverse mode through the last recorded render.  grad_depth (H,W) /
+        grad_position (H,W,4): device float32 tensors of dL/d output (None = 0).
+        grad_sdf: device float32 tensor of num_sdf_blocks*512 entries the voxel
+        SDF gradients are ADDED to (None = skip).  Returns (dL/dT as a (3,4)
+        float64 numpy array, number of hit pixels that could not be
+        recomputed -- 0 when the render used this scene and pose)."""
+        import torch
+
+        T = np.ascontiguousarray(np.asarray(pose, np.float32).reshape(16))
+        gp = torch.zeros(12, dtype=torch.float64, device="cuda")
+        skipped = ctypes.c_uint32()
+        check("vsg_render_backward", self.L.vsg_render_backward(
+            self.h, scene.h, _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _dptr(grad_depth), _dptr(grad_position),
+            _dptr(gp), _dptr(grad_sdf), ctypes.byref(skipped), _stream(stream)))
+        return gp.cpu().numpy().reshape(3, 4), int(skipped.value)
+
+    def normals(self, scene: "Scene", pose, fx, fy, cx, cy, out=None, stream=None):
+        """Normals of the last recorded render: (H,W,4) float32 device tensor."""
+        import torch
+
+        T = np.ascontiguousarray(np.asarray(pose, np.float32).reshape(16))
+        if out is None:
+            out = torch.empty((self.height, self.width, 4), dtype=torch.float32, device="cuda")
+        skipped = ctypes.c_uint32()
+        check("vsg_render_normals", self.L.vsg_render_normals(
+            self.h, scene.h, _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _dptr(out), ctypes.byref(skipped),
+            _stream(stream)))
+        return out, int(skipped.value)
+
+    def depth_tensor(self):
+        """The depth output buffer as a (H,W) float32 torch tensor view."""
+        import torch
+
+        return torch.as_tensor(_DeviceArray(self.outputs()["depth"], (self.height, self.width), "<f4"),
+                               device="cuda")
 
     def outputs(self) -> dict:
         ps = [_P() for _ in range(4)]

@@ -1,0 +1,133 @@
+"""Float64 restatement of a hit pixel's ray-cast depth as a function of the
+camera pose and the voxel SDF values, with the march's discrete decisions
+held fixed -- test infrastructure for the adjoint (vsg_render_backward).
+
+Per pixel: ray direction wd = normalize(R cd) from the pixel's normalised
+camera direction cd, origin o = translation (RayCastRender.cu:447-470); the
+zero-crossing bracket [a, b] (march parameters, pose-independent) comes from
+the oracle's FP32 march; f(t) is the trilinear SDF at o + t wd
+(RayCastRender.cu:127-215) with each sample's 8 tap voxels, their weights'
+integer bases and validity frozen at the base pose; three regula-falsi steps
+RF(a, fa, b, fb) = a + fa / (fa - fb) (b - a) (:229-271), the side each step
+keeps frozen at the base pose; depth = alpha * cd_z.  Central differences of
+this function in float64 are what the GPU gradient is checked against.
+"""
+import numpy as np
+
+
+class Volume:
+    """Exported blocks: sdf (n,512) float64, weight (n,512), coord -> row."""
+
+    def __init__(self, coords, vox_bytes):
+        v = np.ascontiguousarray(vox_bytes).reshape(-1, 512, 8)
+        self.sdf = np.ascontiguousarray(v[:, :, :4]).view(np.float32).reshape(-1, 512).astype(np.float64)
+        self.w = v[:, :, 7].astype(np.int64)
+        self.coords = np.asarray(coords)
+        self.row = {tuple(c): i for i, c in enumerate(self.coords.tolist())}
+
+
+def _tap(q):
+    return np.floor(q + 0.5 * np.sign(q)).astype(np.int64)
+
+
+class Evaluator:
+    def __init__(self, vol: Volume, voxel: float, K, pix, brackets):
+        self.vol = vol
+        self.v = float(np.float32(voxel))
+        self.K = K
+        self.pix = np.asarray(pix, np.float64)
+        self.br = np.asarray(brackets, np.float64)
+        self.frozen = None
+
+    def rays(self, T):
+        K = self.K
+        x, y = self.pix[:, 0], self.pix[:, 1]
+        cd = np.stack([(x - K.cx) / K.fx, (y - K.cy) / K.fy, np.ones_like(x)], 1)
+        cd /= np.linalg.norm(cd, axis=1, keepdims=True)
+        u = cd @ np.asarray(T, np.float64)[:3, :3].T
+        wd = u / np.linalg.norm(u, axis=1, keepdims=True)
+        o = np.asarray(T, np.float64)[:3, 3]
+        return cd, wd, o
+
+    def _taps(self, p):
+        v = self.v
+        q = (p - v / 2) / v
+        fl = np.floor(q)
+        t0, t1 = _tap(q), _tap(q + 1.0)
+        N = p.shape[0]
+        idx = np.full((N, 8), -1, np.int64)
+        valid = np.zeros((N, 8), bool)
+        for i in range(8):
+            vx = np.stack([t1[:, 0] if i & 1 else t0[:, 0], t1[:, 1] if i & 2 else t0[:, 1],
+                           t1[:, 2] if i & 4 else t0[:, 2]], 1)
+            blk, loc = vx >> 3, vx & 7
+            for n in range(N):
+                r = self.vol.row.get(tuple(blk[n].tolist()))
+                if r is not None:
+                    li = loc[n, 0] + 8 * loc[n, 1] + 64 * loc[n, 2]
+                    idx[n, i] = r * 512 + li
+                    valid[n, i] = self.vol.w[r, li] > 0
+        return {"fl": fl, "idx": idx, "valid": valid}
+
+    def _f(self, p, tp, sdf):
+        v = self.v
+        w = (p - v / 2) / v - tp["fl"]
+        tw = np.ones((p.shape[0], 8))
+        for i in range(8):
+            for a, bit in enumerate((1, 2, 4)):
+                tw[:, i] *= w[:, a] if i & bit else (1.0 - w[:, a])
+        tw = tw * tp["valid"]
+        s = sdf.reshape(-1)[np.maximum(tp["idx"], 0)]
+        return (tw * s).sum(1) / tw.sum(1)
+
+    def _grad_f(self, p, tp, sdf):
+        eps = 1e-7
+        g = np.zeros_like(p)
+        for a in range(3):
+            d = np.zeros(3)
+            d[a] = eps
+            g[:, a] = (self._f(p + d, tp, sdf) - self._f(p - d, tp, sdf)) / (2 * eps)
+        return g
+
+    def depth(self, T, sdf=None, want_normal=False):
+        """Depth of every pixel; the first call fixes the decisions."""
+        sdf = self.vol.sdf if sdf is None else sdf
+        cd, wd, o = self.rays(T)
+        N = len(self.pix)
+        first = self.frozen is None
+        if first:
+            self.frozen = {"taps": [], "side": []}
+        P = np.zeros((N, 4))
+        F = np.zeros((N, 4))
+        P[:, 0], P[:, 1] = self.br[:, 0], self.br[:, 1]
+        ia = np.zeros(N, np.int64)
+        ib = np.ones(N, np.int64)
+        rows = np.arange(N)
+
+        def sample(k):
+            p = o + P[:, k:k + 1] * wd
+            if first:
+                self.frozen["taps"].append(self._taps(p))
+            F[:, k] = self._f(p, self.frozen["taps"][k], sdf)
+
+        sample(0)
+        sample(1)
+        for k in (2, 3):
+            a, fa, b, fb = P[rows, ia], F[rows, ia], P[rows, ib], F[rows, ib]
+            P[:, k] = a + fa / (fa - fb) * (b - a)
+            sample(k)
+            if first:
+                self.frozen["side"].append(F[rows, ia] * F[:, k] > 0)
+            keep = self.frozen["side"][k - 2]
+            ia = np.where(keep, k, ia)
+            ib = np.where(keep, ib, k)
+        a, fa, b, fb = P[rows, ia], F[rows, ia], P[rows, ib], F[rows, ib]
+        alpha = a + fa / (fa - fb) * (b - a)
+        out = alpha * cd[:, 2]
+        if want_normal:
+            p = o + alpha[:, None] * wd
+            if "hit_taps" not in self.frozen:
+                self.frozen["hit_taps"] = self._taps(p)
+            g = self._grad_f(p, self.frozen["hit_taps"], sdf)
+            return out, g / np.linalg.norm(g, axis=1, keepdims=True), alpha, wd, o
+        return out
