@@ -80,6 +80,116 @@ class Evaluator:
         s = sdf.reshape(-1)[np.maximum(tp["idx"], 0)]
         return (tw * s).sum(1) / tw.sum(1)
 
+    def _f_and_grad(self, p, tp, sdf):
+        """f and its analytic position gradient (frozen taps)."""
+        v = self.v
+        w = (p - v / 2) / v - tp["fl"]
+        valid = tp["valid"]
+        s = sdf.reshape(-1)[np.maximum(tp["idx"], 0)]
+        terms = [[w[:, a] if i & bit else 1.0 - w[:, a] for a, bit in enumerate((1, 2, 4))] for i in range(8)]
+        tw = np.stack([terms[i][0] * terms[i][1] * terms[i][2] for i in range(8)], 1) * valid
+        W = tw.sum(1)
+        f = (tw * s).sum(1) / W
+        g = np.zeros_like(p)
+        for a, bit in enumerate((1, 2, 4)):
+            dtw = np.stack([(1.0 if i & bit else -1.0) * np.prod([terms[i][b] for b in range(3) if b != a], 0)
+                            for i in range(8)], 1) * valid
+            g[:, a] = (dtw * (s - f[:, None])).sum(1) / W / v
+        return f, g, tw / W[:, None]
+
+    def analytic_grad(self, T, gd, gpos):
+        """Reverse mode through the fixed-decision depth (the GPU kernel's
+        algorithm in float64): dL/dT (3,4) for L = sum gd*depth + gpos.pos."""
+        cd, wd, o = self.rays(T)
+        T = np.asarray(T, np.float64)
+        N = len(self.pix)
+        rows = np.arange(N)
+        P = np.zeros((N, 4))
+        F = np.zeros((N, 4))
+        G = np.zeros((N, 4, 3))
+        P[:, 0], P[:, 1] = self.br[:, 0], self.br[:, 1]
+        ia = np.zeros(N, np.int64)
+        ib = np.ones(N, np.int64)
+        steps = []
+        for k in range(4):
+            if k >= 2:
+                steps.append((ia.copy(), ib.copy()))
+                a, fa, b, fb = P[rows, ia], F[rows, ia], P[rows, ib], F[rows, ib]
+                P[:, k] = a + fa / (fa - fb) * (b - a)
+            F[:, k], G[:, k], _ = self._f_and_grad(o + P[:, k:k + 1] * wd, self.frozen["taps"][k], self.vol.sdf)
+            if k >= 2:
+                keep = self.frozen["side"][k - 2]
+                ia = np.where(keep, k, ia)
+                ib = np.where(keep, ib, k)
+        steps.append((ia.copy(), ib.copy()))
+        a, fa, b, fb = P[rows, ia], F[rows, ia], P[rows, ib], F[rows, ib]
+        alpha = a + fa / (fa - fb) * (b - a)
+        g_alpha = gd * cd[:, 2] + (gpos * wd).sum(1)
+        go = gpos.copy()
+        gw = alpha[:, None] * gpos
+        gP = np.zeros((N, 4))
+        gF = np.zeros((N, 4))
+
+        def rf_back(ia, ib, g):
+            a, fa, b, fb = P[rows, ia], F[rows, ia], P[rows, ib], F[rows, ib]
+            den = fa - fb
+            t = fa / den
+            np.add.at(gP, (rows, ia), (1 - t) * g)
+            np.add.at(gP, (rows, ib), t * g)
+            np.add.at(gF, (rows, ia), (b - a) * (-fb / den ** 2) * g)
+            np.add.at(gF, (rows, ib), (b - a) * (fa / den ** 2) * g)
+
+        rf_back(*steps[2], g_alpha)
+        for k in (3, 2, 1, 0):
+            gf = gF[:, k]
+            go += gf[:, None] * G[:, k]
+            gw += (gf * P[:, k])[:, None] * G[:, k]
+            gP[:, k] += gf * (G[:, k] * wd).sum(1)
+            if k >= 2:
+                rf_back(*steps[k - 2], gP[:, k])
+        u = cd @ T[:3, :3].T
+        wl = np.linalg.norm(u, axis=1)
+        gu = (gw - wd * (gw * wd).sum(1, keepdims=True)) / wl[:, None]
+        out = np.zeros((3, 4))
+        out[:, :3] = gu.T @ cd
+        out[:, 3] = go.sum(0)
+        return out
+
+    def weight_sums(self, T):
+        """Per pixel, the smallest normalising weight (sum of the valid taps'
+        trilinear weights) over the crossing's samples: where it is small the
+        depth is a steep function of the pose and finite differences need a
+        tiny step."""
+        cd, wd, o = self.rays(T)
+        N = len(self.pix)
+        rows = np.arange(N)
+        P = np.zeros((N, 4))
+        F = np.zeros((N, 4))
+        P[:, 0], P[:, 1] = self.br[:, 0], self.br[:, 1]
+        ia = np.zeros(N, np.int64)
+        ib = np.ones(N, np.int64)
+        wmin = np.full(N, np.inf)
+        for k in range(4):
+            if k >= 2:
+                a, fa, b, fb = P[rows, ia], F[rows, ia], P[rows, ib], F[rows, ib]
+                P[:, k] = a + fa / (fa - fb) * (b - a)
+            p = o + P[:, k:k + 1] * wd
+            tp = self.frozen["taps"][k]
+            v = self.v
+            w = (p - v / 2) / v - tp["fl"]
+            tw = np.ones((N, 8))
+            for i in range(8):
+                for ax, bit in enumerate((1, 2, 4)):
+                    tw[:, i] *= w[:, ax] if i & bit else (1.0 - w[:, ax])
+            tw = tw * tp["valid"]
+            wmin = np.minimum(wmin, tw.sum(1))
+            F[:, k] = self._f(p, tp, self.vol.sdf)
+            if k >= 2:
+                keep = self.frozen["side"][k - 2]
+                ia = np.where(keep, k, ia)
+                ib = np.where(keep, ib, k)
+        return wmin
+
     def _grad_f(self, p, tp, sdf):
         eps = 1e-7
         g = np.zeros_like(p)

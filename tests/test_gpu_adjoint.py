@@ -14,6 +14,15 @@ pytestmark = pytest.mark.gpu
 VOXEL, TRUNC, MIN_D, MAX_D = 0.004, 0.02, 0.2, 3.0
 POSE_TOL = 1e-4  # relative error of the pose gradient against FP64 central differences
 SDF_TOL = 1e-3   # relative error per voxel SDF gradient
+# Central-difference steps.  The fixed-decision depth has large third
+# derivatives (three regula-falsi divisions, trilinear weights renormalised
+# over the valid taps), so the truncation error of a central difference is
+# about 1e-2 relative at h = 1e-4 and falls as h^2: 1e-4 at 1e-5, 1e-6 at
+# 1e-6 (measured on this scene); float64 round-off stays below 1e-9 there.
+H_POSE, H_SDF = 1e-6, 1e-7
+# Pixels whose samples renormalise over valid taps with total weight below
+# this are left out: there the depth is so steep that no step resolves it.
+MIN_WEIGHT_SUM = 0.05
 
 
 def _setup(cuda, synth_mod, oracle_mod, frames=4, W=160, H=120):
@@ -48,6 +57,19 @@ def _subset(depth, n, rng):
     return sel[:, ::-1].copy()  # (x, y)
 
 
+def _well_conditioned(vol, K, depth, T, o, n, rng):
+    """n hit pixels whose crossing samples all have weight sum >= MIN_WEIGHT_SUM,
+    with their brackets and a base-pose evaluator."""
+    pix = _subset(depth, 3 * n, rng)
+    br = o.brackets(K.width, K.height, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)[pix[:, 1], pix[:, 0]]
+    ev = Evaluator(vol, VOXEL, K, pix, br)
+    ev.depth(T.astype(np.float64))
+    keep = np.nonzero(ev.weight_sums(T.astype(np.float64)) >= MIN_WEIGHT_SUM)[0][:n]
+    pix, br = pix[keep], br[keep]
+    ev = Evaluator(vol, VOXEL, K, pix, br)
+    return pix, ev
+
+
 def test_pose_and_sdf_gradients_match_fp64_central_differences(cuda, synth_mod, oracle_mod):
     vsg, fr, K, sc, rr, o, vol = _setup(cuda, synth_mod, oracle_mod)
     T = _pose(fr)
@@ -55,7 +77,8 @@ def test_pose_and_sdf_gradients_match_fp64_central_differences(cuda, synth_mod, 
     out = rr.download()
     depth = out["depth"]
     rng = np.random.default_rng(0)
-    pix = _subset(depth, 600, rng)
+    pix, ev = _well_conditioned(vol, K, depth, T, o, 600, rng)
+    assert len(pix) >= 500
     g = rng.normal(size=len(pix)).astype(np.float32).astype(np.float64)
     gpos = (rng.normal(size=(len(pix), 3)) * 0.5).astype(np.float32).astype(np.float64)
     gd = np.zeros_like(depth)
@@ -68,8 +91,6 @@ def test_pose_and_sdf_gradients_match_fp64_central_differences(cuda, synth_mod, 
                               grad_position=cuda.from_numpy(gp).cuda(), grad_sdf=gsdf)
     assert skipped == 0
 
-    br = o.brackets(K.width, K.height, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)[pix[:, 1], pix[:, 0]]
-    ev = Evaluator(vol, VOXEL, K, pix, br)
     T64 = T.astype(np.float64)
 
     def loss(Tm, sdf=None):
@@ -80,7 +101,7 @@ def test_pose_and_sdf_gradients_match_fp64_central_differences(cuda, synth_mod, 
     base_depth = ev.depth(T64)
     assert np.abs(base_depth - depth[pix[:, 1], pix[:, 0]]).max() < 1e-5  # FP64 restatement agrees
     loss(T64)  # fix the hit-point taps too
-    h = 1e-4
+    h = H_POSE
     fd = np.zeros((3, 4))
     for r in range(3):
         for c in range(4):
@@ -96,7 +117,7 @@ def test_pose_and_sdf_gradients_match_fp64_central_differences(cuda, synth_mod, 
     assert np.all(ptrs >= 0)
     G = gsdf.view(-1, 512).cpu().numpy()[ptrs]
     top = np.argsort(-np.abs(G).ravel())[:20]
-    hs = 1e-5
+    hs = H_SDF
     for flat in top:
         sp, sm = vol.sdf.copy(), vol.sdf.copy()
         sp.ravel()[flat] += hs
@@ -116,12 +137,12 @@ def test_normals_match_fp64_sdf_gradient(cuda, synth_mod, oracle_mod):
     miss = depth >= 1e9
     assert np.all(nrm[miss] == 1e10)
     rng = np.random.default_rng(1)
-    pix = _subset(depth, 400, rng)
-    br = o.brackets(K.width, K.height, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)[pix[:, 1], pix[:, 0]]
-    ev = Evaluator(vol, VOXEL, K, pix, br)
+    pix, ev = _well_conditioned(vol, K, depth, T, o, 400, rng)
     _, n64, _, _, _ = ev.depth(T.astype(np.float64), want_normal=True)
+    ok = np.all(np.isfinite(n64), 1)
+    assert ok.mean() > 0.95
     got = nrm[pix[:, 1], pix[:, 0], :3].astype(np.float64)
-    assert np.abs(got - n64).max() < 1e-4
+    assert np.abs(got[ok] - n64[ok]).max() < 1e-4
     assert np.all(nrm[pix[:, 1], pix[:, 0], 3] == 0.0)
 
 
