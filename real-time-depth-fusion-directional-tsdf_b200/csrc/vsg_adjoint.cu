@@ -20,10 +20,14 @@
 // trilinear interpolations: d(trilinear)/d(position) is the weight
 // derivative, d/d(voxel sdf) is the tap's normalised weight.
 //
+// The recomputation is FP32 (it must retrace the forward's decisions); the
+// derivatives are evaluated at those FP32 points in double precision, so the
+// gradient carries no cancellation error of its own.
+//
 // Work layout: one thread per pixel on the forward's 8x4 warp tiles; pose
 // gradients reduced per warp by shuffles, per CTA in shared memory, then
-// across CTAs in double precision in a fixed order (deterministic); voxel
-// SDF gradients accumulated with float atomics into the caller's buffer.
+// across CTAs in a fixed order (deterministic), all in double; voxel SDF
+// gradients accumulated with float atomics into the caller's buffer.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -48,7 +52,7 @@ struct BackArgs {
     const float4* g_pos;    // may be null
     float* g_sdf;           // may be null
     float4* normals;        // vsg_render_normals output (null in backward)
-    float* partials;        // per CTA 12 floats
+    double* partials;       // per CTA 12 doubles
     unsigned int* skipped;
 };
 
@@ -57,12 +61,12 @@ struct BackArgs {
 // position and, on request, the scatter of g_f into the taps' SDF gradients.
 struct Sample {
     float f;
-    float gx, gy, gz;  // d f / d position
+    double gx, gy, gz;  // d f / d position
     bool ok;
 };
 
 __device__ Sample sample_grad(const SceneDev& s, float px, float py, float pz, float* g_sdf, float g_f) {
-    Sample out{0.0f, 0.0f, 0.0f, 0.0f, false};
+    Sample out{0.0f, 0.0, 0.0, 0.0, false};
     const float off = s.voxel;
     const float v = s.voxel;
     const float dx = px - off / 2.0f, dy = py - off / 2.0f, dz = pz - off / 2.0f;
@@ -104,18 +108,30 @@ __device__ Sample sample_grad(const SceneDev& s, float px, float py, float pz, f
     const float inv = 1.0f / vws;
     out.f = d * inv;
     out.ok = true;
-    float gx = 0.0f, gy = 0.0f, gz = 0.0f;
+    // derivatives in double at the FP32 point
+    double W = 0.0, D = 0.0;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         if (!valid[i]) continue;
-        const float tx = (i & 1) ? wx : (1.0f - wx), ty = (i & 2) ? wy : (1.0f - wy), tz = (i & 4) ? wz : (1.0f - wz);
-        const float r = (sdfv[i] - out.f) * inv;
-        gx += ((i & 1) ? 1.0f : -1.0f) * ty * tz * r;
-        gy += ((i & 2) ? 1.0f : -1.0f) * tx * tz * r;
-        gz += ((i & 4) ? 1.0f : -1.0f) * tx * ty * r;
-        if (g_sdf && g_f != 0.0f) atomicAdd(g_sdf + idx[i], g_f * (tx * ty * tz) * inv);
+        const double tw = ((i & 1) ? (double)wx : 1.0 - wx) * ((i & 2) ? (double)wy : 1.0 - wy) *
+                          ((i & 4) ? (double)wz : 1.0 - wz);
+        W += tw;
+        D += tw * sdfv[i];
     }
-    const float iv = 1.0f / v;  // d(frac(p / v - 1/2)) / dp
+    const double f = D / W;
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (!valid[i]) continue;
+        const double tx = (i & 1) ? (double)wx : 1.0 - wx, ty = (i & 2) ? (double)wy : 1.0 - wy,
+                     tz = (i & 4) ? (double)wz : 1.0 - wz;
+        const double r = ((double)sdfv[i] - f) / W;
+        gx += ((i & 1) ? 1.0 : -1.0) * ty * tz * r;
+        gy += ((i & 2) ? 1.0 : -1.0) * tx * tz * r;
+        gz += ((i & 4) ? 1.0 : -1.0) * tx * ty * r;
+        if (g_sdf && g_f != 0.0f) atomicAdd(g_sdf + idx[i], (float)((double)g_f * (tx * ty * tz) / W));
+    }
+    const double iv = 1.0 / (double)v;  // d(frac(p / v - 1/2)) / dp
     out.gx = gx * iv;
     out.gy = gy * iv;
     out.gz = gz * iv;
@@ -125,12 +141,12 @@ __device__ Sample sample_grad(const SceneDev& s, float px, float py, float pz, f
 // Regula falsi step, RayCastRender.cu:238-240, and its partial derivatives.
 __device__ __forceinline__ float rf(float a, float fa, float b, float fb) { return a + (fa / (fa - fb)) * (b - a); }
 
-__device__ __forceinline__ void rf_back(float a, float fa, float b, float fb, float g, float& ga, float& gfa, float& gb,
-                                        float& gfb) {
-    const float den = fa - fb;
-    const float t = fa / den;
-    const float ba = b - a;
-    ga += (1.0f - t) * g;
+__device__ __forceinline__ void rf_back(double a, double fa, double b, double fb, double g, double& ga, double& gfa,
+                                        double& gb, double& gfb) {
+    const double den = fa - fb;
+    const double t = fa / den;
+    const double ba = b - a;
+    ga += (1.0 - t) * g;
     gb += t * g;
     gfa += ba * (-fb / (den * den)) * g;
     gfb += ba * (fa / (den * den)) * g;
@@ -185,7 +201,7 @@ __device__ __forceinline__ Ray make_ray(const BackArgs& a, int x, int y) {
 // sample is invalid (cannot happen for a hit recorded by the same scene).
 struct Crossing {
     float P[4], F[4];
-    float G[4][3];  // d F / d position at each node
+    double G[4][3];  // d F / d position at each node
     int ia[3], ib[3];  // bracket (node indices) of regula-falsi steps 1..3
     float alpha;
 };
@@ -224,9 +240,9 @@ __global__ void __launch_bounds__(128) k_render_backward(BackArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
     const int y = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
-    float gT[12];
+    double gT[12];
 #pragma unroll
-    for (int i = 0; i < 12; ++i) gT[i] = 0.0f;
+    for (int i = 0; i < 12; ++i) gT[i] = 0.0;
     if (x < a.W && y < a.H) {
         const size_t pi = (size_t)y * a.W + x;
         const float depth = a.depth[pi];
@@ -242,27 +258,29 @@ __global__ void __launch_bounds__(128) k_render_backward(BackArgs a) {
                 atomicAdd(a.skipped, 1u);
             } else {
                 // outputs: depth = alpha / d2r, position = o + alpha wd
-                float g_alpha = gd / d2r + gp.x * r.wdx + gp.y * r.wdy + gp.z * r.wdz;
-                float go[3] = {gp.x, gp.y, gp.z};
-                float gw[3] = {c.alpha * gp.x, c.alpha * gp.y, c.alpha * gp.z};
-                float gP[4] = {0.0f, 0.0f, 0.0f, 0.0f}, gF[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                const double wd[3] = {r.wdx, r.wdy, r.wdz};
+                double g_alpha = (double)gd * (double)r.cdz + (double)gp.x * wd[0] + (double)gp.y * wd[1] +
+                                 (double)gp.z * wd[2];
+                double go[3] = {gp.x, gp.y, gp.z};
+                double gw[3] = {(double)c.alpha * gp.x, (double)c.alpha * gp.y, (double)c.alpha * gp.z};
+                double gP[4] = {0.0, 0.0, 0.0, 0.0}, gF[4] = {0.0, 0.0, 0.0, 0.0};
                 rf_back(c.P[c.ia[2]], c.F[c.ia[2]], c.P[c.ib[2]], c.F[c.ib[2]], g_alpha, gP[c.ia[2]], gF[c.ia[2]],
                         gP[c.ib[2]], gF[c.ib[2]]);
                 // nodes 3, 2 (regula-falsi points), then 1, 0 (bracket ends)
 #pragma unroll
                 for (int k = 3; k >= 0; --k) {
-                    const float gf = gF[k];
-                    if (gf != 0.0f) {
+                    const double gf = gF[k];
+                    if (gf != 0.0) {
                         const float t = c.P[k];
                         if (a.g_sdf)
-                            sample_grad(a.s, r.ox + t * r.wdx, r.oy + t * r.wdy, r.oz + t * r.wdz, a.g_sdf, gf);
+                            sample_grad(a.s, r.ox + t * r.wdx, r.oy + t * r.wdy, r.oz + t * r.wdz, a.g_sdf, (float)gf);
                         go[0] += gf * c.G[k][0];
                         go[1] += gf * c.G[k][1];
                         go[2] += gf * c.G[k][2];
                         gw[0] += gf * t * c.G[k][0];
                         gw[1] += gf * t * c.G[k][1];
                         gw[2] += gf * t * c.G[k][2];
-                        gP[k] += gf * (c.G[k][0] * r.wdx + c.G[k][1] * r.wdy + c.G[k][2] * r.wdz);
+                        gP[k] += gf * (c.G[k][0] * wd[0] + c.G[k][1] * wd[1] + c.G[k][2] * wd[2]);
                     }
                     if (k >= 2) {  // node k = RF of step k-1's bracket
                         const int s = k - 2;
@@ -271,14 +289,14 @@ __global__ void __launch_bounds__(128) k_render_backward(BackArgs a) {
                     }
                 }
                 // wd = u / |u|, u = R cd
-                float gu[3] = {gw[0], gw[1], gw[2]};
+                double gu[3] = {gw[0], gw[1], gw[2]};
                 if (r.wl > 1e-6f) {
-                    const float dot = gw[0] * r.wdx + gw[1] * r.wdy + gw[2] * r.wdz;
-                    gu[0] = (gw[0] - dot * r.wdx) / r.wl;
-                    gu[1] = (gw[1] - dot * r.wdy) / r.wl;
-                    gu[2] = (gw[2] - dot * r.wdz) / r.wl;
+                    const double dot = gw[0] * wd[0] + gw[1] * wd[1] + gw[2] * wd[2];
+                    gu[0] = (gw[0] - dot * wd[0]) / (double)r.wl;
+                    gu[1] = (gw[1] - dot * wd[1]) / (double)r.wl;
+                    gu[2] = (gw[2] - dot * wd[2]) / (double)r.wl;
                 }
-                const float cd[3] = {r.cdx, r.cdy, r.cdz};
+                const double cd[3] = {r.cdx, r.cdy, r.cdz};
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
 #pragma unroll
@@ -289,10 +307,10 @@ __global__ void __launch_bounds__(128) k_render_backward(BackArgs a) {
         }
     }
     // deterministic reduction: warp shuffles, then the CTA's four warps
-    __shared__ float red[4][12];
+    __shared__ double red[4][12];
 #pragma unroll
     for (int i = 0; i < 12; ++i) {
-        float v = gT[i];
+        double v = gT[i];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
         if (lane == 0) red[warp][i] = v;
@@ -305,11 +323,11 @@ __global__ void __launch_bounds__(128) k_render_backward(BackArgs a) {
     }
 }
 
-__global__ void k_reduce_pose(const float* partials, int n, double* out) {
+__global__ void k_reduce_pose(const double* partials, int n, double* out) {
     __shared__ double red[12][32];
     const int i = threadIdx.x / 32, lane = threadIdx.x % 32;  // 384 threads: 12 x 32
     double s = 0.0;
-    for (int k = lane; k < n; k += 32) s += (double)partials[(size_t)k * 12 + i];
+    for (int k = lane; k < n; k += 32) s += partials[(size_t)k * 12 + i];
     red[i][lane] = s;
     __syncthreads();
     if (lane == 0) {
@@ -392,7 +410,7 @@ int vsg_renderer_record(vsg_renderer* rh, int enable) {
         const size_t n = (size_t)r.w * r.h;
         const size_t ctas = (size_t)((r.w + 15) / 16) * ((r.h + 7) / 8);
         if (cudaMalloc(&r.bracket, n * sizeof(float2)) != cudaSuccess ||
-            cudaMalloc(&r.partials, ctas * 12 * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&r.partials, ctas * 12 * sizeof(double)) != cudaSuccess ||
             cudaMalloc(&r.skipped, sizeof(unsigned int)) != cudaSuccess) {
             cudaFree(r.bracket);
             cudaFree(r.partials);

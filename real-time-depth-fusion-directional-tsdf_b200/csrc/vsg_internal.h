@@ -54,7 +54,7 @@ struct Renderer {
     // gradient partials, skipped-pixel counter
     bool record = false;
     float2* bracket = nullptr;
-    float* partials = nullptr;
+    double* partials = nullptr;
     unsigned int* skipped = nullptr;
 };
 
