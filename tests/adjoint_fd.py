@@ -39,6 +39,91 @@ class Evaluator:
         self.br = np.asarray(brackets, np.float64)
         self.frozen = None
 
+    def freeze_fp32(self, T):
+        """Fix the discrete decisions by retracing the crossing in float32
+        with the GPU kernel's operation order (k_render_backward's recompute:
+        ray setup, tap rounding, trilinear sums, regula-falsi steps and their
+        sign tests), so finite differences follow exactly the branch the GPU
+        differentiated.  Returns the float32 depths."""
+        f32 = np.float32
+        K = self.K
+        T = np.asarray(T, np.float32)
+        x = self.pix[:, 0].astype(f32)
+        y = self.pix[:, 1].astype(f32)
+        cdx = (x - f32(K.cx)) / f32(K.fx)
+        cdy = (y - f32(K.cy)) / f32(K.fy)
+        cdz = np.ones_like(cdx)
+        cl = np.sqrt((cdx * cdx + cdy * cdy) + cdz * cdz)
+        m = cl > f32(1e-6)
+        cdx, cdy, cdz = np.where(m, cdx / cl, cdx), np.where(m, cdy / cl, cdy), np.where(m, cdz / cl, cdz)
+        wd = [(T[i, 0] * cdx + T[i, 1] * cdy) + T[i, 2] * cdz for i in range(3)]
+        wl = np.sqrt((wd[0] * wd[0] + wd[1] * wd[1]) + wd[2] * wd[2])
+        m = wl > f32(1e-6)
+        wd = [np.where(m, w / wl, w) for w in wd]
+        o = [T[0, 3], T[1, 3], T[2, 3]]
+        v = f32(self.v)
+        N = len(self.pix)
+        rows = np.arange(N)
+        P = np.zeros((N, 4), f32)
+        F = np.zeros((N, 4), f32)
+        P[:, 0], P[:, 1] = self.br[:, 0].astype(f32), self.br[:, 1].astype(f32)
+        taps, sides = [], []
+
+        def tapv(q):
+            sg = np.where(q > 0, f32(1), np.where(q < 0, f32(-1), f32(0)))
+            return np.floor(q + f32(0.5) * sg).astype(np.int64)
+
+        def sample(t):
+            p = [o[i] + t * wd[i] for i in range(3)]
+            dq = [p[i] - v / f32(2.0) for i in range(3)]
+            fq = [dq[i] / v for i in range(3)]
+            fl = np.stack([np.floor(q) for q in fq], 1).astype(np.float64)
+            t0 = np.stack([tapv(q) for q in fq], 1)
+            t1 = np.stack([tapv((dq[i] + v) / v) for i in range(3)], 1)
+            w = [q - np.floor(q) for q in fq]
+            idx = np.full((N, 8), -1, np.int64)
+            valid = np.zeros((N, 8), bool)
+            d = np.zeros(N, f32)
+            ws = np.zeros(N, f32)
+            for i in range(8):
+                vx = np.stack([t1[:, 0] if i & 1 else t0[:, 0], t1[:, 1] if i & 2 else t0[:, 1],
+                               t1[:, 2] if i & 4 else t0[:, 2]], 1)
+                blk, loc = vx >> 3, vx & 7
+                s = np.zeros(N, f32)
+                for n in range(N):
+                    r = self.vol.row.get(tuple(blk[n].tolist()))
+                    if r is not None:
+                        li = loc[n, 0] + 8 * loc[n, 1] + 64 * loc[n, 2]
+                        idx[n, i] = r * 512 + li
+                        valid[n, i] = self.vol.w[r, li] > 0
+                        s[n] = f32(self.vol.sdf[r, li])
+                tw = ((w[0] if i & 1 else f32(1) - w[0]) * (w[1] if i & 2 else f32(1) - w[1])) * \
+                     (w[2] if i & 4 else f32(1) - w[2])
+                d = np.where(valid[:, i], d + tw * s, d)
+                ws = np.where(valid[:, i], ws + tw, ws)
+            taps.append({"fl": fl, "idx": idx, "valid": valid})
+            return d * (f32(1.0) / ws)
+
+        F[:, 0] = sample(P[:, 0])
+        F[:, 1] = sample(P[:, 1])
+        ia = np.zeros(N, np.int64)
+        ib = np.ones(N, np.int64)
+        for k in (2, 3):
+            a, fa, b, fb = P[rows, ia], F[rows, ia], P[rows, ib], F[rows, ib]
+            P[:, k] = a + (fa / (fa - fb)) * (b - a)
+            F[:, k] = sample(P[:, k])
+            keep = F[rows, ia] * F[:, k] > f32(0)
+            sides.append(keep)
+            ia = np.where(keep, k, ia)
+            ib = np.where(keep, ib, k)
+        a, fa, b, fb = P[rows, ia], F[rows, ia], P[rows, ib], F[rows, ib]
+        alpha = a + (fa / (fa - fb)) * (b - a)
+        d2r = f32(1.0) / cdz
+        self.frozen = {"taps": taps, "side": sides}
+        hit_p = np.stack([o[i] + alpha * wd[i] for i in range(3)], 1).astype(np.float64)
+        self.frozen["hit_taps"] = self._taps(hit_p)
+        return alpha / d2r
+
     def rays(self, T):
         K = self.K
         x, y = self.pix[:, 0], self.pix[:, 1]

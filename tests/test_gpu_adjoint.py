@@ -63,12 +63,12 @@ def _well_conditioned(vol, K, depth, T, o, n, rng):
     pix = _subset(depth, 3 * n, rng)
     br = o.brackets(K.width, K.height, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)[pix[:, 1], pix[:, 0]]
     ev = Evaluator(vol, VOXEL, K, pix, br)
-    d64 = ev.depth(T.astype(np.float64))
-    same = np.abs(d64 - depth[pix[:, 1], pix[:, 0]]) < 1e-6  # FP64 took the FP32 march's decisions
-    assert same.mean() > 0.99
-    keep = np.nonzero((ev.weight_sums(T.astype(np.float64)) >= MIN_WEIGHT_SUM) & same)[0][:n]
+    d32 = ev.freeze_fp32(T)  # the GPU's decisions, retraced in float32
+    assert np.array_equal(d32.view(np.uint32), depth[pix[:, 1], pix[:, 0]].view(np.uint32))
+    keep = np.nonzero(ev.weight_sums(T.astype(np.float64)) >= MIN_WEIGHT_SUM)[0][:n]
     pix, br = pix[keep], br[keep]
     ev = Evaluator(vol, VOXEL, K, pix, br)
+    ev.freeze_fp32(T)
     return pix, ev
 
 
@@ -101,8 +101,7 @@ def test_pose_and_sdf_gradients_match_fp64_central_differences(cuda, synth_mod, 
         return float((g * d).sum() + (gpos * pos).sum())
 
     base_depth = ev.depth(T64)
-    assert np.abs(base_depth - depth[pix[:, 1], pix[:, 0]]).max() < 1e-6  # FP64 restatement agrees
-    loss(T64)  # fix the hit-point taps too
+    assert np.abs(base_depth - depth[pix[:, 1], pix[:, 0]]).max() < 1e-4  # FP64 restatement agrees
     h = H_POSE
     fd = np.zeros((3, 4))
     for r in range(3):
