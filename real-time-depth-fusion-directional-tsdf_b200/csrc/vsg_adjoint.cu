@@ -20,9 +20,13 @@
 // trilinear interpolations: d(trilinear)/d(position) is the weight
 // derivative, d/d(voxel sdf) is the tap's normalised weight.
 //
-// The recomputation is FP32 (it must retrace the forward's decisions); the
-// derivatives are evaluated at those FP32 points in double precision, so the
-// gradient carries no cancellation error of its own.
+// The recomputation is FP32: it retraces the forward's decisions (tap voxels,
+// weight bases, regula-falsi sides) and checks the depth.  The smooth
+// function those decisions define is then evaluated again in double --
+// ray, sample points, trilinear values, regula-falsi steps -- and
+// differentiated there: near the root a sample's FP32 value carries a large
+// relative rounding error that would otherwise enter the regula-falsi
+// derivatives.
 //
 // Work layout: one thread per pixel on the forward's 8x4 warp tiles; pose
 // gradients reduced per warp by shuffles, per CTA in shared memory, then
@@ -65,7 +69,15 @@ struct Sample {
     bool ok;
 };
 
-__device__ Sample sample_grad(const SceneDev& s, float px, float py, float pz, float* g_sdf, float g_f) {
+// The frozen decisions of one sample: tap voxel coordinates and the integer
+// base of its trilinear weights.
+struct NodeTaps {
+    int t0[3], t1[3];
+    float fl[3];
+};
+
+__device__ Sample sample_grad(const SceneDev& s, float px, float py, float pz, float* g_sdf, float g_f,
+                              NodeTaps* nt = nullptr) {
     Sample out{0.0f, 0.0, 0.0, 0.0, false};
     const float off = s.voxel;
     const float v = s.voxel;
@@ -77,6 +89,17 @@ __device__ Sample sample_grad(const SceneDev& s, float px, float py, float pz, f
     const int ax0 = tap_voxel(fx), ay0 = tap_voxel(fy), az0 = tap_voxel(fz);
     const int ax1 = tap_voxel(div_v(dx + off, v, y, fast)), ay1 = tap_voxel(div_v(dy + off, v, y, fast)),
               az1 = tap_voxel(div_v(dz + off, v, y, fast));
+    if (nt) {
+        nt->t0[0] = ax0;
+        nt->t0[1] = ay0;
+        nt->t0[2] = az0;
+        nt->t1[0] = ax1;
+        nt->t1[1] = ay1;
+        nt->t1[2] = az1;
+        nt->fl[0] = floorf(fx);
+        nt->fl[1] = floorf(fy);
+        nt->fl[2] = floorf(fz);
+    }
     float d = 0.0f, vws = 0.0f;
     float sdfv[8];
     size_t idx[8];
@@ -138,8 +161,65 @@ __device__ Sample sample_grad(const SceneDev& s, float px, float py, float pz, f
     return out;
 }
 
+// The same trilinear sample in double at a double position, with the taps and
+// weight bases frozen: value, position gradient, and (on request) the
+// scatter of g_f into the taps' SDF gradients.
+__device__ bool sample64(const SceneDev& s, const double p[3], const NodeTaps& nt, double& f, double g[3],
+                         float* g_sdf, double g_f) {
+    const double v = s.voxel;
+    double w[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) w[a] = (p[a] - v / 2.0) / v - (double)nt.fl[a];
+    double sdfv[8];
+    size_t idx[8];
+    bool valid[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int vx = (i & 1) ? nt.t1[0] : nt.t0[0], vy = (i & 2) ? nt.t1[1] : nt.t0[1],
+                  vz = (i & 4) ? nt.t1[2] : nt.t0[2];
+        const int b = block_ptr(s, vox_to_block(vx), vox_to_block(vy), vox_to_block(vz));
+        valid[i] = false;
+        sdfv[i] = 0.0;
+        idx[i] = 0;
+        if (b >= 0) {
+            idx[i] = (size_t)b * kVoxPerBlock + vox_local(vx) + vox_local(vy) * kBlock + vox_local(vz) * kBlock * kBlock;
+            const uint2 raw = __ldg(reinterpret_cast<const uint2*>(s.voxels + idx[i]));
+            if ((raw.y >> 24) != 0u) {
+                valid[i] = true;
+                sdfv[i] = (double)__uint_as_float(raw.x);
+            }
+        }
+    }
+    double W = 0.0, D = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (!valid[i]) continue;
+        const double tw = ((i & 1) ? w[0] : 1.0 - w[0]) * ((i & 2) ? w[1] : 1.0 - w[1]) * ((i & 4) ? w[2] : 1.0 - w[2]);
+        W += tw;
+        D += tw * sdfv[i];
+    }
+    if (!(W > 0.0)) return false;
+    f = D / W;
+    g[0] = g[1] = g[2] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (!valid[i]) continue;
+        const double tx = (i & 1) ? w[0] : 1.0 - w[0], ty = (i & 2) ? w[1] : 1.0 - w[1],
+                     tz = (i & 4) ? w[2] : 1.0 - w[2];
+        const double r = (sdfv[i] - f) / W;
+        g[0] += ((i & 1) ? 1.0 : -1.0) * ty * tz * r;
+        g[1] += ((i & 2) ? 1.0 : -1.0) * tx * tz * r;
+        g[2] += ((i & 4) ? 1.0 : -1.0) * tx * ty * r;
+        if (g_sdf && g_f != 0.0) atomicAdd(g_sdf + idx[i], (float)(g_f * (tx * ty * tz) / W));
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) g[a] /= v;
+    return true;
+}
+
 // Regula falsi step, RayCastRender.cu:238-240, and its partial derivatives.
 __device__ __forceinline__ float rf(float a, float fa, float b, float fb) { return a + (fa / (fa - fb)) * (b - a); }
+__device__ __forceinline__ double rf64(double a, double fa, double b, double fb) { return a + (fa / (fa - fb)) * (b - a); }
 
 __device__ __forceinline__ void rf_back(double a, double fa, double b, double fb, double g, double& ga, double& gfa,
                                         double& gb, double& gfb) {
@@ -202,6 +282,7 @@ __device__ __forceinline__ Ray make_ray(const BackArgs& a, int x, int y) {
 struct Crossing {
     float P[4], F[4];
     double G[4][3];  // d F / d position at each node
+    NodeTaps taps[4];
     int ia[3], ib[3];  // bracket (node indices) of regula-falsi steps 1..3
     float alpha;
 };
@@ -217,7 +298,8 @@ __device__ bool recompute(const SceneDev& s, const Ray& r, float a0, float b0, C
             c.P[k] = rf(c.P[ia], c.F[ia], c.P[ib], c.F[ib]);
         }
         const float t = c.P[k];
-        const Sample sm = sample_grad(s, r.ox + t * r.wdx, r.oy + t * r.wdy, r.oz + t * r.wdz, nullptr, 0.0f);
+        const Sample sm = sample_grad(s, r.ox + t * r.wdx, r.oy + t * r.wdy, r.oz + t * r.wdz, nullptr, 0.0f,
+                                      &c.taps[k]);
         if (!sm.ok) return false;
         c.F[k] = sm.f;
         c.G[k][0] = sm.gx;
@@ -257,51 +339,85 @@ __global__ void __launch_bounds__(128) k_render_backward(BackArgs a) {
                 __float_as_uint(c.alpha / d2r) != __float_as_uint(depth)) {
                 atomicAdd(a.skipped, 1u);
             } else {
-                // outputs: depth = alpha / d2r, position = o + alpha wd
-                const double wd[3] = {r.wdx, r.wdy, r.wdz};
-                double g_alpha = (double)gd * (double)r.cdz + (double)gp.x * wd[0] + (double)gp.y * wd[1] +
+                // the smooth function of the frozen decisions, in double
+                double cd[3] = {((double)x - a.cx) / a.fx, ((double)y - a.cy) / a.fy, 1.0};
+                {
+                    const double cl = sqrt(cd[0] * cd[0] + cd[1] * cd[1] + cd[2] * cd[2]);
+                    cd[0] /= cl;
+                    cd[1] /= cl;
+                    cd[2] /= cl;
+                }
+                const float* T = a.pose.T;
+                double u[3], wd[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    u[i] = (double)T[4 * i] * cd[0] + (double)T[4 * i + 1] * cd[1] + (double)T[4 * i + 2] * cd[2];
+                const double wl = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) wd[i] = u[i] / wl;
+                const double o[3] = {T[3], T[7], T[11]};
+                double P[4] = {0.0, 0.0, 0.0, 0.0}, F[4] = {0.0, 0.0, 0.0, 0.0}, G[4][3] = {};
+                P[0] = br.x;
+                P[1] = br.y;
+                bool ok = true;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (k >= 2) {
+                        const int s = k - 2;
+                        P[k] = rf64(P[c.ia[s]], F[c.ia[s]], P[c.ib[s]], F[c.ib[s]]);
+                    }
+                    const double q[3] = {o[0] + P[k] * wd[0], o[1] + P[k] * wd[1], o[2] + P[k] * wd[2]};
+                    ok = ok && sample64(a.s, q, c.taps[k], F[k], G[k], nullptr, 0.0);
+                }
+                if (!ok) atomicAdd(a.skipped, 1u);
+                const double alpha = ok ? rf64(P[c.ia[2]], F[c.ia[2]], P[c.ib[2]], F[c.ib[2]]) : 0.0;
+                // outputs: depth = alpha cd_z, position = o + alpha wd
+                double g_alpha = (double)gd * cd[2] + (double)gp.x * wd[0] + (double)gp.y * wd[1] +
                                  (double)gp.z * wd[2];
                 double go[3] = {gp.x, gp.y, gp.z};
-                double gw[3] = {(double)c.alpha * gp.x, (double)c.alpha * gp.y, (double)c.alpha * gp.z};
+                double gw[3] = {alpha * gp.x, alpha * gp.y, alpha * gp.z};
                 double gP[4] = {0.0, 0.0, 0.0, 0.0}, gF[4] = {0.0, 0.0, 0.0, 0.0};
-                rf_back(c.P[c.ia[2]], c.F[c.ia[2]], c.P[c.ib[2]], c.F[c.ib[2]], g_alpha, gP[c.ia[2]], gF[c.ia[2]],
-                        gP[c.ib[2]], gF[c.ib[2]]);
-                // nodes 3, 2 (regula-falsi points), then 1, 0 (bracket ends)
+                if (ok) {
+                    rf_back(P[c.ia[2]], F[c.ia[2]], P[c.ib[2]], F[c.ib[2]], g_alpha, gP[c.ia[2]], gF[c.ia[2]],
+                            gP[c.ib[2]], gF[c.ib[2]]);
+                    // nodes 3, 2 (regula-falsi points), then 1, 0 (bracket ends)
 #pragma unroll
-                for (int k = 3; k >= 0; --k) {
-                    const double gf = gF[k];
-                    if (gf != 0.0) {
-                        const float t = c.P[k];
-                        if (a.g_sdf)
-                            sample_grad(a.s, r.ox + t * r.wdx, r.oy + t * r.wdy, r.oz + t * r.wdz, a.g_sdf, (float)gf);
-                        go[0] += gf * c.G[k][0];
-                        go[1] += gf * c.G[k][1];
-                        go[2] += gf * c.G[k][2];
-                        gw[0] += gf * t * c.G[k][0];
-                        gw[1] += gf * t * c.G[k][1];
-                        gw[2] += gf * t * c.G[k][2];
-                        gP[k] += gf * (c.G[k][0] * wd[0] + c.G[k][1] * wd[1] + c.G[k][2] * wd[2]);
+                    for (int k = 3; k >= 0; --k) {
+                        const double gf = gF[k];
+                        if (gf != 0.0) {
+                            if (a.g_sdf) {
+                                const double q[3] = {o[0] + P[k] * wd[0], o[1] + P[k] * wd[1], o[2] + P[k] * wd[2]};
+                                double fdummy, gdummy[3];
+                                sample64(a.s, q, c.taps[k], fdummy, gdummy, a.g_sdf, gf);
+                            }
+                            go[0] += gf * G[k][0];
+                            go[1] += gf * G[k][1];
+                            go[2] += gf * G[k][2];
+                            gw[0] += gf * P[k] * G[k][0];
+                            gw[1] += gf * P[k] * G[k][1];
+                            gw[2] += gf * P[k] * G[k][2];
+                            gP[k] += gf * (G[k][0] * wd[0] + G[k][1] * wd[1] + G[k][2] * wd[2]);
+                        }
+                        if (k >= 2) {  // node k = RF of step k-1's bracket
+                            const int s = k - 2;
+                            rf_back(P[c.ia[s]], F[c.ia[s]], P[c.ib[s]], F[c.ib[s]], gP[k], gP[c.ia[s]], gF[c.ia[s]],
+                                    gP[c.ib[s]], gF[c.ib[s]]);
+                        }
                     }
-                    if (k >= 2) {  // node k = RF of step k-1's bracket
-                        const int s = k - 2;
-                        rf_back(c.P[c.ia[s]], c.F[c.ia[s]], c.P[c.ib[s]], c.F[c.ib[s]], gP[k], gP[c.ia[s]],
-                                gF[c.ia[s]], gP[c.ib[s]], gF[c.ib[s]]);
+                    // wd = u / |u|, u = R cd
+                    double gu[3];
+                    {
+                        const double dot = gw[0] * wd[0] + gw[1] * wd[1] + gw[2] * wd[2];
+                        gu[0] = (gw[0] - dot * wd[0]) / wl;
+                        gu[1] = (gw[1] - dot * wd[1]) / wl;
+                        gu[2] = (gw[2] - dot * wd[2]) / wl;
                     }
-                }
-                // wd = u / |u|, u = R cd
-                double gu[3] = {gw[0], gw[1], gw[2]};
-                if (r.wl > 1e-6f) {
-                    const double dot = gw[0] * wd[0] + gw[1] * wd[1] + gw[2] * wd[2];
-                    gu[0] = (gw[0] - dot * wd[0]) / (double)r.wl;
-                    gu[1] = (gw[1] - dot * wd[1]) / (double)r.wl;
-                    gu[2] = (gw[2] - dot * wd[2]) / (double)r.wl;
-                }
-                const double cd[3] = {r.cdx, r.cdy, r.cdz};
 #pragma unroll
-                for (int i = 0; i < 3; ++i) {
+                    for (int i = 0; i < 3; ++i) {
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) gT[4 * i + j] = gu[i] * cd[j];
-                    gT[4 * i + 3] = go[i];
+                        for (int j = 0; j < 3; ++j) gT[4 * i + j] = gu[i] * cd[j];
+                        gT[4 * i + 3] = go[i];
+                    }
                 }
             }
         }
