@@ -199,9 +199,12 @@ VSG_API int vsg_renderer_record(vsg_renderer* r, int enable);
  * rotation entries 0-2, 4-6, 8-10, translation 3, 7, 11).  grad_sdf: device
  * float[num_sdf_blocks * 512] indexed like the voxel pool (pool block * 512 +
  * x + 8y + 64z), ACCUMULATED with atomics (NULL = skip).  n_skipped: if not
- * NULL, the call synchronises and stores the number of hit pixels whose
- * recomputation did not reproduce the rendered depth (0 when the
- * preconditions hold). */
+ * NULL, the call synchronises and stores the number of hit pixels left out:
+ * those whose recomputation did not reproduce the rendered depth (none when
+ * the preconditions hold) and those where the depth has no derivative (a
+ * regula-falsi step between two equal values, e.g. samples that read only
+ * truncation-clamped voxels, where the forward step is decided by
+ * rounding). */
 VSG_API int vsg_render_backward(const vsg_renderer* r, const vsg_scene* s, const float pose[16], float fx, float fy,
                                 float cx, float cy, const float* grad_depth, const float* grad_position,
                                 double* grad_pose, float* grad_sdf, uint32_t* n_skipped, vsg_stream_t stream);

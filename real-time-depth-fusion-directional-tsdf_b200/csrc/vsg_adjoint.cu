@@ -364,13 +364,19 @@ __global__ void __launch_bounds__(128) k_render_backward(BackArgs a) {
                 for (int k = 0; k < 4; ++k) {
                     if (k >= 2) {
                         const int s = k - 2;
+                        ok = ok && F[c.ia[s]] != F[c.ib[s]];
                         P[k] = rf64(P[c.ia[s]], F[c.ia[s]], P[c.ib[s]], F[c.ib[s]]);
                     }
                     const double q[3] = {o[0] + P[k] * wd[0], o[1] + P[k] * wd[1], o[2] + P[k] * wd[2]};
                     ok = ok && sample64(a.s, q, c.taps[k], F[k], G[k], nullptr, 0.0);
                 }
-                if (!ok) atomicAdd(a.skipped, 1u);
+                // a step whose two values coincide in exact arithmetic (e.g. both
+                // samples read truncation-clamped voxels only) has no derivative:
+                // the forward's step there was decided by rounding noise
+                ok = ok && F[c.ia[2]] != F[c.ib[2]];
                 const double alpha = ok ? rf64(P[c.ia[2]], F[c.ia[2]], P[c.ib[2]], F[c.ib[2]]) : 0.0;
+                ok = ok && isfinite(alpha);
+                if (!ok) atomicAdd(a.skipped, 1u);
                 // outputs: depth = alpha cd_z, position = o + alpha wd
                 double g_alpha = (double)gd * cd[2] + (double)gp.x * wd[0] + (double)gp.y * wd[1] +
                                  (double)gp.z * wd[2];
