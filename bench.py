@@ -277,6 +277,7 @@ def run_ours(args):
     line["marching_cubes"] = mc_measure(sc, peak)
     line["surface_points"] = points_measure(sc, peak)
     line["streaming"] = stream_measure(sc)
+    line["adjoint"] = adjoint_measure(sc, frames, K)
     if not args.no_e2e:
         line["e2e"] = e2e(args, frames, K, sc, rr)
     if not args.no_batched:
@@ -344,6 +345,73 @@ def points_measure(sc, peak: float, reps: int = 10) -> dict:
     gbs = alg / (ms * 1e-3) / 1e9
     return {"points": n, "ms_per_launch": ms, "alg_bytes": alg, "achieved_gbs": gbs, "frac_of_peak": gbs / peak,
             "launches_timed": int(kcnt[5])}
+
+
+def adjoint_measure(sc, frames, K, reps: int = 10) -> dict:
+    """Ray-cast adjoint at the last frame's pose of the final volume: device
+    time of a recording render plus vsg_render_backward (dL/ddepth = 1 on
+    every hit pixel, pose and voxel-SDF gradients), and a 20-step Adam pose
+    refinement through the torch wrapper from a pose perturbed by ~1 cm /
+    1 degree (Huber depth loss against the render at the true pose)."""
+    import torch
+
+    import vsg
+
+    W, H = K.width, K.height
+    rr = vsg.Renderer(W, H)
+    rr.record(True)
+    T = np.asarray(frames[-1].pose, np.float32)
+    gsdf = torch.zeros(sc.params.num_sdf_blocks * 512, dtype=torch.float32, device="cuda")
+    rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
+    gd = (rr.depth_tensor() < 1e9).float()
+    hits = int(gd.sum().item())
+    for _ in range(3):
+        rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
+        rr.backward(sc, T, K.fx, K.fy, K.cx, K.cy, grad_depth=gd, grad_sdf=gsdf)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    fwd = bwd = 0.0
+    skipped = 0
+    for _ in range(reps):
+        e[0].record()
+        rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
+        e[1].record()
+        _, skipped = rr.backward(sc, T, K.fx, K.fy, K.cx, K.cy, grad_depth=gd, grad_sdf=gsdf)
+        e[2].record()
+        torch.cuda.synchronize()
+        fwd += e[0].elapsed_time(e[1])
+        bwd += e[1].elapsed_time(e[2])
+    # pose refinement
+    T_true = torch.tensor(T, dtype=torch.float64)
+    target = vsg.render_depth(sc, rr, T_true.float(), K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D).detach()
+    rng = np.random.default_rng(7)
+    d0 = np.concatenate([rng.normal(size=3) / np.sqrt(3) * np.deg2rad(1.0), rng.normal(size=3) / np.sqrt(3) * 0.01])
+    xi = torch.tensor(d0, dtype=torch.float64, requires_grad=True)
+    opt = torch.optim.Adam([xi], lr=2e-3)
+
+    def se3(x):
+        w, t = x[:3], x[3:]
+        th = torch.sqrt((w * w).sum() + 1e-18)
+        z = torch.zeros((), dtype=x.dtype)
+        Wm = torch.stack([torch.stack([z, -w[2], w[1]]), torch.stack([w[2], z, -w[0]]),
+                          torch.stack([-w[1], w[0], z])])
+        R = torch.eye(3, dtype=x.dtype) + torch.sin(th) / th * Wm + (1 - torch.cos(th)) / th ** 2 * (Wm @ Wm)
+        return torch.cat([torch.cat([R, t[:, None]], 1), torch.eye(4, dtype=x.dtype)[3:]], 0)
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(20):
+        opt.zero_grad()
+        d = vsg.render_depth(sc, rr, (T_true @ se3(xi)).float(), K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
+        m = (d < 1e9) & (target < 1e9)
+        torch.nn.functional.huber_loss(d[m], target[m], delta=0.01).backward()
+        opt.step()
+    torch.cuda.synchronize()
+    step_ms = (time.perf_counter() - t0) * 1e3 / 20
+    rr.close()
+    return {"hit_pixels": hits, "render_record_ms": fwd / reps, "backward_ms": bwd / reps,
+            "skipped_pixels": skipped, "refine": {"steps": 20, "ms_per_step_wall": step_ms,
+                                                  "initial_err": float(np.linalg.norm(d0)),
+                                                  "final_err": float(xi.detach().norm())}}
 
 
 def stream_measure(sc) -> dict:
