@@ -198,16 +198,21 @@ VSG_API int vsg_renderer_record(vsg_renderer* r, int enable);
  * receiving dL/dT for the row-major 3x4 camera->world matrix (written;
  * rotation entries 0-2, 4-6, 8-10, translation 3, 7, 11).  grad_sdf: device
  * float[num_sdf_blocks * 512] indexed like the voxel pool (pool block * 512 +
- * x + 8y + 64z), ACCUMULATED with atomics (NULL = skip).  n_skipped: if not
+ * x + 8y + 64z), ACCUMULATED with atomics (NULL = skip).  min_weight_sum:
+ * leave out pixels where a sample of the crossing renormalises over valid
+ * taps whose trilinear weights sum to less (0 keeps every pixel; near the
+ * edge of observed space that sum is small and the depth -- hence its
+ * gradient -- is steep: 0.5 suits pose optimisation).  n_skipped: if not
  * NULL, the call synchronises and stores the number of hit pixels left out:
  * those whose recomputation did not reproduce the rendered depth (none when
- * the preconditions hold) and those where the depth has no derivative (a
- * regula-falsi step between two equal values, e.g. samples that read only
- * truncation-clamped voxels, where the forward step is decided by
- * rounding). */
+ * the preconditions hold), those below min_weight_sum, and those where the
+ * depth has no derivative (a regula-falsi step between two equal values,
+ * e.g. samples that read only truncation-clamped voxels, where the forward
+ * step is decided by rounding). */
 VSG_API int vsg_render_backward(const vsg_renderer* r, const vsg_scene* s, const float pose[16], float fx, float fy,
                                 float cx, float cy, const float* grad_depth, const float* grad_position,
-                                double* grad_pose, float* grad_sdf, uint32_t* n_skipped, vsg_stream_t stream);
+                                double* grad_pose, float* grad_sdf, float min_weight_sum, uint32_t* n_skipped,
+                                vsg_stream_t stream);
 /* Pool indices of the given blocks (host int32 coords[n*3] -> host int32
  * ptrs[n], -1 = not allocated): the row of grad_sdf, or of the voxel pool,
  * that holds each block.  Synchronises. */

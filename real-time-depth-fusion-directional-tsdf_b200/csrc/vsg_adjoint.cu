@@ -57,6 +57,7 @@ struct BackArgs {
     float* g_sdf;           // may be null
     float4* normals;        // vsg_render_normals output (null in backward)
     double* partials;       // per CTA 12 doubles
+    float min_w;            // leave out pixels whose samples renormalise over less weight
     unsigned int* skipped;
 };
 
@@ -165,7 +166,7 @@ __device__ Sample sample_grad(const SceneDev& s, float px, float py, float pz, f
 // weight bases frozen: value, position gradient, and (on request) the
 // scatter of g_f into the taps' SDF gradients.
 __device__ bool sample64(const SceneDev& s, const double p[3], const NodeTaps& nt, double& f, double g[3],
-                         float* g_sdf, double g_f) {
+                         float* g_sdf, double g_f, double* wsum = nullptr) {
     const double v = s.voxel;
     double w[3];
 #pragma unroll
@@ -198,6 +199,7 @@ __device__ bool sample64(const SceneDev& s, const double p[3], const NodeTaps& n
         W += tw;
         D += tw * sdfv[i];
     }
+    if (wsum) *wsum = W;
     if (!(W > 0.0)) return false;
     f = D / W;
     g[0] = g[1] = g[2] = 0.0;
@@ -368,7 +370,9 @@ __global__ void __launch_bounds__(128) k_render_backward(BackArgs a) {
                         P[k] = rf64(P[c.ia[s]], F[c.ia[s]], P[c.ib[s]], F[c.ib[s]]);
                     }
                     const double q[3] = {o[0] + P[k] * wd[0], o[1] + P[k] * wd[1], o[2] + P[k] * wd[2]};
-                    ok = ok && sample64(a.s, q, c.taps[k], F[k], G[k], nullptr, 0.0);
+                    double wsum = 0.0;
+                    ok = ok && sample64(a.s, q, c.taps[k], F[k], G[k], nullptr, 0.0, &wsum);
+                    ok = ok && wsum >= (double)a.min_w;
                 }
                 // a step whose two values coincide in exact arithmetic (e.g. both
                 // samples read truncation-clamped voxels only) has no derivative:
@@ -549,8 +553,8 @@ int vsg_renderer_record(vsg_renderer* rh, int enable) {
 
 int vsg_render_backward(const vsg_renderer* rh, const vsg_scene* s, const float pose[16], float fx, float fy,
                         float cx, float cy, const float* grad_depth, const float* grad_position, double* grad_pose,
-                        float* grad_sdf, uint32_t* n_skipped, vsg_stream_t stream) {
-    if (!rh || !s || !pose || !grad_pose) return VSG_ERR_INVALID_ARG;
+                        float* grad_sdf, float min_weight_sum, uint32_t* n_skipped, vsg_stream_t stream) {
+    if (!rh || !s || !pose || !grad_pose || !(min_weight_sum >= 0.0f)) return VSG_ERR_INVALID_ARG;
     const vsg::Renderer& r = rh->impl;
     vsg::BackArgs a;
     const int rc = vsg::prepare(r, s->impl, pose, fx, fy, cx, cy, a);
@@ -558,6 +562,7 @@ int vsg_render_backward(const vsg_renderer* rh, const vsg_scene* s, const float 
     a.g_depth = grad_depth;
     a.g_pos = reinterpret_cast<const float4*>(grad_position);
     a.g_sdf = grad_sdf;
+    a.min_w = min_weight_sum;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (cudaMemsetAsync(r.skipped, 0, sizeof(unsigned int), st) != cudaSuccess) return VSG_ERR_CUDA;
     const dim3 grid((r.w + 15) / 16, (r.h + 7) / 8);

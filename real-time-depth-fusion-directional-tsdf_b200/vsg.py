@@ -136,7 +136,7 @@ def lib() -> ctypes.CDLL:
         L.vsg_points_save_ply.argtypes = [_P, ctypes.c_char_p]
         L.vsg_renderer_record.argtypes = [_P, _I]
         L.vsg_scene_lookup_blocks.argtypes = [_P, _P, ctypes.c_uint32, _P]
-        L.vsg_render_backward.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, _P, _P, _P,
+        L.vsg_render_backward.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, _P, _P, _P, _F,
                                           ctypes.POINTER(ctypes.c_uint32), _P]
         L.vsg_render_normals.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, ctypes.POINTER(ctypes.c_uint32), _P]
         _lib = L
@@ -185,11 +185,13 @@ class _DeviceArray:
                                          "version": 3}
 
 
-def render_depth(scene, renderer, pose, fx, fy, cx, cy, min_depth, max_depth):
+def render_depth(scene, renderer, pose, fx, fy, cx, cy, min_depth, max_depth, min_weight_sum: float = 0.5):
     """Differentiable ray cast (torch autograd): depth (H,W) of `scene` seen
     from `pose` (a (4,4) float32 torch tensor, camera->world; may require
     grad).  The backward pass returns dL/dpose (rows 0-2; row 3 zero) through
-    vsg_render_backward.  Misses hold 1e10 and carry no gradient."""
+    vsg_render_backward.  Misses hold 1e10 and carry no gradient; so do
+    pixels whose crossing samples renormalise over less than min_weight_sum
+    of trilinear weight (steep near the edge of observed space)."""
     import torch
 
     class _Render(torch.autograd.Function):
@@ -205,7 +207,8 @@ def render_depth(scene, renderer, pose, fx, fy, cx, cy, min_depth, max_depth):
         @staticmethod
         def backward(ctx, g):
             g = g.contiguous().to(torch.float32)
-            gT, skipped = renderer.backward(scene, ctx.Th, fx, fy, cx, cy, grad_depth=g)
+            gT, skipped = renderer.backward(scene, ctx.Th, fx, fy, cx, cy, grad_depth=g,
+                                            min_weight_sum=min_weight_sum)
             out = torch.zeros((4, 4), dtype=torch.float64)
             out[:3] = torch.from_numpy(gT)
             return out.to(device=ctx.dev, dtype=ctx.dtype)
@@ -351,7 +354,7 @@ class Renderer:
         check("vsg_renderer_record", self.L.vsg_renderer_record(self.h, int(enable)))
 
     def backward(self, scene: "Scene", pose, fx, fy, cx, cy, grad_depth=None, grad_position=None, grad_sdf=None,
-                 stream=None):
+                 min_weight_sum: float = 0.0, stream=None):
         """Reverse mode through the last recorded render.  grad_depth (H,W) /
         grad_position (H,W,4): device float32 tensors of dL/d output (None = 0).
         grad_sdf: device float32 tensor of num_sdf_blocks*512 entries the voxel
@@ -365,7 +368,7 @@ class Renderer:
         skipped = ctypes.c_uint32()
         check("vsg_render_backward", self.L.vsg_render_backward(
             self.h, scene.h, _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _dptr(grad_depth), _dptr(grad_position),
-            _dptr(gp), _dptr(grad_sdf), ctypes.byref(skipped), _stream(stream)))
+            _dptr(gp), _dptr(grad_sdf), _F(min_weight_sum), ctypes.byref(skipped), _stream(stream)))
         return gp.cpu().numpy().reshape(3, 4), int(skipped.value)
 
     def normals(self, scene: "Scene", pose, fx, fy, cx, cy, out=None, stream=None):
