@@ -386,7 +386,7 @@ def adjoint_measure(sc, frames, K, reps: int = 10) -> dict:
     rng = np.random.default_rng(7)
     d0 = np.concatenate([rng.normal(size=3) / np.sqrt(3) * np.deg2rad(1.0), rng.normal(size=3) / np.sqrt(3) * 0.01])
     xi = torch.tensor(d0, dtype=torch.float64, requires_grad=True)
-    opt = torch.optim.Adam([xi], lr=2e-3)
+    opt = torch.optim.Adam([xi], lr=5e-4)
 
     def se3(x):
         w, t = x[:3], x[3:]
