@@ -149,6 +149,17 @@ VSG_API int vsg_integrate_noalloc(vsg_scene* s, const float* pointmap, const uin
                                   int w, int h, float truncation, const float pose[16], float fx, float fy,
                                   float cx, float cy, vsg_stream_t stream);
 
+/* Depth image -> camera-space point map (no counterpart on the reference's
+ * path, which receives point maps from CustomDepthMapGenerator,
+ * CustomDepthMapGenerator.cpp:81-222): p = ((x - cx) d / fx, (y - cy) d / fy,
+ * d) per pixel, (0,0,0) where d is not a positive finite number; normals (may
+ * be NULL) as that generator's fallback computes them (:163-209): normalised
+ * cross product of the right and lower neighbours' offsets, interior pixels
+ * with d > 0, else (0,0,0).  depth: device float[w*h]; pointmap, normals:
+ * device float3[w*h].  Stream-ordered. */
+VSG_API int vsg_depth_to_pointmap(const float* depth, int w, int h, float fx, float fy, float cx, float cy,
+                                  float* pointmap, float* normals, vsg_stream_t stream);
+
 /* Counters of the scene and of its last frame / render.  Synchronises. */
 VSG_API int vsg_scene_stats(vsg_scene* s, vsg_stats* out);
 

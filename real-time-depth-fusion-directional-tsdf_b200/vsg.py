@@ -34,6 +34,7 @@ EXPORTS = [
     "vsg_points_create", "vsg_points_destroy", "vsg_extract_points", "vsg_points_count", "vsg_points_buffers",
     "vsg_points_download", "vsg_points_save_ply",
     "vsg_renderer_record", "vsg_render_backward", "vsg_render_normals", "vsg_scene_lookup_blocks",
+    "vsg_depth_to_pointmap",
 ]
 
 
@@ -135,6 +136,7 @@ def lib() -> ctypes.CDLL:
         L.vsg_points_download.argtypes = [_P, _P, _P, _P, ctypes.POINTER(ctypes.c_int64)]
         L.vsg_points_save_ply.argtypes = [_P, ctypes.c_char_p]
         L.vsg_renderer_record.argtypes = [_P, _I]
+        L.vsg_depth_to_pointmap.argtypes = [_P, _I, _I, _F, _F, _F, _F, _P, _P, _P]
         L.vsg_scene_lookup_blocks.argtypes = [_P, _P, ctypes.c_uint32, _P]
         L.vsg_render_backward.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, _P, _P, _P, _F,
                                           ctypes.POINTER(ctypes.c_uint32), _P]
@@ -175,6 +177,20 @@ def default_params(**kw) -> Params:
     for k, v in kw.items():
         setattr(p, k, v)
     return p
+
+
+def depth_to_pointmap(depth, fx, fy, cx, cy, normals: bool = True, stream=None):
+    """(H,W) float32 device depth tensor -> ((H,W,3) point map, (H,W,3)
+    normals or None) device tensors (vsg_depth_to_pointmap)."""
+    import torch
+
+    H, W = depth.shape
+    d = depth.contiguous().to(torch.float32)
+    pm = torch.empty((H, W, 3), dtype=torch.float32, device=d.device)
+    nm = torch.empty((H, W, 3), dtype=torch.float32, device=d.device) if normals else None
+    check("vsg_depth_to_pointmap", lib().vsg_depth_to_pointmap(_dptr(d), W, H, _F(fx), _F(fy), _F(cx), _F(cy),
+                                                               _dptr(pm), _dptr(nm), _stream(stream)))
+    return pm, nm
 
 
 class _DeviceArray:
