@@ -126,3 +126,37 @@ def test_render_empty_scene_leaves_outputs(cuda, synth_mod):
     second = rr.download()
     for k in first:
         assert np.array_equal(first[k].view(np.uint32), second[k].view(np.uint32)), k
+
+
+def test_room_1280x720_2mm(cuda, oracle_mod, synth_mod):
+    """The room workload: 1280x720 frames of a seeded 4x3x2.5 m room with 40
+    boxes and 20 spheres on a random walk, 2 mm voxels, truncation 0.01 m,
+    2^20 buckets and pool blocks.  Volumes bit-exact after every frame; the
+    ray cast compared on a band of rows at full width (the oracle's full
+    frame would take minutes)."""
+    import vsg
+
+    fr, K = synth_mod.room_stream(1, 3, 1280, 720)
+    voxel, trunc = 0.002, 0.01
+    sc = vsg.Scene(voxel_size=voxel, truncation=trunc, hash_num_slots=1 << 20, num_sdf_blocks=1 << 20)
+    rr = vsg.Renderer(K.width, K.height)
+    orc = oracle_mod.OracleScene(voxel)
+    for i, f in enumerate(fr):
+        pm, rgb, nm = _upload(cuda, f)
+        sc.integrate(pm, rgb, nm, K.width, K.height, trunc, f.pose, K.fx, K.fy, K.cx, K.cy)
+        ost = orc.integrate(f.pointmap, f.rgb, trunc, f.pose, K.fx, K.fy, K.cx, K.cy)
+        gc, gv = sc.export()
+        oc, ov = orc.export()
+        v = compare_volumes(gc, gv, oc, ov["raw"])
+        assert v["same_blocks"] and v["bit_exact"], (i, v)
+        st = sc.stats()
+        assert st["flags"] == 0 and st["frame_new_blocks"] == ost["new_blocks"]
+    f = fr[-1]
+    rr.render(sc, f.pose, K.fx, K.fy, K.cx, K.cy, 0.2, 4.0)
+    g = rr.download()
+    rows = (340, 372)
+    o = orc.render(K.width, K.height, f.pose, K.fx, K.fy, K.cx, K.cy, 0.2, 4.0, rows=rows)
+    band = {k: g[k][rows[0]:rows[1]] for k in ("depth", "position", "color", "normal")}
+    want = {k: o[k][rows[0]:rows[1]] for k in ("depth", "position", "color", "normal")}
+    r = compare_renders(band, want, DEPTH_TOL)
+    assert r["bit_exact_all"] and r["hits_gpu"] > 0.5 * r["pixels"], r
