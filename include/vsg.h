@@ -224,6 +224,22 @@ VSG_API int vsg_render_backward(const vsg_renderer* r, const vsg_scene* s, const
                                 float cx, float cy, const float* grad_depth, const float* grad_position,
                                 double* grad_pose, float* grad_sdf, float min_weight_sum, uint32_t* n_skipped,
                                 vsg_stream_t stream);
+/* Adjoint of one frame's integration (no reference counterpart): call right
+ * after the vsg_integrate of that frame, with the same point map, pose,
+ * intrinsics and truncation.  grad_sdf: device float[num_sdf_blocks * 512]
+ * holding dL/d(voxel SDF after the frame), pool-indexed; for every voxel the
+ * frame updated it is replaced IN PLACE by dL/d(SDF before the frame) (the
+ * others are unchanged).  grad_pose: DEVICE double[12] receiving dL/dT of the
+ * row-major 3x4 camera->world matrix (written); grad_pointmap: device
+ * float3[w*h] dL/dp, ACCUMULATED (NULL = skip).  Decisions (each voxel's
+ * pixel, sign, truncation test) are the forward's; a voxel found at the
+ * weight cap (255) is taken to have reached it with this frame.
+ * n_updated: if not NULL, synchronises and stores the voxels the frame
+ * updated. */
+VSG_API int vsg_integrate_backward(vsg_scene* s, const float* pointmap, int w, int h, float truncation,
+                                   const float pose[16], float fx, float fy, float cx, float cy, float* grad_sdf,
+                                   double* grad_pose, float* grad_pointmap, uint32_t* n_updated,
+                                   vsg_stream_t stream);
 /* Pool indices of the given blocks (host int32 coords[n*3] -> host int32
  * ptrs[n], -1 = not allocated): the row of grad_sdf, or of the voxel pool,
  * that holds each block.  Synchronises. */

@@ -34,7 +34,7 @@ EXPORTS = [
     "vsg_points_create", "vsg_points_destroy", "vsg_extract_points", "vsg_points_count", "vsg_points_buffers",
     "vsg_points_download", "vsg_points_save_ply",
     "vsg_renderer_record", "vsg_render_backward", "vsg_render_normals", "vsg_scene_lookup_blocks",
-    "vsg_depth_to_pointmap",
+    "vsg_depth_to_pointmap", "vsg_integrate_backward",
 ]
 
 
@@ -137,6 +137,8 @@ def lib() -> ctypes.CDLL:
         L.vsg_points_save_ply.argtypes = [_P, ctypes.c_char_p]
         L.vsg_renderer_record.argtypes = [_P, _I]
         L.vsg_depth_to_pointmap.argtypes = [_P, _I, _I, _F, _F, _F, _F, _P, _P, _P]
+        L.vsg_integrate_backward.argtypes = [_P, _P, _I, _I, _F, _P, _F, _F, _F, _F, _P, _P, _P,
+                                             ctypes.POINTER(ctypes.c_uint32), _P]
         L.vsg_scene_lookup_blocks.argtypes = [_P, _P, ctypes.c_uint32, _P]
         L.vsg_render_backward.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, _P, _P, _P, _F,
                                           ctypes.POINTER(ctypes.c_uint32), _P]
@@ -289,6 +291,22 @@ class Scene:
         check("vsg_scene_export", self.L.vsg_scene_export(
             self.h, _hptr(coords), _hptr(vox) if with_voxels else None, cnt, ctypes.byref(n)))
         return coords[:cnt], (vox[:cnt] if with_voxels else None)
+
+    def integrate_backward(self, pointmap, width, height, truncation, pose, fx, fy, cx, cy, grad_sdf,
+                           grad_pointmap=None, stream=None):
+        """Adjoint of the last vsg_integrate (same inputs): grad_sdf (device
+        float32, num_sdf_blocks*512, dL/d SDF after the frame) becomes dL/d SDF
+        before it for the updated voxels, in place; grad_pointmap (H,W,3) device
+        tensor is added to.  Returns (dL/dT (3,4) float64 numpy, voxels updated)."""
+        import torch
+
+        T = np.ascontiguousarray(np.asarray(pose, np.float32).reshape(16))
+        gp = torch.zeros(12, dtype=torch.float64, device="cuda")
+        n = ctypes.c_uint32()
+        check("vsg_integrate_backward", self.L.vsg_integrate_backward(
+            self.h, _dptr(pointmap), int(width), int(height), _F(truncation), _hptr(T), _F(fx), _F(fy), _F(cx),
+            _F(cy), _dptr(grad_sdf), _dptr(gp), _dptr(grad_pointmap), ctypes.byref(n), _stream(stream)))
+        return gp.cpu().numpy().reshape(3, 4), int(n.value)
 
     def lookup_blocks(self, coords) -> np.ndarray:
         """Pool index of each block coordinate (-1 = not allocated)."""
