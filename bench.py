@@ -220,9 +220,9 @@ def run_ours(args):
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        import shard
+
+        ms = shard.max_over_ranks(ms, dist)
     # per step: reset (3 kernels) + per frame: frame_begin, alloc, select, integrate, render_begin, render
     launches_per_step = 3 + len(dev) * 6
     # per-kernel times (separate pass with events around each launch)
@@ -281,7 +281,7 @@ def run_ours(args):
     if not args.no_e2e:
         line["e2e"] = e2e(args, frames, K, sc, rr)
     if not args.no_batched:
-        line["batched"] = run_batched(args)
+        line["batched"] = run_batched(args, dist)
     if not args.no_cpu and rank == 0:
         line["cpu_baseline"] = cpu_baseline(frames, K)
     if rank == 0:
@@ -438,19 +438,26 @@ def stream_measure(sc) -> dict:
             "in_gbs": n_in * nb / max(t2 - t1, 1e-9) / 1e9}
 
 
-def run_batched(args) -> dict:
+def run_batched(args, dist=None) -> dict:
     """Batched plain method: independent tabletop scans (own seeds; 160x120 /
     320x240 / 640x480; U[10,200] frames; 50000-400000 buckets) integrated and
     ray cast frame by frame.  Times the same frames one scan after the other
     through vsg_integrate + vsg_render ("plain per-scene") and all scans
     together through vsg_batch_step (graph-replayed steps, autotuned ray
-    cast).  Frames are generated on the GPU and resident before timing."""
+    cast).  Frames are generated on the GPU and resident before timing.
+    On N GPUs the scans are partitioned by frames x pixels (no exchange on
+    the data path); times are the maximum over ranks."""
     import torch
 
+    import shard
     import synth
     import vsg
 
-    scans = synth.batched_scans(args.batched_scans)
+    world = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
+    all_scans = synth.batched_scans(args.batched_scans)
+    work = [len(s["poses"]) * s["K"].width * s["K"].height for s in all_scans]
+    scans = [all_scans[i] for i in shard.partition(work, world)[rank]]
     scenes, rends, frames = [], [], []
     for i, sc in enumerate(scans):
         K = sc["K"]
@@ -492,24 +499,30 @@ def run_batched(args) -> dict:
         for s in scenes:
             s.reset()
         torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         fn()
         e1.record()
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) * 1e-3
+        return shard.max_over_ranks(e0.elapsed_time(e1) * 1e-3, dist)
 
     timed(batched_pass)  # first pass: eager steps, autotuning, graph captures
     t_batched = timed(batched_pass)
     timed(plain_pass)  # warm
     t_plain = timed(plain_pass)
     batch.close()
-    res = {"workload": f"{len(scans)} tabletop scans (160x120/320x240/640x480, U[10,200] frames), "
+    n_frames = int(shard.sum_over_ranks(n_frames, dist))
+    n_pix = shard.sum_over_ranks(n_pix, dist)
+    res = {"workload": f"{len(all_scans)} tabletop scans (160x120/320x240/640x480, U[10,200] frames), "
                        f"{n_frames} frames, voxel 4mm, trunc 0.02m",
            "frames": n_frames, "steps": steps,
            "frames_per_s": n_frames / t_batched, "mpix_per_s": n_pix / t_batched / 1e6,
            "plain_per_scene_frames_per_s": n_frames / t_plain,
-           "speedup_vs_plain": t_plain / t_batched}
+           "speedup_vs_plain": t_plain / t_batched,
+           "sharding": f"{world} rank(s), scans partitioned by frames x pixels, no data-path collective"}
     for s in scenes:
         s.close()
     for r in rends:
