@@ -35,6 +35,10 @@ def lib(nofma: bool = True):
         L.ref_export.restype = _I
         L.ref_export.argtypes = [_P, _P, _P, _I]
         L.ref_voxel_bytes.restype = _I
+        L.ref_integrate_dev.restype = _F
+        L.ref_integrate_dev.argtypes = [_P, _P, _P, _P, _I, _I, _F, _P, _P, _F, _F, _F, _F]
+        L.ref_render_dev.restype = _F
+        L.ref_render_dev.argtypes = [_P, _I, _I, _P, _P, _F, _F, _F, _F, _F, _F, _P, _P, _P, _P]
         _libs[nofma] = L
     return _libs[nofma]
 

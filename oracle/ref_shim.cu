@@ -151,4 +151,51 @@ int ref_export(void* h, int32_t* coords, uint8_t* vox8, int max_blocks) {
 
 int ref_voxel_bytes(void) { return (int)sizeof(VoxelData); }
 
+// Device-resident variants for timing the reference's launchers: inputs,
+// outputs and the pose already on the device; the returned value is the
+// device time (ms, CUDA events) of the launcher calls, host work inside them
+// (their own syncs and small allocations) included.
+float ref_integrate_dev(void* h, const float* pm, const uint8_t* rgb, const float* nm, int W, int H, float trunc,
+                        const float* T_host, float* T_dev, float fx, float fy, float cx, float cy) {
+    RefScene* s = static_cast<RefScene*>(h);
+    const float3 cam = make_float3(T_host[3], T_host[7], T_host[11]);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    allocBlocksFromDepthMapCUDA(s->hash, s->params, reinterpret_cast<const float3*>(pm),
+                                reinterpret_cast<const float3*>(nm), W, H, trunc, cam, T_dev);
+    compactifyHashCUDA(s->hash, s->params);
+    integrateDepthMapIntoBlocksCUDA(s->hash, s->params, reinterpret_cast<const float3*>(pm),
+                                    reinterpret_cast<const uchar3*>(rgb), reinterpret_cast<const float3*>(nm), W, H,
+                                    trunc, cam, T_dev, fx, fy, cx, cy);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = -1.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return cudaDeviceSynchronize() == cudaSuccess ? ms : -1.0f;
+}
+
+float ref_render_dev(void* h, int W, int H, const float* T_host, float* T_dev, float fx, float fy, float cx, float cy,
+                     float minD, float maxD, float* depth, float* pos, float* col, float* nrm) {
+    RefScene* s = static_cast<RefScene*>(h);
+    const float3 cam = make_float3(T_host[3], T_host[7], T_host[11]);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    rayCastRenderCUDA(s->hash, W, H, depth, reinterpret_cast<float4*>(pos), reinterpret_cast<float4*>(col),
+                      reinterpret_cast<float4*>(nrm), cam, T_dev, fx, fy, cx, cy, minD, maxD, s->params.voxelSize,
+                      s->params.hashSlotNum, s->params.slotSize, s->params.totalHashSize);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = -1.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return cudaDeviceSynchronize() == cudaSuccess ? ms : -1.0f;
+}
+
 }  // extern "C"
