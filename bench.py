@@ -350,9 +350,10 @@ def points_measure(sc, peak: float, reps: int = 10) -> dict:
 def adjoint_measure(sc, frames, K, reps: int = 10, n_poses: int = 16) -> dict:
     """Ray-cast adjoint at the last frame's pose of the final volume: device
     time of a recording render plus vsg_render_backward (dL/ddepth = 1 on
-    every hit pixel, pose and voxel-SDF gradients), and a 20-step Adam pose
-    refinement through the torch wrapper from a pose perturbed by ~1 cm /
-    1 degree (Huber depth loss against the render at the true pose)."""
+    every hit pixel, pose and voxel-SDF gradients), and an 8-step
+    Gauss-Newton pose refinement (vsg.refine_pose) from poses perturbed by
+    ~1 cm / 1 degree per axis (Huber depth residuals against the render at
+    the true pose)."""
     import torch
 
     import vsg
@@ -380,44 +381,43 @@ def adjoint_measure(sc, frames, K, reps: int = 10, n_poses: int = 16) -> dict:
         torch.cuda.synchronize()
         fwd += e[0].elapsed_time(e[1])
         bwd += e[1].elapsed_time(e[2])
+    # Gauss-Newton normal equations (residual 1 on every hit pixel)
+    ne = 0.0
+    for _ in range(reps):
+        e[0].record()
+        rr.pose_normal_equations(sc, T, K.fx, K.fy, K.cx, K.cy, gd)
+        e[1].record()
+        torch.cuda.synchronize()
+        ne += e[0].elapsed_time(e[1])
     # pose refinement: target poses are the stream's frames, each perturbed by
     # seeded SE(3) noise (translation N(0, 1 cm), rotation N(0, 1 deg) per
-    # axis); 20 Adam steps of a Huber depth loss against the render at the
-    # true pose
-    def se3(x):
-        w, t = x[:3], x[3:]
-        th = torch.sqrt((w * w).sum() + 1e-18)
-        z = torch.zeros((), dtype=x.dtype)
-        Wm = torch.stack([torch.stack([z, -w[2], w[1]]), torch.stack([w[2], z, -w[0]]),
-                          torch.stack([-w[1], w[0], z])])
-        R = torch.eye(3, dtype=x.dtype) + torch.sin(th) / th * Wm + (1 - torch.cos(th)) / th ** 2 * (Wm @ Wm)
-        return torch.cat([torch.cat([R, t[:, None]], 1), torch.eye(4, dtype=x.dtype)[3:]], 0)
-
+    # axis); 8 Gauss-Newton steps of Huber-weighted depth residuals against
+    # the render at the true pose (vsg.refine_pose)
     rng = np.random.default_rng(7)
     ratios = []
+    gn_steps = 8
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     n_steps = 0
     for k in range(n_poses):
-        T_true = torch.tensor(np.asarray(frames[(k * 7) % len(frames)].pose, np.float32), dtype=torch.float64)
-        target = vsg.render_depth(sc, rr, T_true.float(), K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D).detach()
+        T_true = np.asarray(frames[(k * 7) % len(frames)].pose, np.float32)
+        rr.render(sc, T_true, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
+        target = rr.depth_tensor().clone()
         d0 = np.concatenate([rng.normal(size=3) * np.deg2rad(1.0), rng.normal(size=3) * 0.01])
-        xi = torch.tensor(d0, dtype=torch.float64, requires_grad=True)
-        opt = torch.optim.Adam([xi], lr=5e-4)
-        for _ in range(20):
-            opt.zero_grad()
-            d = vsg.render_depth(sc, rr, (T_true @ se3(xi)).float(), K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
-            m = (d < 1e9) & (target < 1e9)
-            torch.nn.functional.huber_loss(d[m], target[m], delta=0.01).backward()
-            opt.step()
-            n_steps += 1
-        ratios.append(float(xi.detach().norm()) / float(np.linalg.norm(d0)))
+        T_fin, _ = vsg.refine_pose(sc, rr, target, T_true.astype(np.float64) @ vsg.se3_exp(d0), K.fx, K.fy,
+                                   K.cx, K.cy, MIN_D, MAX_D, steps=gn_steps)
+        n_steps += gn_steps
+        D = np.linalg.inv(T_true.astype(np.float64)) @ T_fin
+        ang = np.arccos(np.clip((np.trace(D[:3, :3]) - 1) / 2, -1, 1))
+        ratios.append(float(np.hypot(ang, np.linalg.norm(D[:3, 3])) /
+                            np.hypot(np.linalg.norm(d0[:3]), np.linalg.norm(d0[3:]))))
     torch.cuda.synchronize()
     step_ms = (time.perf_counter() - t0) * 1e3 / n_steps
     rr.close()
     return {"hit_pixels": hits, "render_record_ms": fwd / reps, "backward_ms": bwd / reps,
-            "skipped_pixels": skipped,
-            "refine": {"poses": n_poses, "steps_per_pose": 20, "ms_per_step_wall": step_ms,
+            "normal_equations_ms": ne / reps, "skipped_pixels": skipped,
+            "refine": {"method": "gauss-newton", "poses": n_poses, "steps_per_pose": gn_steps,
+                       "ms_per_step_wall": step_ms,
                        "median_final_over_initial_err": float(np.median(ratios)),
                        "frac_poses_improved": float(np.mean(np.array(ratios) < 1.0))}}
 

@@ -244,6 +244,20 @@ VSG_API int vsg_integrate_backward(vsg_scene* s, const float* pointmap, int w, i
  * ptrs[n], -1 = not allocated): the row of grad_sdf, or of the voxel pool,
  * that holds each block.  Synchronises. */
 VSG_API int vsg_scene_lookup_blocks(const vsg_scene* s, const int32_t* coords, uint32_t n, int32_t* ptrs);
+/* Gauss-Newton normal equations of a weighted depth least-squares pose
+ * problem on the last recorded render (no reference counterpart): with
+ * J_i = d depth_i / d xi for the pose perturbation T exp(xi), xi = (omega,
+ * v) (dR = R [omega]x, dt = R v), accumulates H = sum w_i J_i J_i^T and
+ * b = sum w_i J_i r_i over hit pixels in double.  residual: device
+ * float[w*h] (e.g. rendered minus observed depth); weights: device float[w*h]
+ * (robust weights; NULL = 1; 0 leaves a pixel out).  normal_eq: DEVICE
+ * double[27] receiving H's upper triangle row by row (21) then b (6); the
+ * step is xi = -H^-1 b.  min_weight_sum and n_skipped as for
+ * vsg_render_backward. */
+VSG_API int vsg_render_pose_normal_equations(const vsg_renderer* r, const vsg_scene* s, const float pose[16],
+                                             float fx, float fy, float cx, float cy, const float* residual,
+                                             const float* weights, float min_weight_sum, double* normal_eq,
+                                             uint32_t* n_skipped, vsg_stream_t stream);
 /* Normals of the last recorded render (the reference never writes its normal
  * output): the normalised trilinear SDF gradient at each hit point, pointing
  * towards increasing SDF like computeNormalFromSDF (RayCastRender.cu:629-677);

@@ -55,6 +55,8 @@ struct BackArgs {
     const float* g_depth;   // may be null
     const float4* g_pos;    // may be null
     float* g_sdf;           // may be null
+    const float* resid;     // normal equations: per-pixel residual
+    const float* wts;       // normal equations: per-pixel weight (null = 1)
     float4* normals;        // vsg_render_normals output (null in backward)
     double* partials;       // per CTA 12 doubles
     float min_w;            // leave out pixels whose samples renormalise over less weight
@@ -320,6 +322,115 @@ __device__ bool recompute(const SceneDev& s, const Ray& r, float a0, float b0, C
     return true;
 }
 
+// One hit pixel's reverse pass: dL/dT (12 entries, written to gT) for
+// dL/ddepth = gd and dL/dposition = gp.  false (and counted in a.skipped)
+// when the pixel is left out; gT is then untouched.
+__device__ bool pixel_grad(const BackArgs& a, int x, int y, size_t pi, float depth, float gd, float4 gp,
+                           double gT[12]) {
+    const Ray r = make_ray(a, x, y);
+    const float2 br = a.rec[pi];
+    Crossing c;
+    const float d2r = 1.0f / r.cdz;
+    if (!recompute(a.s, r, br.x, br.y, c) ||
+        __float_as_uint(c.alpha / d2r) != __float_as_uint(depth)) {
+        atomicAdd(a.skipped, 1u);
+        return false;
+    } else {
+        // the smooth function of the frozen decisions, in double
+        double cd[3] = {((double)x - a.cx) / a.fx, ((double)y - a.cy) / a.fy, 1.0};
+        {
+            const double cl = sqrt(cd[0] * cd[0] + cd[1] * cd[1] + cd[2] * cd[2]);
+            cd[0] /= cl;
+            cd[1] /= cl;
+            cd[2] /= cl;
+        }
+        const float* T = a.pose.T;
+        double u[3], wd[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            u[i] = (double)T[4 * i] * cd[0] + (double)T[4 * i + 1] * cd[1] + (double)T[4 * i + 2] * cd[2];
+        const double wl = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) wd[i] = u[i] / wl;
+        const double o[3] = {T[3], T[7], T[11]};
+        double P[4] = {0.0, 0.0, 0.0, 0.0}, F[4] = {0.0, 0.0, 0.0, 0.0}, G[4][3] = {};
+        P[0] = br.x;
+        P[1] = br.y;
+        bool ok = true;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k >= 2) {
+                const int s = k - 2;
+                ok = ok && F[c.ia[s]] != F[c.ib[s]];
+                P[k] = rf64(P[c.ia[s]], F[c.ia[s]], P[c.ib[s]], F[c.ib[s]]);
+            }
+            const double q[3] = {o[0] + P[k] * wd[0], o[1] + P[k] * wd[1], o[2] + P[k] * wd[2]};
+            double wsum = 0.0;
+            ok = ok && sample64(a.s, q, c.taps[k], F[k], G[k], nullptr, 0.0, &wsum);
+            ok = ok && wsum >= (double)a.min_w;
+        }
+        // a step whose two values coincide in exact arithmetic (e.g. both
+        // samples read truncation-clamped voxels only) has no derivative:
+        // the forward's step there was decided by rounding noise
+        ok = ok && F[c.ia[2]] != F[c.ib[2]];
+        const double alpha = ok ? rf64(P[c.ia[2]], F[c.ia[2]], P[c.ib[2]], F[c.ib[2]]) : 0.0;
+        ok = ok && isfinite(alpha);
+        if (!ok) {
+            atomicAdd(a.skipped, 1u);
+            return false;
+        }
+        // outputs: depth = alpha cd_z, position = o + alpha wd
+        double g_alpha = (double)gd * cd[2] + (double)gp.x * wd[0] + (double)gp.y * wd[1] +
+                         (double)gp.z * wd[2];
+        double go[3] = {gp.x, gp.y, gp.z};
+        double gw[3] = {alpha * gp.x, alpha * gp.y, alpha * gp.z};
+        double gP[4] = {0.0, 0.0, 0.0, 0.0}, gF[4] = {0.0, 0.0, 0.0, 0.0};
+        if (ok) {
+            rf_back(P[c.ia[2]], F[c.ia[2]], P[c.ib[2]], F[c.ib[2]], g_alpha, gP[c.ia[2]], gF[c.ia[2]],
+                    gP[c.ib[2]], gF[c.ib[2]]);
+            // nodes 3, 2 (regula-falsi points), then 1, 0 (bracket ends)
+#pragma unroll
+            for (int k = 3; k >= 0; --k) {
+                const double gf = gF[k];
+                if (gf != 0.0) {
+                    if (a.g_sdf) {
+                        const double q[3] = {o[0] + P[k] * wd[0], o[1] + P[k] * wd[1], o[2] + P[k] * wd[2]};
+                        double fdummy, gdummy[3];
+                        sample64(a.s, q, c.taps[k], fdummy, gdummy, a.g_sdf, gf);
+                    }
+                    go[0] += gf * G[k][0];
+                    go[1] += gf * G[k][1];
+                    go[2] += gf * G[k][2];
+                    gw[0] += gf * P[k] * G[k][0];
+                    gw[1] += gf * P[k] * G[k][1];
+                    gw[2] += gf * P[k] * G[k][2];
+                    gP[k] += gf * (G[k][0] * wd[0] + G[k][1] * wd[1] + G[k][2] * wd[2]);
+                }
+                if (k >= 2) {  // node k = RF of step k-1's bracket
+                    const int s = k - 2;
+                    rf_back(P[c.ia[s]], F[c.ia[s]], P[c.ib[s]], F[c.ib[s]], gP[k], gP[c.ia[s]], gF[c.ia[s]],
+                            gP[c.ib[s]], gF[c.ib[s]]);
+                }
+            }
+            // wd = u / |u|, u = R cd
+            double gu[3];
+            {
+                const double dot = gw[0] * wd[0] + gw[1] * wd[1] + gw[2] * wd[2];
+                gu[0] = (gw[0] - dot * wd[0]) / wl;
+                gu[1] = (gw[1] - dot * wd[1]) / wl;
+                gu[2] = (gw[2] - dot * wd[2]) / wl;
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+#pragma unroll
+                for (int j = 0; j < 3; ++j) gT[4 * i + j] = gu[i] * cd[j];
+                gT[4 * i + 3] = go[i];
+            }
+        }
+    }
+    return true;
+}
+
 __global__ void __launch_bounds__(128) k_render_backward(BackArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
@@ -332,105 +443,8 @@ __global__ void __launch_bounds__(128) k_render_backward(BackArgs a) {
         const float depth = a.depth[pi];
         const float gd = a.g_depth ? a.g_depth[pi] : 0.0f;
         const float4 gp = a.g_pos ? a.g_pos[pi] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (depth < 0.5f * kMinf && (gd != 0.0f || gp.x != 0.0f || gp.y != 0.0f || gp.z != 0.0f)) {
-            const Ray r = make_ray(a, x, y);
-            const float2 br = a.rec[pi];
-            Crossing c;
-            const float d2r = 1.0f / r.cdz;
-            if (!recompute(a.s, r, br.x, br.y, c) ||
-                __float_as_uint(c.alpha / d2r) != __float_as_uint(depth)) {
-                atomicAdd(a.skipped, 1u);
-            } else {
-                // the smooth function of the frozen decisions, in double
-                double cd[3] = {((double)x - a.cx) / a.fx, ((double)y - a.cy) / a.fy, 1.0};
-                {
-                    const double cl = sqrt(cd[0] * cd[0] + cd[1] * cd[1] + cd[2] * cd[2]);
-                    cd[0] /= cl;
-                    cd[1] /= cl;
-                    cd[2] /= cl;
-                }
-                const float* T = a.pose.T;
-                double u[3], wd[3];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-                    u[i] = (double)T[4 * i] * cd[0] + (double)T[4 * i + 1] * cd[1] + (double)T[4 * i + 2] * cd[2];
-                const double wl = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-#pragma unroll
-                for (int i = 0; i < 3; ++i) wd[i] = u[i] / wl;
-                const double o[3] = {T[3], T[7], T[11]};
-                double P[4] = {0.0, 0.0, 0.0, 0.0}, F[4] = {0.0, 0.0, 0.0, 0.0}, G[4][3] = {};
-                P[0] = br.x;
-                P[1] = br.y;
-                bool ok = true;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    if (k >= 2) {
-                        const int s = k - 2;
-                        ok = ok && F[c.ia[s]] != F[c.ib[s]];
-                        P[k] = rf64(P[c.ia[s]], F[c.ia[s]], P[c.ib[s]], F[c.ib[s]]);
-                    }
-                    const double q[3] = {o[0] + P[k] * wd[0], o[1] + P[k] * wd[1], o[2] + P[k] * wd[2]};
-                    double wsum = 0.0;
-                    ok = ok && sample64(a.s, q, c.taps[k], F[k], G[k], nullptr, 0.0, &wsum);
-                    ok = ok && wsum >= (double)a.min_w;
-                }
-                // a step whose two values coincide in exact arithmetic (e.g. both
-                // samples read truncation-clamped voxels only) has no derivative:
-                // the forward's step there was decided by rounding noise
-                ok = ok && F[c.ia[2]] != F[c.ib[2]];
-                const double alpha = ok ? rf64(P[c.ia[2]], F[c.ia[2]], P[c.ib[2]], F[c.ib[2]]) : 0.0;
-                ok = ok && isfinite(alpha);
-                if (!ok) atomicAdd(a.skipped, 1u);
-                // outputs: depth = alpha cd_z, position = o + alpha wd
-                double g_alpha = (double)gd * cd[2] + (double)gp.x * wd[0] + (double)gp.y * wd[1] +
-                                 (double)gp.z * wd[2];
-                double go[3] = {gp.x, gp.y, gp.z};
-                double gw[3] = {alpha * gp.x, alpha * gp.y, alpha * gp.z};
-                double gP[4] = {0.0, 0.0, 0.0, 0.0}, gF[4] = {0.0, 0.0, 0.0, 0.0};
-                if (ok) {
-                    rf_back(P[c.ia[2]], F[c.ia[2]], P[c.ib[2]], F[c.ib[2]], g_alpha, gP[c.ia[2]], gF[c.ia[2]],
-                            gP[c.ib[2]], gF[c.ib[2]]);
-                    // nodes 3, 2 (regula-falsi points), then 1, 0 (bracket ends)
-#pragma unroll
-                    for (int k = 3; k >= 0; --k) {
-                        const double gf = gF[k];
-                        if (gf != 0.0) {
-                            if (a.g_sdf) {
-                                const double q[3] = {o[0] + P[k] * wd[0], o[1] + P[k] * wd[1], o[2] + P[k] * wd[2]};
-                                double fdummy, gdummy[3];
-                                sample64(a.s, q, c.taps[k], fdummy, gdummy, a.g_sdf, gf);
-                            }
-                            go[0] += gf * G[k][0];
-                            go[1] += gf * G[k][1];
-                            go[2] += gf * G[k][2];
-                            gw[0] += gf * P[k] * G[k][0];
-                            gw[1] += gf * P[k] * G[k][1];
-                            gw[2] += gf * P[k] * G[k][2];
-                            gP[k] += gf * (G[k][0] * wd[0] + G[k][1] * wd[1] + G[k][2] * wd[2]);
-                        }
-                        if (k >= 2) {  // node k = RF of step k-1's bracket
-                            const int s = k - 2;
-                            rf_back(P[c.ia[s]], F[c.ia[s]], P[c.ib[s]], F[c.ib[s]], gP[k], gP[c.ia[s]], gF[c.ia[s]],
-                                    gP[c.ib[s]], gF[c.ib[s]]);
-                        }
-                    }
-                    // wd = u / |u|, u = R cd
-                    double gu[3];
-                    {
-                        const double dot = gw[0] * wd[0] + gw[1] * wd[1] + gw[2] * wd[2];
-                        gu[0] = (gw[0] - dot * wd[0]) / wl;
-                        gu[1] = (gw[1] - dot * wd[1]) / wl;
-                        gu[2] = (gw[2] - dot * wd[2]) / wl;
-                    }
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-#pragma unroll
-                        for (int j = 0; j < 3; ++j) gT[4 * i + j] = gu[i] * cd[j];
-                        gT[4 * i + 3] = go[i];
-                    }
-                }
-            }
-        }
+        if (depth < 0.5f * kMinf && (gd != 0.0f || gp.x != 0.0f || gp.y != 0.0f || gp.z != 0.0f))
+            pixel_grad(a, x, y, pi, depth, gd, gp, gT);
     }
     // deterministic reduction: warp shuffles, then the CTA's four warps
     __shared__ double red[4][12];
@@ -446,6 +460,92 @@ __global__ void __launch_bounds__(128) k_render_backward(BackArgs a) {
         const int i = threadIdx.x;
         a.partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 12 + i] =
             ((red[0][i] + red[1][i]) + red[2][i]) + red[3][i];
+    }
+}
+
+// Gauss-Newton normal equations of a weighted depth least-squares problem in
+// the pose's right-perturbation coordinates xi = (omega, v): T exp(xi),
+// dR = R [omega]x, dt = R v.  Per hit pixel the reverse pass with dL/ddepth
+// = 1 gives the depth's Jacobian J_T (12); J_xi follows by the chain rule,
+// and the pixel adds w J J^T and w J r.  Output per CTA: H's upper triangle
+// (21, row-major) then b (6), in double.
+constexpr int kNeVals = 27;
+
+__global__ void __launch_bounds__(128) k_pose_normal_equations(BackArgs a) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
+    const int y = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
+    double acc[kNeVals];
+#pragma unroll
+    for (int i = 0; i < kNeVals; ++i) acc[i] = 0.0;
+    if (x < a.W && y < a.H) {
+        const size_t pi = (size_t)y * a.W + x;
+        const float depth = a.depth[pi];
+        const float w = a.wts ? a.wts[pi] : 1.0f;
+        const float res = a.resid[pi];
+        double gT[12];
+        if (depth < 0.5f * kMinf && w != 0.0f && isfinite(res) &&
+            pixel_grad(a, x, y, pi, depth, 1.0f, make_float4(0.0f, 0.0f, 0.0f, 0.0f), gT)) {
+            const float* T = a.pose.T;
+            double J[6];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                // d depth / d omega_k = sum_ij J_T[i][j] (R (e_k x e_j))_i
+                double sum = 0.0;
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    double c[3] = {0.0, 0.0, 0.0};  // e_k x e_j
+                    const int m = 3 - k - j;        // the remaining axis when k != j
+                    if (k != j) c[m] = ((j - k + 3) % 3 == 1) ? 1.0 : -1.0;
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        const double Rc = (double)T[4 * i] * c[0] + (double)T[4 * i + 1] * c[1] +
+                                          (double)T[4 * i + 2] * c[2];
+                        sum += gT[4 * i + j] * Rc;
+                    }
+                }
+                J[k] = sum;
+                // d depth / d v_k = sum_i J_t[i] R[i][k]
+                J[3 + k] = gT[3] * (double)T[k] + gT[7] * (double)T[4 + k] + gT[11] * (double)T[8 + k];
+            }
+            int n = 0;
+#pragma unroll
+            for (int p = 0; p < 6; ++p)
+#pragma unroll
+                for (int q = p; q < 6; ++q) acc[n++] += (double)w * J[p] * J[q];
+#pragma unroll
+            for (int p = 0; p < 6; ++p) acc[21 + p] += (double)w * J[p] * (double)res;
+        }
+    }
+    __shared__ double red[4][kNeVals];
+#pragma unroll
+    for (int i = 0; i < kNeVals; ++i) {
+        double v = acc[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        if (lane == 0) red[warp][i] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kNeVals) {
+        const int i = threadIdx.x;
+        a.partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * kNeVals + i] =
+            ((red[0][i] + red[1][i]) + red[2][i]) + red[3][i];
+    }
+}
+
+// Sum nv values (nv <= 32) over n partial records in a fixed order.
+__global__ void k_reduce_records(const double* partials, int n, int nv, double* out) {
+    __shared__ double red[32][33];
+    const int i = threadIdx.x / 32, lane = threadIdx.x % 32;
+    double s = 0.0;
+    if (i < nv)
+        for (int k = lane; k < n; k += 32) s += partials[(size_t)k * nv + i];
+    red[i][lane] = s;
+    __syncthreads();
+    if (lane == 0 && i < nv) {
+        double t = 0.0;
+        for (int k = 0; k < 32; ++k) t += red[i][k];
+        out[i] = t;
     }
 }
 
@@ -536,7 +636,7 @@ int vsg_renderer_record(vsg_renderer* rh, int enable) {
         const size_t n = (size_t)r.w * r.h;
         const size_t ctas = (size_t)((r.w + 15) / 16) * ((r.h + 7) / 8);
         if (cudaMalloc(&r.bracket, n * sizeof(float2)) != cudaSuccess ||
-            cudaMalloc(&r.partials, ctas * 12 * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&r.partials, ctas * vsg::kNeVals * sizeof(double)) != cudaSuccess ||
             cudaMalloc(&r.skipped, sizeof(unsigned int)) != cudaSuccess) {
             cudaFree(r.bracket);
             cudaFree(r.partials);
@@ -589,6 +689,27 @@ int vsg_scene_lookup_blocks(const vsg_scene* s, const int32_t* coords, uint32_t 
     }
     cudaFree(d);
     return rc;
+}
+
+int vsg_render_pose_normal_equations(const vsg_renderer* rh, const vsg_scene* s, const float pose[16], float fx,
+                                     float fy, float cx, float cy, const float* residual, const float* weights,
+                                     float min_weight_sum, double* normal_eq, uint32_t* n_skipped,
+                                     vsg_stream_t stream) {
+    if (!rh || !s || !pose || !residual || !normal_eq || !(min_weight_sum >= 0.0f)) return VSG_ERR_INVALID_ARG;
+    const vsg::Renderer& r = rh->impl;
+    vsg::BackArgs a;
+    const int rc = vsg::prepare(r, s->impl, pose, fx, fy, cx, cy, a);
+    if (rc != VSG_OK) return rc;
+    a.resid = residual;
+    a.wts = weights;
+    a.min_w = min_weight_sum;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(r.skipped, 0, sizeof(unsigned int), st) != cudaSuccess) return VSG_ERR_CUDA;
+    const dim3 grid((r.w + 15) / 16, (r.h + 7) / 8);
+    vsg::k_pose_normal_equations<<<grid, 128, 0, st>>>(a);
+    vsg::k_reduce_records<<<1, 32 * 32, 0, st>>>(r.partials, (int)(grid.x * grid.y), vsg::kNeVals, normal_eq);
+    if (cudaGetLastError() != cudaSuccess) return VSG_ERR_CUDA;
+    return vsg::read_skipped(r, n_skipped, st);
 }
 
 int vsg_render_normals(const vsg_renderer* rh, const vsg_scene* s, const float pose[16], float fx, float fy,

@@ -34,7 +34,7 @@ EXPORTS = [
     "vsg_points_create", "vsg_points_destroy", "vsg_extract_points", "vsg_points_count", "vsg_points_buffers",
     "vsg_points_download", "vsg_points_save_ply",
     "vsg_renderer_record", "vsg_render_backward", "vsg_render_normals", "vsg_scene_lookup_blocks",
-    "vsg_depth_to_pointmap", "vsg_integrate_backward",
+    "vsg_depth_to_pointmap", "vsg_integrate_backward", "vsg_render_pose_normal_equations",
 ]
 
 
@@ -142,6 +142,8 @@ def lib() -> ctypes.CDLL:
         L.vsg_scene_lookup_blocks.argtypes = [_P, _P, ctypes.c_uint32, _P]
         L.vsg_render_backward.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, _P, _P, _P, _F,
                                           ctypes.POINTER(ctypes.c_uint32), _P]
+        L.vsg_render_pose_normal_equations.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, _P, _F, _P,
+                                                       ctypes.POINTER(ctypes.c_uint32), _P]
         L.vsg_render_normals.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, ctypes.POINTER(ctypes.c_uint32), _P]
         _lib = L
     return _lib
@@ -232,6 +234,56 @@ def render_depth(scene, renderer, pose, fx, fy, cx, cy, min_depth, max_depth, mi
             return out.to(device=ctx.dev, dtype=ctx.dtype)
 
     return _Render.apply(pose)
+
+
+def se3_exp(xi) -> np.ndarray:
+    """exp of a twist xi = (omega, v) as a 4x4 float64 matrix (Rodrigues'
+    formula for R, V v with V = I + (1 - cos th)/th^2 W + (th - sin th)/th^3
+    W^2 for t; the series below th = 1e-8)."""
+    xi = np.asarray(xi, np.float64)
+    w, v = xi[:3], xi[3:]
+    th = float(np.linalg.norm(w))
+    W = np.array([[0.0, -w[2], w[1]], [w[2], 0.0, -w[0]], [-w[1], w[0], 0.0]])
+    if th < 1e-8:
+        A, B, C = 1.0, 0.5, 1.0 / 6.0
+    else:
+        A, B, C = np.sin(th) / th, (1 - np.cos(th)) / th ** 2, (th - np.sin(th)) / th ** 3
+    out = np.eye(4)
+    out[:3, :3] = np.eye(3) + A * W + B * (W @ W)
+    out[:3, 3] = (np.eye(3) + B * W + C * (W @ W)) @ v
+    return out
+
+
+def refine_pose(scene, renderer, target_depth, pose, fx, fy, cx, cy, min_depth, max_depth, steps: int = 8,
+                huber: float = 0.01, damping: float = 1e-6, min_weight_sum: float = 0.5):
+    """Gauss-Newton alignment of a camera pose to a target depth image (H,W
+    device float32, misses >= 1e9) through the ray cast: each step renders at
+    the current pose, forms residuals (rendered - target) on pixels hit in
+    both with Huber weights (1 inside `huber` metres, huber/|r| outside),
+    solves (H + damping diag(H)) xi = -b from
+    vsg_render_pose_normal_equations and right-multiplies the pose by
+    exp(xi).  Returns (4x4 float64 pose, per-step weighted RMS residual)."""
+    import torch
+
+    T = np.asarray(pose, np.float64).reshape(4, 4).copy()
+    renderer.record(True)
+    rms = []
+    for _ in range(steps):
+        T32 = T.astype(np.float32)
+        renderer.render(scene, T32, fx, fy, cx, cy, min_depth, max_depth)
+        d = renderer.depth_tensor()
+        m = (d < 1e9) & (target_depth < 1e9)
+        r = torch.where(m, d - target_depth, torch.zeros_like(d))
+        a = r.abs()
+        w = torch.where(m, torch.where(a <= huber, torch.ones_like(a), huber / a.clamp_min(huber)),
+                        torch.zeros_like(a))
+        Hm, b, _ = renderer.pose_normal_equations(scene, T32, fx, fy, cx, cy, r, w, min_weight_sum)
+        rms.append(float(torch.sqrt((w * r * r).sum() / w.sum().clamp_min(1e-30))))
+        A = Hm + damping * np.diag(np.diag(Hm))
+        if not np.all(np.isfinite(A)) or np.linalg.matrix_rank(A) < 6:
+            break
+        T = T @ se3_exp(-np.linalg.solve(A, b))
+    return T, rms
 
 
 class Scene:
@@ -404,6 +456,28 @@ class Renderer:
             self.h, scene.h, _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _dptr(grad_depth), _dptr(grad_position),
             _dptr(gp), _dptr(grad_sdf), _F(min_weight_sum), ctypes.byref(skipped), _stream(stream)))
         return gp.cpu().numpy().reshape(3, 4), int(skipped.value)
+
+    def pose_normal_equations(self, scene: "Scene", pose, fx, fy, cx, cy, residual, weights=None,
+                              min_weight_sum: float = 0.5, stream=None):
+        """Gauss-Newton system of the last recorded render for per-pixel
+        residuals (H,W) and optional weights (device float32 tensors):
+        returns (H (6,6), b (6,)) float64 numpy in the right-perturbation
+        coordinates (omega, v) of T exp(xi), and the skipped-pixel count."""
+        import torch
+
+        T = np.ascontiguousarray(np.asarray(pose, np.float32).reshape(16))
+        ne = torch.zeros(27, dtype=torch.float64, device="cuda")
+        skipped = ctypes.c_uint32()
+        check("vsg_render_pose_normal_equations", self.L.vsg_render_pose_normal_equations(
+            self.h, scene.h, _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _dptr(residual.contiguous()),
+            _dptr(weights.contiguous() if weights is not None else None), _F(min_weight_sum), _dptr(ne),
+            ctypes.byref(skipped), _stream(stream)))
+        v = ne.cpu().numpy()
+        Hm = np.zeros((6, 6))
+        iu = np.triu_indices(6)
+        Hm[iu] = v[:21]
+        Hm = Hm + np.triu(Hm, 1).T
+        return Hm, v[21:], int(skipped.value)
 
     def normals(self, scene: "Scene", pose, fx, fy, cx, cy, out=None, stream=None):
         """Normals of the last recorded render: (H,W,4) float32 device tensor."""
