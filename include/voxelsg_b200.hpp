@@ -11,7 +11,7 @@
  *                         integrateFromScanData, getNumIntegratedFrames,
  *                         isAllocated, getParams, getHeapFreeCount
  *   RayCastRender        (RayCastRender.h:20-124): initialize, render,
- *                         downloadResults, downloadDepthFloat,
+ *                         downloadResults, downloadDepthFloat, savePointCloudPLY,
  *                         getOutputDepth/Color/Normal/Positions,
  *                         extractSurfacePoints, saveExtractedSurfacePointsPLY
  *   MarchingCubesParams, MarchingCubesOutput, allocateMarchingCubesOutput,
@@ -169,6 +169,10 @@ public:
             std::cerr << "VoxelScene: allocation failed (status " << rc << ")" << std::endl;
             m_scene = nullptr;
         }
+#ifdef USE_NORMAL_DIR_ALLOC
+        // the reference's compile-time switch (VoxelScene.cu:8, 1688)
+        if (m_scene) vsg_scene_set_alloc_method(m_scene, 2);
+#endif
     }
     ~VoxelScene() {
         if (m_scene) vsg_scene_destroy(m_scene);
@@ -299,6 +303,20 @@ public:
     void downloadDepthFloat(float* h_outputDepthFloat) {
         if (!m_r || h_outputDepthFloat == nullptr) return;
         vsg_renderer_download(m_r, h_outputDepthFloat, nullptr, nullptr, nullptr);
+    }
+
+    bool savePointCloudPLY(const std::string& filePath) {
+        if (!m_r) {
+            std::cerr << "RayCastRender: Not initialized!" << std::endl;
+            return false;
+        }
+        int64_t n = 0;
+        if (vsg_renderer_save_ply(m_r, filePath.c_str(), &n) != VSG_OK) {
+            std::cerr << "RayCastRender: No valid raycast points to export." << std::endl;
+            return false;
+        }
+        std::cout << "RayCastRender: Saved point cloud to " << filePath << " (" << n << " points)" << std::endl;
+        return true;
     }
 
     /* the depth buffer holds floats although typed float4*, as in the

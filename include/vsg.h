@@ -68,7 +68,10 @@ enum {
     VSG_FLAG_CHAIN_EXHAUSTED = 2u,  /* bucket overflow chain pool ran out */
     VSG_FLAG_COORD_RANGE = 4u,      /* a block coordinate outside +-2^20 was skipped */
     VSG_FLAG_INSERT_RETRY = 8u,     /* a bounded insert retry loop gave up */
-    VSG_FLAG_MARCH_LIMIT = 16u      /* a ray hit the iteration guard */
+    VSG_FLAG_MARCH_LIMIT = 16u,     /* a ray hit the iteration guard */
+    VSG_FLAG_PARENT_OVERFLOW = 32u  /* normal-direction allocation: a frame's parent records
+                                       overflowed (a DDA ran to its 1024-block guard); some
+                                       blocks kept an older parent pixel */
 };
 
 /* GlobalParamsConfig knobs (globalPramasConfig.h:101-109) and the sizes
@@ -122,8 +125,9 @@ VSG_API int vsg_scene_params(const vsg_scene* s, vsg_params* out);
  * band, select the blocks the frame can touch, update their voxels.
  * pointmap: device float3[w*h] camera-space points ((0,0,0) = invalid);
  * rgb: device uchar3[w*h]; normals: device float3[w*h] (must be non-null,
- * as in the reference, but is not read); pose: HOST float[16] row-major
- * camera->world.  Stream-ordered; does not synchronise. */
+ * as in the reference; read only by the normal-direction allocation);
+ * pose: HOST float[16] row-major camera->world.  Stream-ordered; does not
+ * synchronise. */
 VSG_API int vsg_integrate(vsg_scene* s, const float* pointmap, const uint8_t* rgb, const float* normals, int w,
                   int h, float truncation, const float pose[16], float fx, float fy, float cx, float cy,
                   vsg_stream_t stream);
@@ -143,11 +147,34 @@ VSG_API int vsg_integrate(vsg_scene* s, const float* pointmap, const uint8_t* rg
  *     (cudaGetSymbolAddress) and should come before any stream capture;
  *   - every call on a device shares the one array, so calls whose work
  *     overlaps on the GPU (other streams, other scenes) race; serialise them;
- *   - the scene must live on the current device (else VSG_ERR_INVALID_ARG).
+ *   - the scene must live on the current device (else VSG_ERR_INVALID_ARG);
+ *   - scenes set to the normal-direction allocation (method 2) are refused
+ *     with VSG_ERR_INVALID_ARG: that allocation keeps per-frame records in
+ *     buffers of the scene's own.
  * The scene itself is created beforehand with vsg_scene_create. */
 VSG_API int vsg_integrate_noalloc(vsg_scene* s, const float* pointmap, const uint8_t* rgb, const float* normals,
                                   int w, int h, float truncation, const float pose[16], float fx, float fy,
                                   float cx, float cy, vsg_stream_t stream);
+
+/* Allocation mode of vsg_integrate (allocBlocksFromDepthMapCUDA,
+ * VoxelScene.cu:1676-1721, chooses at compile time with
+ * USE_NORMAL_DIR_ALLOC):
+ *   1  (default) Method 1, VoxelScene.cu:487-633: per pixel the blocks of
+ *      the camera-space segment p.z -+ truncation;
+ *   2  Method 2, VoxelScene.cu:768-912: per pixel with a normal of length
+ *      >= 0.1, the blocks of the camera ray from the point to truncation
+ *      behind it and of the normal ray from the point to truncation inside
+ *      the surface.  A block on a normal ray records the pixel as its
+ *      parent (the last such pixel of the last such frame; of one frame's
+ *      rays the last in row-major order); integration then updates every
+ *      voxel of that block from the parent pixel's point instead of the
+ *      voxel's own projection whenever that pixel lies inside the frame and
+ *      holds a point (VoxelScene.cu:1015-1035).  Images up to 65535 pixels
+ *      on a side (VSG_ERR_TOO_LARGE beyond); not available to
+ *      vsg_integrate_noalloc or vsg_batch_step (VSG_ERR_INVALID_ARG).
+ * Parents persist until the scene is reset or the block is freed, and are
+ * honoured in either mode.  Takes effect at the next vsg_integrate. */
+VSG_API int vsg_scene_set_alloc_method(vsg_scene* s, int method);
 
 /* Depth image -> camera-space point map (no counterpart on the reference's
  * path, which receives point maps from CustomDepthMapGenerator,
@@ -192,6 +219,14 @@ VSG_API int vsg_renderer_outputs(const vsg_renderer* r, float** depth, float** p
 /* Copy the outputs to host memory (any pointer may be NULL); synchronous. */
 VSG_API int vsg_renderer_download(const vsg_renderer* r, float* depth, float* position, float* color,
                           float* normal);
+/* RayCastRender::savePointCloudPLY (RayCastRender.cpp:221-302): ASCII PLY
+ * of the last render's hit positions (depth finite, > 0 and < 1e9; position
+ * finite) with colour channels clamped to [0, 1] and rounded to 0..255
+ * (non-finite -> 255); parent directories are created.  No file and
+ * VSG_ERR_INVALID_ARG when no pixel is valid or the file cannot be
+ * written.  *n_points (may be NULL) receives the number written.
+ * Synchronous. */
+VSG_API int vsg_renderer_save_ply(const vsg_renderer* r, const char* path, int64_t* n_points);
 
 /* ---- adjoint of the ray cast (no counterpart in the reference) ----------
  * A hit pixel's depth and position are smooth functions of the camera pose

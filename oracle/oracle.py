@@ -52,6 +52,9 @@ def lib():
         L.orc_alloc.argtypes = [_p, _p, _i, _i, _f, _p, _p]
         L.orc_integrate_blocks.argtypes = [_p, _p, _p, _i, _i, _f, _p, _p, _f, _f, _f, _f, _p]
         L.orc_integrate.argtypes = [_p, _p, _p, _i, _i, _f, _p, _f, _f, _f, _f, _p]
+        L.orc_integrate_nm.argtypes = [_p, _p, _p, _p, _i, _i, _f, _p, _f, _f, _f, _f, _p]
+        L.orc_set_alloc_method.argtypes = [_p, _i]
+        L.orc_export_parents.argtypes = [_p, _p]
         L.orc_render.argtypes = [_p, _i, _i, _p, _p, _f, _f, _f, _f, _f, _f, _p, _p, _p, _p, _p]
         L.orc_render_rows.argtypes = [_p, _i, _i, _i, _i, _p, _p, _f, _f, _f, _f, _f, _f, _p, _p, _p,
                                       _p, _p]
@@ -104,14 +107,20 @@ class OracleScene:
     def num_blocks(self) -> int:
         return int(self.L.orc_num_blocks(self.h))
 
-    def integrate(self, pointmap, rgb, trunc, pose, fx, fy, cx, cy) -> dict:
+    def set_alloc_method(self, method: int):
+        """1: camera-z band (allocBlocksFromDepthMapMethod1Kernel); 2: camera
+        and normal rays with parent pixels (Method2, VoxelScene.cu:768-912)."""
+        self.L.orc_set_alloc_method(self.h, int(method))
+
+    def integrate(self, pointmap, rgb, trunc, pose, fx, fy, cx, cy, normals=None) -> dict:
         pm = _f32(pointmap)
         cm = np.ascontiguousarray(rgb, dtype=np.uint8)
+        nm = _f32(normals) if normals is not None else None
         T = _f32(pose).reshape(16)
         H, W = pm.shape[:2]
         out = np.zeros(4, np.int64)
-        self.L.orc_integrate(self.h, _ptr(pm), _ptr(cm), W, H, _f(trunc), _ptr(T), _f(fx), _f(fy),
-                             _f(cx), _f(cy), _ptr(out))
+        self.L.orc_integrate_nm(self.h, _ptr(pm), _ptr(cm), _ptr(nm) if nm is not None else None, W, H,
+                                _f(trunc), _ptr(T), _f(fx), _f(fy), _f(cx), _f(cy), _ptr(out))
         return {"new_blocks": int(out[0]), "updated_blocks": int(out[1]), "updated_voxels": int(out[2]),
                 "blocks": int(out[3])}
 
@@ -203,6 +212,13 @@ class OracleScene:
         vox = np.zeros((n, 512 * 8), np.uint8) if with_voxels else None
         self.L.orc_export(self.h, _ptr(coords), _ptr(vox) if with_voxels else None)
         return coords, (split_voxels(vox) if with_voxels else None)
+
+    def export_parents(self):
+        """Per block in export() order: the parent tag of the normal-direction
+        allocation, (frame + 1) << 32 | y << 16 | x, 0 = none."""
+        out = np.zeros(self.num_blocks, np.uint64)
+        self.L.orc_export_parents(self.h, _ptr(out))
+        return out
 
     def load(self, coords, voxel_bytes):
         coords = np.ascontiguousarray(coords, dtype=np.int32)

@@ -55,6 +55,12 @@ typedef struct {
     int64_t n, cap;
     uint64_t* keys;
     ovox* vox;
+    /* normal-direction allocation (VoxelScene.cu:768-912): per block the
+     * parent pixel of the last normal ray through it, (frame + 1) << 32 |
+     * y << 16 | x, 0 = none */
+    uint64_t* parent;
+    uint32_t frames; /* frames integrated since reset */
+    int alloc_method; /* 1 (camera-z band) or 2 (camera + normal rays) */
     int64_t coord_range_drops;
 } orc_scene;
 
@@ -151,10 +157,12 @@ static int scene_add(orc_scene* s, uint64_t key) {
         int64_t nc = s->cap ? s->cap * 2 : 1024;
         s->keys = (uint64_t*)realloc(s->keys, sizeof(uint64_t) * nc);
         s->vox = (ovox*)realloc(s->vox, sizeof(ovox) * VPB * nc);
+        s->parent = (uint64_t*)realloc(s->parent, sizeof(uint64_t) * nc);
         s->cap = nc;
     }
     map_grow(s, s->n + 1);
     s->keys[s->n] = key;
+    s->parent[s->n] = 0;
     memset(s->vox + s->n * VPB, 0, sizeof(ovox) * VPB);
     map_put_raw(s->mkeys, s->mvals, s->mcap, key, (int32_t)s->n);
     s->n++;
@@ -164,6 +172,7 @@ static int scene_add(orc_scene* s, uint64_t key) {
 orc_scene* orc_create(float voxel) {
     orc_scene* s = (orc_scene*)calloc(1, sizeof(orc_scene));
     s->voxel = voxel;
+    s->alloc_method = 1;
     return s;
 }
 
@@ -172,7 +181,10 @@ void orc_reset(orc_scene* s) {
     if (s->mkeys)
         for (int64_t i = 0; i < s->mcap; i++) s->mkeys[i] = KEY_EMPTY;
     s->coord_range_drops = 0;
+    s->frames = 0;
 }
+
+void orc_set_alloc_method(orc_scene* s, int method) { s->alloc_method = method; }
 
 void orc_destroy(orc_scene* s) {
     if (!s) return;
@@ -180,6 +192,7 @@ void orc_destroy(orc_scene* s) {
     free(s->mvals);
     free(s->keys);
     free(s->vox);
+    free(s->parent);
     free(s);
 }
 
@@ -327,13 +340,121 @@ int64_t orc_alloc(orc_scene* s, const float* pm, int W, int H, float trunc, cons
     return added;
 }
 
+/* allocBlocksFromDepthMapMethod2Kernel, VoxelScene.cu:797-911, per pixel:
+ * the blocks of the camera ray from the point to truncation behind it
+ * (out0) and of the normal ray from the point to truncation inside the
+ * surface (out1). */
+static void pixel_alloc_blocks_m2(const float* p, const float* nc, float trunc, const float* T, const float* cam,
+                                  float v, int32_t* out0, int* n0, int32_t* out1, int* n1) {
+    *n0 = *n1 = 0;
+    if (p[0] == 0.0f && p[1] == 0.0f && p[2] == 0.0f) return; /* :802 */
+    float nl = sqrtf(nc[0] * nc[0] + nc[1] * nc[1] + nc[2] * nc[2]);
+    if (nl < 0.1f) return; /* :806 */
+    const float n[3] = {nc[0] / nl, nc[1] / nl, nc[2] / nl};
+    float w[3];
+    xform_point(T, p, w);
+    float nw[3] = {T[0] * n[0] + T[1] * n[1] + T[2] * n[2], T[4] * n[0] + T[5] * n[1] + T[6] * n[2],
+                   T[8] * n[0] + T[9] * n[1] + T[10] * n[2]}; /* :822-827 */
+    nl = sqrtf(nw[0] * nw[0] + nw[1] * nw[1] + nw[2] * nw[2]);
+    if (nl > 1e-6f) {
+        nw[0] /= nl;
+        nw[1] /= nl;
+        nw[2] /= nl;
+    }
+    float rd[3] = {w[0] - cam[0], w[1] - cam[1], w[2] - cam[2]}; /* :840-858 */
+    const float rl = sqrtf(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2]);
+    if (rl > 0.0f) {
+        rd[0] /= rl;
+        rd[1] /= rl;
+        rd[2] /= rl;
+        const float e[3] = {w[0] + rd[0] * trunc, w[1] + rd[1] * trunc, w[2] + rd[2] * trunc};
+        *n0 = orc_dda_blocks(w, e, v, out0);
+    }
+    const float e1[3] = {w[0] - nw[0] * trunc, w[1] - nw[1] * trunc, w[2] - nw[2] * trunc}; /* :884-889 */
+    *n1 = orc_dda_blocks(w, e1, v, out1);
+}
+
+/* Normal-direction allocation of every block either ray visits ("ideal"
+ * allocation); each block on a normal ray takes the pixel as parent, the
+ * last in row-major order when several rays of the frame cross it.
+ * Returns the number of newly allocated blocks. */
+int64_t orc_alloc_m2(orc_scene* s, const float* pm, const float* nm, int W, int H, float trunc, const float* T,
+                     const float* cam) {
+    int64_t npx = (int64_t)W * H;
+    int nthr = 1;
+#ifdef _OPENMP
+    nthr = omp_get_max_threads();
+#endif
+    uint64_t** lists = (uint64_t**)calloc(nthr, sizeof(uint64_t*));
+    uint32_t** tags = (uint32_t**)calloc(nthr, sizeof(uint32_t*));
+    int64_t* lens = (int64_t*)calloc(nthr, sizeof(int64_t));
+    int64_t* caps = (int64_t*)calloc(nthr, sizeof(int64_t));
+    int64_t drops = 0;
+#pragma omp parallel reduction(+ : drops)
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        int32_t* b0 = (int32_t*)malloc(sizeof(int32_t) * 3 * 1024);
+        int32_t* b1 = (int32_t*)malloc(sizeof(int32_t) * 3 * 1024);
+#pragma omp for schedule(dynamic, 4096)
+        for (int64_t i = 0; i < npx; i++) {
+            int n0, n1;
+            pixel_alloc_blocks_m2(pm + 3 * i, nm + 3 * i, trunc, T, cam, s->voxel, b0, &n0, b1, &n1);
+            const uint32_t ptag = ((uint32_t)(i / W) << 16) | (uint32_t)(i % W);
+            for (int r = 0; r < 2; r++) {
+                const int n = r ? n1 : n0;
+                const int32_t* buf = r ? b1 : b0;
+                for (int j = 0; j < n; j++) {
+                    if (!in_range(buf + 3 * j)) {
+                        drops++;
+                        continue;
+                    }
+                    if (lens[tid] == caps[tid]) {
+                        caps[tid] = caps[tid] ? caps[tid] * 2 : 4096;
+                        lists[tid] = (uint64_t*)realloc(lists[tid], sizeof(uint64_t) * caps[tid]);
+                        tags[tid] = (uint32_t*)realloc(tags[tid], sizeof(uint32_t) * caps[tid]);
+                    }
+                    lists[tid][lens[tid]] = pack_key(buf[3 * j], buf[3 * j + 1], buf[3 * j + 2]);
+                    tags[tid][lens[tid]] = r ? ptag + 1u : 0u;
+                    lens[tid]++;
+                }
+            }
+        }
+        free(b0);
+        free(b1);
+    }
+    int64_t added = 0;
+    const uint64_t fr = (uint64_t)(s->frames + 1u) << 32;
+    for (int t = 0; t < nthr; t++) {
+        for (int64_t j = 0; j < lens[t]; j++) {
+            added += scene_add(s, lists[t][j]);
+            if (tags[t][j]) {
+                const int64_t at = map_find(s, lists[t][j]);
+                const uint64_t tag = fr | (uint64_t)(tags[t][j] - 1u);
+                if (tag > s->parent[at]) s->parent[at] = tag;
+            }
+        }
+        free(lists[t]);
+        free(tags[t]);
+    }
+    free(lists);
+    free(tags);
+    free(lens);
+    free(caps);
+    s->coord_range_drops += drops;
+    return added;
+}
+
 /* ---------------------------------------------------------- integration */
 
 /* integrateDepthMapIntoBlocksKernel, VoxelScene.cu:918-1146, for one voxel.
  * Returns 1 when the voxel was updated. */
 static inline int integrate_voxel(ovox* vx, int bx, int by, int bz, int idx, const float* pm,
                                   const uint8_t* rgb, int W, int H, float trunc, const float* T,
-                                  const float* cam, float v, float fx, float fy, float cx, float cy) {
+                                  const float* cam, float v, float fx, float fy, float cx, float cy,
+                                  int64_t parent_pi) {
     int lx = idx % BS, ly = (idx / BS) % BS, lz = idx / (BS * BS);
     /* (blockCoord*8 + local) * voxelSize, :959-963 (int arithmetic wraps) */
     float wx = (float)(int32_t)((uint32_t)bx * 8u + (uint32_t)lx) * v;
@@ -346,8 +467,11 @@ static inline int integrate_voxel(ovox* vx, int bx, int by, int bz, int idx, con
     float sx = px * fx / pz + cx; /* :984-987 */
     float sy = py * fy / pz + cy;
     int ix = f2i(sx + 0.5f), iy = f2i(sy + 0.5f); /* :990-993 */
-    if (!(ix >= 0 && ix < W && iy >= 0 && iy < H)) return 0;
-    int64_t pi = (int64_t)iy * W + ix;
+    int64_t pi = parent_pi; /* a valid stored parent pixel, :1015-1035 */
+    if (pi < 0) {
+        if (!(ix >= 0 && ix < W && iy >= 0 && iy < H)) return 0;
+        pi = (int64_t)iy * W + ix;
+    }
     const float* P = pm + 3 * pi;
     if (!(P[0] != 0.0f || P[1] != 0.0f || P[2] != 0.0f)) return 0; /* :1040-1046 */
     float Pw[3];
@@ -390,10 +514,20 @@ void orc_integrate_blocks(orc_scene* s, const float* pm, const uint8_t* rgb, int
         int32_t bc[3];
         unpack_key(s->keys[b], bc);
         ovox* blk = s->vox + b * VPB;
+        /* the block's parent pixel when inside this image and holding a
+         * point (VoxelScene.cu:1015-1035) */
+        int64_t ppi = -1;
+        if (s->parent[b]) {
+            const int px = (int)(s->parent[b] & 0xFFFFu), py = (int)((s->parent[b] >> 16) & 0xFFFFu);
+            if (px < W && py < H) {
+                const float* P = pm + 3 * ((int64_t)py * W + px);
+                if (P[0] != 0.0f || P[1] != 0.0f || P[2] != 0.0f) ppi = (int64_t)py * W + px;
+            }
+        }
         int cnt = 0;
         for (int i = 0; i < VPB; i++)
             cnt += integrate_voxel(blk + i, bc[0], bc[1], bc[2], i, pm, rgb, W, H, trunc, T, cam, s->voxel,
-                                   fx, fy, cx, cy);
+                                   fx, fy, cx, cy, ppi);
         nvox += cnt;
         nupd += cnt > 0;
     }
@@ -405,15 +539,24 @@ void orc_integrate_blocks(orc_scene* s, const float* pm, const uint8_t* rgb, int
  * is the translation column of the row-major camera->world matrix
  * (:462-466); allocation, then integration.  out[0]=new blocks,
  * out[1]=updated blocks, out[2]=updated voxels, out[3]=total blocks. */
-void orc_integrate(orc_scene* s, const float* pm, const uint8_t* rgb, int W, int H, float trunc,
-                   const float* T, float fx, float fy, float cx, float cy, int64_t* out) {
+void orc_integrate_nm(orc_scene* s, const float* pm, const uint8_t* rgb, const float* nm, int W, int H,
+                      float trunc, const float* T, float fx, float fy, float cx, float cy, int64_t* out) {
     float cam[3] = {T[3], T[7], T[11]};
-    out[0] = orc_alloc(s, pm, W, H, trunc, T, cam);
+    /* without normals the normal-direction allocation is skipped, as in
+     * allocBlocksFromDepthMapCUDA (VoxelScene.cu:1693-1715) */
+    out[0] = s->alloc_method == 2 ? (nm ? orc_alloc_m2(s, pm, nm, W, H, trunc, T, cam) : 0)
+                                  : orc_alloc(s, pm, W, H, trunc, T, cam);
     int64_t r[2];
     orc_integrate_blocks(s, pm, rgb, W, H, trunc, T, cam, fx, fy, cx, cy, r);
     out[1] = r[0];
     out[2] = r[1];
     out[3] = s->n;
+    s->frames++;
+}
+
+void orc_integrate(orc_scene* s, const float* pm, const uint8_t* rgb, int W, int H, float trunc,
+                   const float* T, float fx, float fy, float cx, float cy, int64_t* out) {
+    orc_integrate_nm(s, pm, rgb, NULL, W, H, trunc, T, fx, fy, cx, cy, out);
 }
 
 /* ------------------------------------------------------------- ray casting */
@@ -894,6 +1037,7 @@ int64_t orc_stream_out(orc_scene* s, const float* c, float radius, int32_t* coor
         } else {
             if (keep != i) {
                 s->keys[keep] = s->keys[i];
+                s->parent[keep] = s->parent[i];
                 memcpy(s->vox + keep * VPB, s->vox + i * VPB, sizeof(ovox) * VPB);
             }
             keep++;
@@ -978,6 +1122,19 @@ void orc_export(const orc_scene* s, int32_t* coords, uint8_t* voxels) {
         memcpy(coords + 3 * i, t[i].c, sizeof(int32_t) * 3);
         if (voxels) memcpy(voxels + i * VPB * 8, s->vox + (int64_t)t[i].idx * VPB, VPB * 8);
     }
+    free(t);
+}
+
+/* Parent tags of the blocks in orc_export's order (0 = none, else
+ * (frame + 1) << 32 | y << 16 | x). */
+void orc_export_parents(const orc_scene* s, uint64_t* out) {
+    keyidx* t = (keyidx*)malloc(sizeof(keyidx) * (s->n ? s->n : 1));
+    for (int64_t i = 0; i < s->n; i++) {
+        unpack_key(s->keys[i], t[i].c);
+        t[i].idx = (int32_t)i;
+    }
+    qsort(t, s->n, sizeof(keyidx), cmp_key3);
+    for (int64_t i = 0; i < s->n; i++) out[i] = s->parent[t[i].idx];
     free(t);
 }
 

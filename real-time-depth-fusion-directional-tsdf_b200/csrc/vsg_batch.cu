@@ -236,6 +236,8 @@ int vsg_batch_step(vsg_batch* b, const vsg_batch_frame* frames, int n_frames, vs
         if (f.scene < 0 || f.scene >= (int)B.scenes.size() || seen[f.scene]) return VSG_ERR_INVALID_ARG;
         seen[f.scene] = 1;
         if (!f.pointmap || !f.rgb || !f.normals || f.w <= 0 || f.h <= 0) return VSG_ERR_INVALID_ARG;
+        // normal-direction allocation needs its own parent pass: per-scene calls only
+        if (B.scenes[f.scene]->dev.alloc_method == 2) return VSG_ERR_INVALID_ARG;
         if (f.render) {
             Renderer* r = B.renderers[f.scene];
             if (!r || r->w != f.w || r->h != f.h) return VSG_ERR_INVALID_ARG;
@@ -280,6 +282,7 @@ int vsg_batch_step(vsg_batch* b, const vsg_batch_frame* frames, int n_frames, vs
         A.s = sc->dev;
         A.pm = f.pointmap;
         A.rgb = f.rgb;
+        A.nm = f.normals;
         A.W = f.w;
         A.H = f.h;
         A.trunc = f.truncation;

@@ -9,7 +9,9 @@
 #include <algorithm>
 #include <array>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
+#include <filesystem>
 #include <new>
 #include <vector>
 
@@ -164,8 +166,15 @@ int vsg_integrate(vsg_scene* s, const float* pointmap, const uint8_t* rgb, const
     if (!s) return VSG_ERR_NOT_ALLOCATED;
     if (!pointmap || !rgb || !normals || !pose) return VSG_ERR_INVALID_ARG;
     if (w <= 0 || h <= 0 || (long long)w * h > (1ll << 30)) return VSG_ERR_INVALID_ARG;
-    return vsg::scene_integrate(&s->impl, pointmap, rgb, w, h, truncation, pose, fx, fy, cx, cy,
+    return vsg::scene_integrate(&s->impl, pointmap, rgb, normals, w, h, truncation, pose, fx, fy, cx, cy,
                                 (cudaStream_t)stream);
+}
+
+int vsg_scene_set_alloc_method(vsg_scene* s, int method) {
+    if (!s) return VSG_ERR_NOT_ALLOCATED;
+    if (method != 1 && method != 2) return VSG_ERR_INVALID_ARG;
+    s->impl.dev.alloc_method = method;
+    return VSG_OK;
 }
 
 int vsg_scene_stats(vsg_scene* s, vsg_stats* out) {
@@ -313,6 +322,47 @@ int vsg_renderer_download(const vsg_renderer* r, float* depth, float* position, 
     if (color && cudaMemcpy(color, r->impl.color, n * 16, cudaMemcpyDeviceToHost) != cudaSuccess) return VSG_ERR_CUDA;
     if (normal && cudaMemcpy(normal, r->impl.normal, n * 16, cudaMemcpyDeviceToHost) != cudaSuccess)
         return VSG_ERR_CUDA;
+    return VSG_OK;
+}
+
+int vsg_renderer_save_ply(const vsg_renderer* r, const char* path, int64_t* n_points) {
+    if (!r || !path) return VSG_ERR_INVALID_ARG;
+    if (n_points) *n_points = 0;
+    const size_t n = (size_t)r->impl.w * r->impl.h;
+    std::vector<float> D(n);
+    std::vector<float4> P(n), C(n);
+    int rc = vsg_renderer_download(r, D.data(), reinterpret_cast<float*>(P.data()),
+                                   reinterpret_cast<float*>(C.data()), nullptr);
+    if (rc != VSG_OK) return rc;
+    auto valid = [&](size_t i) {
+        return std::isfinite(D[i]) && D[i] > 0.0f && std::fabs(D[i]) < 1e9f && std::isfinite(P[i].x) &&
+               std::isfinite(P[i].y) && std::isfinite(P[i].z);
+    };
+    int64_t count = 0;
+    for (size_t i = 0; i < n; ++i) count += valid(i) ? 1 : 0;
+    if (count == 0) return VSG_ERR_INVALID_ARG;
+    std::error_code ec;
+    const std::filesystem::path out(path);
+    if (out.has_parent_path()) std::filesystem::create_directories(out.parent_path(), ec);
+    FILE* f = std::fopen(path, "w");
+    if (!f) return VSG_ERR_INVALID_ARG;
+    std::fprintf(f,
+                 "ply\nformat ascii 1.0\ncomment Generated by RayCastRender\nelement vertex %lld\n"
+                 "property float x\nproperty float y\nproperty float z\n"
+                 "property uchar red\nproperty uchar green\nproperty uchar blue\nend_header\n",
+                 (long long)count);
+    auto channel = [](float c) -> int {
+        if (!std::isfinite(c)) return 255;
+        c = c < 0.0f ? 0.0f : (c > 1.0f ? 1.0f : c);
+        return static_cast<int>(c * 255.0f + 0.5f);
+    };
+    for (size_t i = 0; i < n; ++i) {
+        if (!valid(i)) continue;
+        std::fprintf(f, "%g %g %g %d %d %d\n", P[i].x, P[i].y, P[i].z, channel(C[i].x), channel(C[i].y),
+                     channel(C[i].z));
+    }
+    if (std::fclose(f) != 0) return VSG_ERR_INVALID_ARG;
+    if (n_points) *n_points = count;
     return VSG_OK;
 }
 

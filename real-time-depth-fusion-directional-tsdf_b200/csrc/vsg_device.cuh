@@ -98,7 +98,7 @@ struct FrameCounters {
     uint32_t blocks_read;    // distinct blocks the last render read (instrumented runs)
     uint32_t lane_iters;     // march loop iterations summed over rays (x1/32 per warp)
     uint32_t warp_iters;     // per-warp maximum iterations summed over warps
-    uint32_t pad2;
+    uint32_t n_parent;       // normal-direction allocation: parent records appended
 };
 
 struct SceneDev {
@@ -118,6 +118,17 @@ struct SceneDev {
     uint32_t* visible;
     float4* pix_world;   // per pixel of the current frame: T*p and |T*p - c| (-1 = invalid)
     uint32_t* pix_rgb;   // per pixel: r | g<<8 | b<<16
+    // normal-direction allocation (VoxelScene.cu:768-912): per pool block the
+    // parent pixel of the last normal ray that visited it, packed as
+    // (frame + 1) << 32 | y << 16 | x (0 = none); cleared when the block is
+    // claimed.  Integration reads a block's parent pixel instead of each
+    // voxel's projection (VoxelScene.cu:1015-1035).
+    unsigned long long* block_parent;
+    unsigned long long* parent_key;  // this frame's (block, pixel) records from k_alloc
+    uint32_t* parent_tag;            // y << 16 | x
+    uint32_t parent_cap;
+    int alloc_method;                // 1: camera-z band (Method 1), 2: camera + normal rays (Method 2)
+    uint32_t frame_seq;              // frames integrated since reset (the parent tags' frame)
     SceneCounters* ctr;
     FrameCounters* frame;
     uint32_t num_buckets;

@@ -19,6 +19,7 @@
 //                   (VoxelScene.cu:918-1146)
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -37,6 +38,10 @@ namespace vsg {
 // ====================================================================
 
 __global__ void __launch_bounds__(kTile* kTile) k_alloc(AllocArgs a) { alloc_tile(a, blockIdx.x, blockIdx.y); }
+
+__global__ void __launch_bounds__(256) k_parents(SceneDev s) {
+    apply_parents(s, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
 
 __global__ void __launch_bounds__(256) k_select(IntegArgs a) {
     select_blocks(a, blockIdx.x * blockDim.x, gridDim.x * blockDim.x);
@@ -89,6 +94,7 @@ int scene_alloc_device(Scene* sc) {
     VSG_MALLOC(d.block_fresh, B);
     VSG_MALLOC(d.block_wmask, B * sizeof(unsigned long long));
     VSG_MALLOC(d.block_touched, B);
+    VSG_MALLOC(d.block_parent, B * sizeof(unsigned long long));
     VSG_MALLOC(d.heap, B * sizeof(uint32_t));
     VSG_MALLOC(d.bindex, sizeof(unsigned long long) << (3 * sc->bidx_log2));
     VSG_MALLOC(d.dwm, sizeof(unsigned long long) << (3 * sc->bidx_log2));
@@ -97,6 +103,10 @@ int scene_alloc_device(Scene* sc) {
     d.pix_world = nullptr;
     d.pix_rgb = nullptr;
     sc->pix_capacity = 0;
+    d.parent_key = nullptr;
+    d.parent_tag = nullptr;
+    d.parent_cap = 0;
+    d.alloc_method = 1;
     VSG_MALLOC(d.ctr, sizeof(SceneCounters));
     VSG_MALLOC(d.frame, sizeof(FrameCounters));
 #undef VSG_MALLOC
@@ -117,7 +127,7 @@ int scene_alloc_device(Scene* sc) {
 
 void scene_free_device(Scene* sc) {
     SceneDev& d = sc->dev;
-    void* ptrs[] = {d.block_touched, d.sup, d.dwm,     d.bindex,    d.block_wmask, d.buckets,   d.bucket_next,
+    void* ptrs[] = {d.block_parent, d.parent_key, d.parent_tag, d.block_touched, d.sup, d.dwm,     d.bindex,    d.block_wmask, d.buckets,   d.bucket_next,
                     d.nodes,     d.voxels,  d.block_key, d.block_slot,  d.block_fresh, d.heap,
                     d.visible,   d.pix_world, d.pix_rgb, d.ctr,         d.frame};
     for (void* p : ptrs)
@@ -134,6 +144,7 @@ int scene_reset_device(Scene* sc, cudaStream_t st) {
     cudaMemsetAsync(d.nodes, 0xFF, M * sizeof(Node), st);
     cudaMemsetAsync(d.block_key, 0xFF, B * sizeof(unsigned long long), st);
     cudaMemsetAsync(d.block_fresh, 0, B, st);
+    cudaMemsetAsync(d.block_parent, 0, B * sizeof(unsigned long long), st);
     cudaMemsetAsync(d.bindex, 0xFF, sizeof(unsigned long long) << (3 * sc->bidx_log2), st);
     cudaMemsetAsync(d.dwm, 0, sizeof(unsigned long long) << (3 * sc->bidx_log2), st);
     cudaMemsetAsync(d.sup, 0, sup_words(sc->bidx_log2) * 4, st);
@@ -142,6 +153,29 @@ int scene_reset_device(Scene* sc, cudaStream_t st) {
     k_frame_begin<<<1, 1, 0, st>>>(d.frame);
     sc->integrated_frames = 0;
     return cudaGetLastError() == cudaSuccess ? VSG_OK : VSG_ERR_CUDA;
+}
+
+// Parent records of one normal-direction allocation: a normal ray of length
+// truncation visits at most 1 + 3 (floor(t / 8v) + 1) blocks; one record
+// per (tile, block) and per block a full tile set could not take, so
+// pixels x that bound covers every frame (grows only).
+int ensure_parent_buffers(Scene* sc, size_t npx, float trunc) {
+    SceneDev& d = sc->dev;
+    const double ext = 8.0 * (double)d.voxel;
+    const double per_ray = 1.0 + 3.0 * (std::floor(std::fabs((double)trunc) / ext) + 1.0);
+    const double want = std::ceil((double)npx * per_ray);
+    if (want > 4.0e9) return VSG_ERR_TOO_LARGE;
+    if ((size_t)want <= d.parent_cap) return VSG_OK;
+    cudaFree(d.parent_key);
+    cudaFree(d.parent_tag);
+    d.parent_key = nullptr;
+    d.parent_tag = nullptr;
+    d.parent_cap = 0;
+    if (cudaMalloc(&d.parent_key, (size_t)want * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&d.parent_tag, (size_t)want * sizeof(uint32_t)) != cudaSuccess)
+        return VSG_ERR_OUT_OF_MEMORY;
+    d.parent_cap = (uint32_t)want;
+    return VSG_OK;
 }
 
 int ensure_pixel_buffers(Scene* sc, size_t npx) {
@@ -159,10 +193,14 @@ int ensure_pixel_buffers(Scene* sc, size_t npx) {
     return VSG_OK;
 }
 
-int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H, float trunc,
+int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, const float* nm, int W, int H, float trunc,
                     const float* pose, float fx, float fy, float cx, float cy, cudaStream_t st) {
-    const int prc = ensure_pixel_buffers(sc, (size_t)W * H);
+    const bool by_normal = sc->dev.alloc_method == 2;
+    if (by_normal && (W > 65535 || H > 65535)) return VSG_ERR_TOO_LARGE;
+    int prc = ensure_pixel_buffers(sc, (size_t)W * H);
+    if (prc == VSG_OK && by_normal) prc = ensure_parent_buffers(sc, (size_t)W * H, trunc);
     if (prc != VSG_OK) return prc;
+    sc->dev.frame_seq = sc->integrated_frames;
     Pose P;
     memcpy(P.T, pose, sizeof(P.T));
     k_frame_begin<<<1, 1, 0, st>>>(sc->dev.frame);
@@ -170,6 +208,7 @@ int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H
     aa.s = sc->dev;
     aa.pm = pm;
     aa.rgb = rgb;
+    aa.nm = nm;
     aa.W = W;
     aa.H = H;
     aa.trunc = trunc;
@@ -177,6 +216,7 @@ int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H
     dim3 grid((W + kTile - 1) / kTile, (H + kTile - 1) / kTile);
     timing_begin(sc, kSlotAlloc, st);
     k_alloc<<<grid, kTile * kTile, 0, st>>>(aa);
+    if (by_normal) k_parents<<<sc->sm_count * 2, 256, 0, st>>>(sc->dev);
     timing_end(sc, kSlotAlloc, st);
     IntegArgs ia;
     ia.s = sc->dev;
@@ -204,6 +244,9 @@ int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H
 int scene_integrate_with_pixels(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H, float trunc,
                                 const float* pose, float fx, float fy, float cx, float cy, float4* pix_world,
                                 uint32_t* pix_rgb, cudaStream_t st) {
+    // normal-direction allocation keeps per-frame parent records in buffers
+    // of the scene's own: not available here
+    if (sc->dev.alloc_method == 2) return VSG_ERR_INVALID_ARG;
     Pose P;
     memcpy(P.T, pose, sizeof(P.T));
     SceneDev dev = sc->dev;
@@ -214,6 +257,7 @@ int scene_integrate_with_pixels(Scene* sc, const float* pm, const uint8_t* rgb, 
     aa.s = dev;
     aa.pm = pm;
     aa.rgb = rgb;
+    aa.nm = nullptr;
     aa.W = W;
     aa.H = H;
     aa.trunc = trunc;

@@ -21,6 +21,7 @@ struct AllocArgs {
     SceneDev s;
     const float* pm;
     const uint8_t* rgb;
+    const float* nm;  // camera-space normals (normal-direction allocation only)
     int W, H;
     float trunc;
     Pose pose;
@@ -71,6 +72,7 @@ static __device__ __noinline__ bool claim_block(const SceneDev& s, unsigned long
     s.block_key[blk] = key;
     s.block_slot[blk] = slot_index;
     s.block_fresh[blk] = 1;
+    s.block_parent[blk] = 0ull;
     atomicMax(&s.ctr->high_water, blk + 1);
     int x, y, z;
     unpack_key(key, x, y, z);
@@ -217,30 +219,112 @@ static __device__ void coop_insert(const SceneDev& s, unsigned long long key, bo
     if (pending && sub == 0) atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_INSERT_RETRY);
 }
 
-static __device__ __forceinline__ bool set_insert(unsigned long long* set, unsigned long long k) {
+// Slot of k in the tile's shared set (inserted when absent), or -1 when
+// the probe gives up (the set is full).
+static __device__ __forceinline__ int set_insert(unsigned long long* set, unsigned long long k) {
     uint32_t h = (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> 54) & (kSetCap - 1);
 #pragma unroll 1
     for (int p = 0; p < 32; ++p) {
         unsigned long long cur = *(volatile unsigned long long*)(set + h);
-        if (cur == k) return true;
+        if (cur == k) return (int)h;
         if (cur == kKeyEmpty) {
             unsigned long long prev = atomicCAS(set + h, kKeyEmpty, k);
-            if (prev == kKeyEmpty || prev == k) return true;
+            if (prev == kKeyEmpty || prev == k) return (int)h;
         }
         h = (h + 1) & (kSetCap - 1);
     }
-    return false;
+    return -1;
+}
+
+// A (block, parent pixel) record for apply_parents.
+static __device__ __forceinline__ void append_parent(const SceneDev& s, unsigned long long key, uint32_t tag) {
+    const uint32_t i = atomicAdd(&s.frame->n_parent, 1u);
+    if (i < s.parent_cap) {
+        s.parent_key[i] = key;
+        s.parent_tag[i] = tag;
+    } else {
+        atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_PARENT_OVERFLOW);
+    }
+}
+
+// allocateBlocksAlongRay, VoxelScene.cu:295-481: nothing when both ends
+// fall in one block (:345-348); else a block-level DDA from st to en with
+// boundaries at (id + [step > 0]) * 8v - v/2 (:373-394), x only when its
+// tMax is strictly smallest, then y when tMax.y < tMax.z, else z
+// (:464-475), at most 1024 blocks (:417).  Visited blocks go into the
+// tile's set, or straight into the table when the set is full.  ptag != 0
+// (normal rays): (y << 16 | x) + 1 of the pixel, kept as the maximum per
+// set slot.
+static __device__ void dda_ray(const SceneDev& s, unsigned long long* set, uint32_t* set_tag, const float st[3],
+                               const float en[3], uint32_t ptag) {
+    const float v = s.voxel;
+    int c[3], e[3];
+    world_to_block_alloc(st[0], st[1], st[2], v, c[0], c[1], c[2]);
+    world_to_block_alloc(en[0], en[1], en[2], v, e[0], e[1], e[2]);
+    if (c[0] == e[0] && c[1] == e[1] && c[2] == e[2]) return;
+    float d[3] = {en[0] - st[0], en[1] - st[1], en[2] - st[2]};
+    const float len = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    if (len < 1e-6f) return;
+    d[0] /= len;
+    d[1] /= len;
+    d[2] /= len;
+    const float ext = (float)kBlock * v;
+    float step[3], tmax[3], tdel[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        step[k] = (d[k] > 0) ? 1.0f : -1.0f;
+        const float sc = (step[k] > 0) ? 1.0f : 0.0f;
+        const float bnd = ((float)c[k] + sc) * ext - 0.5f * v;
+        tmax[k] = (bnd - st[k]) / d[k];
+        tdel[k] = (step[k] * ext) / d[k];
+        if (d[k] == 0.0f) {
+            tmax[k] = 1e6f;
+            tdel[k] = 1e6f;
+        }
+    }
+#pragma unroll 1
+    for (int it = 0; it < kMaxDDA; ++it) {
+        if (coord_ok(c[0], c[1], c[2])) {
+            const unsigned long long k = pack_key(c[0], c[1], c[2]);
+            const int slot = set_insert(set, k);
+            if (slot < 0) {
+                insert_single(s, k, c[0], c[1], c[2]);
+                if (ptag) append_parent(s, k, ptag - 1u);
+            } else if (ptag) {
+                atomicMax(set_tag + slot, ptag);
+            }
+        } else {
+            atomicAdd(&s.ctr->coord_drops, 1u);
+            atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_COORD_RANGE);
+        }
+        if (c[0] == e[0] && c[1] == e[1] && c[2] == e[2]) break;
+        if (tmax[0] < tmax[1] && tmax[0] < tmax[2]) {
+            tmax[0] += tdel[0];
+            c[0] += (int)step[0];
+        } else if (tmax[1] < tmax[2]) {
+            tmax[1] += tdel[1];
+            c[1] += (int)step[1];
+        } else {
+            tmax[2] += tdel[2];
+            c[2] += (int)step[2];
+        }
+    }
 }
 
 // One 16x16 pixel tile (tile_x, tile_y) per CTA of kTile*kTile threads.
 static __device__ __forceinline__ void alloc_tile(const AllocArgs& a, int tile_x, int tile_y) {
     __shared__ unsigned long long set[kSetCap];
     __shared__ unsigned long long list[kSetCap];
+    __shared__ uint32_t set_tag[kSetCap];
     __shared__ int list_n;
     __shared__ uint32_t s_zmin, s_zmax, s_nonfinite, s_valid;
     const int tid = threadIdx.x;
     const SceneDev& s = a.s;
-    for (int i = tid; i < kSetCap; i += blockDim.x) set[i] = kKeyEmpty;
+    const bool by_normal = s.alloc_method == 2;
+    for (int i = tid; i < kSetCap; i += blockDim.x) {
+        set[i] = kKeyEmpty;
+        if (by_normal) set_tag[i] = 0u;
+    }
     if (tid == 0) {
         list_n = 0;
         s_zmin = 0xFFFFFFFFu;
@@ -275,74 +359,65 @@ static __device__ __forceinline__ void alloc_tile(const AllocArgs& a, int tile_x
         s.pix_world[pi] = prep;
         s.pix_rgb[pi] = (uint32_t)__ldg(a.rgb + 3 * pi) | ((uint32_t)__ldg(a.rgb + 3 * pi + 1) << 8) |
                         ((uint32_t)__ldg(a.rgb + 3 * pi + 2) << 16);
-        // allocBlocksFromDepthMapMethod1Kernel, VoxelScene.cu:547-633
-        if (!(p2 <= 1e-6f)) {
-            const float cx = a.pose.T[3], cy = a.pose.T[7], cz = a.pose.T[11];
-            float wx, wy, wz;
-            xform(a.pose, p0, p1, p2, wx, wy, wz);
-            const float rx = wx - cx, ry = wy - cy, rz = wz - cz;
-            const float rl = sqrtf(rx * rx + ry * ry + rz * rz);
-            if (!(rl < 1e-6f)) {
-                float s0, s1, s2, e0, e1, e2;
-                xform(a.pose, p0, p1, p2 - a.trunc, s0, s1, s2);
-                xform(a.pose, p0, p1, p2 + a.trunc, e0, e1, e2);
-                // allocateBlocksAlongRay, VoxelScene.cu:295-481
-                const float v = s.voxel;
-                int c[3], e[3];
-                world_to_block_alloc(s0, s1, s2, v, c[0], c[1], c[2]);
-                world_to_block_alloc(e0, e1, e2, v, e[0], e[1], e[2]);
-                if (!(c[0] == e[0] && c[1] == e[1] && c[2] == e[2])) {
-                    float d[3] = {e0 - s0, e1 - s1, e2 - s2};
-                    const float len = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-                    if (!(len < 1e-6f)) {
-                        d[0] /= len;
-                        d[1] /= len;
-                        d[2] /= len;
-                        const float st[3] = {s0, s1, s2};
-                        const float ext = (float)kBlock * v;
-                        float step[3], tmax[3], tdel[3];
-#pragma unroll
-                        for (int k = 0; k < 3; ++k) {
-                            step[k] = (d[k] > 0) ? 1.0f : -1.0f;
-                            const float sc = (step[k] > 0) ? 1.0f : 0.0f;
-                            const float bnd = ((float)c[k] + sc) * ext - 0.5f * v;
-                            tmax[k] = (bnd - st[k]) / d[k];
-                            tdel[k] = (step[k] * ext) / d[k];
-                            if (d[k] == 0.0f) {
-                                tmax[k] = 1e6f;
-                                tdel[k] = 1e6f;
-                            }
-                        }
-#pragma unroll 1
-                        for (int it = 0; it < kMaxDDA; ++it) {
-                            if (coord_ok(c[0], c[1], c[2])) {
-                                const unsigned long long k = pack_key(c[0], c[1], c[2]);
-                                if (!set_insert(set, k)) insert_single(s, k, c[0], c[1], c[2]);
-                            } else {
-                                atomicAdd(&s.ctr->coord_drops, 1u);
-                                atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_COORD_RANGE);
-                            }
-                            if (c[0] == e[0] && c[1] == e[1] && c[2] == e[2]) break;
-                            if (tmax[0] < tmax[1] && tmax[0] < tmax[2]) {
-                                tmax[0] += tdel[0];
-                                c[0] += (int)step[0];
-                            } else if (tmax[1] < tmax[2]) {
-                                tmax[1] += tdel[1];
-                                c[1] += (int)step[1];
-                            } else {
-                                tmax[2] += tdel[2];
-                                c[2] += (int)step[2];
-                            }
-                        }
-                    }
+        const float cx = a.pose.T[3], cy = a.pose.T[7], cz = a.pose.T[11];
+        if (!by_normal) {
+            // allocBlocksFromDepthMapMethod1Kernel, VoxelScene.cu:547-633:
+            // the camera-space segment p.z -+ truncation
+            if (!(p2 <= 1e-6f)) {
+                float wx, wy, wz;
+                xform(a.pose, p0, p1, p2, wx, wy, wz);
+                const float rx = wx - cx, ry = wy - cy, rz = wz - cz;
+                const float rl = sqrtf(rx * rx + ry * ry + rz * rz);
+                if (!(rl < 1e-6f)) {
+                    float st[3], en[3];
+                    xform(a.pose, p0, p1, p2 - a.trunc, st[0], st[1], st[2]);
+                    xform(a.pose, p0, p1, p2 + a.trunc, en[0], en[1], en[2]);
+                    dda_ray(s, set, set_tag, st, en, 0u);
                 }
+            }
+        } else if (p0 != 0.0f || p1 != 0.0f || p2 != 0.0f) {
+            // allocBlocksFromDepthMapMethod2Kernel, VoxelScene.cu:797-911
+            float n0 = __ldg(a.nm + 3 * pi + 0), n1 = __ldg(a.nm + 3 * pi + 1), n2 = __ldg(a.nm + 3 * pi + 2);
+            float nl = sqrtf(n0 * n0 + n1 * n1 + n2 * n2);
+            if (!(nl < 0.1f)) {
+                n0 /= nl;
+                n1 /= nl;
+                n2 /= nl;
+                float w[3];
+                xform(a.pose, p0, p1, p2, w[0], w[1], w[2]);
+                const float* T = a.pose.T;
+                float nw[3] = {T[0] * n0 + T[1] * n1 + T[2] * n2, T[4] * n0 + T[5] * n1 + T[6] * n2,
+                               T[8] * n0 + T[9] * n1 + T[10] * n2};
+                nl = sqrtf(nw[0] * nw[0] + nw[1] * nw[1] + nw[2] * nw[2]);
+                if (nl > 1e-6f) {
+                    nw[0] /= nl;
+                    nw[1] /= nl;
+                    nw[2] /= nl;
+                }
+                // camera ray: from the point to truncation behind it
+                float rd[3] = {w[0] - cx, w[1] - cy, w[2] - cz};
+                const float rl = sqrtf(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2]);
+                if (rl > 0.0f) {
+                    rd[0] /= rl;
+                    rd[1] /= rl;
+                    rd[2] /= rl;
+                    const float en[3] = {w[0] + rd[0] * a.trunc, w[1] + rd[1] * a.trunc, w[2] + rd[2] * a.trunc};
+                    dda_ray(s, set, set_tag, w, en, 0u);
+                }
+                // normal ray: from the point to truncation inside the surface;
+                // its blocks take this pixel as parent
+                const float en[3] = {w[0] - nw[0] * a.trunc, w[1] - nw[1] * a.trunc, w[2] - nw[2] * a.trunc};
+                dda_ray(s, set, set_tag, w, en, (((uint32_t)py << 16) | (uint32_t)px) + 1u);
             }
         }
     }
     __syncthreads();
     for (int i = tid; i < kSetCap; i += blockDim.x) {
         const unsigned long long k = set[i];
-        if (k != kKeyEmpty) list[atomicAdd(&list_n, 1)] = k;
+        if (k != kKeyEmpty) {
+            list[atomicAdd(&list_n, 1)] = k;
+            if (by_normal && set_tag[i]) append_parent(s, k, set_tag[i] - 1u);
+        }
     }
     __syncthreads();
     const int n = list_n;
@@ -362,6 +437,34 @@ static __device__ __forceinline__ void alloc_tile(const AllocArgs& a, int tile_x
             if (s_nonfinite) atomicOr(&s.frame->nonfinite, 1u);
         }
     }
+}
+
+// After a normal-direction allocation: each (block, pixel) record raises
+// the block's parent to (frame + 1) << 32 | y << 16 | x.  Of several normal
+// rays through one block in a frame the last pixel in row-major order
+// wins (the reference keeps whichever write lands last).
+static __device__ __forceinline__ void apply_parents(const SceneDev& s, uint32_t first, uint32_t stride) {
+    const uint32_t n = min(*(volatile uint32_t*)&s.frame->n_parent, s.parent_cap);
+    const unsigned long long fr = (unsigned long long)(s.frame_seq + 1u) << 32;
+    for (uint32_t i = first; i < n; i += stride) {
+        const unsigned long long key = s.parent_key[i];
+        int x, y, z;
+        unpack_key(key, x, y, z);
+        const int b = lookup_block(s, key, x, y, z);
+        if (b >= 0) atomicMax(s.block_parent + b, fr | (unsigned long long)s.parent_tag[i]);
+    }
+}
+
+// The parent pixel a block integrates from this frame (VoxelScene.cu:
+// 1015-1035): its stored parent when that lies inside this frame's image
+// and holds a point; else -1 (each voxel projects).
+static __device__ __forceinline__ int parent_pixel(const SceneDev& s, int blk, int W, int H) {
+    const unsigned long long t = s.block_parent[blk];
+    if (!t) return -1;
+    const int x = (int)(t & 0xFFFFu), y = (int)((t >> 16) & 0xFFFFu);
+    if (x >= W || y >= H) return -1;
+    const int pi = y * W + x;
+    return s.pix_world[pi].w < 0.0f ? -1 : pi;
 }
 
 // ====================================================================
@@ -415,6 +518,25 @@ static __device__ bool block_maybe_updated(const IntegArgs& a, int bx, int by, i
     return true;
 }
 
+// Can a voxel of block (bx,by,bz) lie within the truncation distance of
+// the world point P its parent pixel gives every voxel?  Distance from P to
+// the box of the block's voxel centres, with a rounding margin.
+static __device__ __forceinline__ bool parent_near(const IntegArgs& a, int bx, int by, int bz, float4 P) {
+    if (!(isfinite(P.x) && isfinite(P.y) && isfinite(P.z))) return true;
+    const float v = a.s.voxel, eps = 1e-3f + 2.0f * v;
+    const float p[3] = {P.x, P.y, P.z};
+    const int b[3] = {bx, by, bz};
+    float d2 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float lo = (float)(b[k] * 8) * v - eps, hi = (float)(b[k] * 8 + 7) * v + eps;
+        const float d = p[k] < lo ? lo - p[k] : (p[k] > hi ? p[k] - hi : 0.0f);
+        d2 += d * d;
+    }
+    const float r = a.trunc + eps;
+    return d2 <= r * r;
+}
+
 // Visible-block compaction: one thread per pool block in [0, high_water),
 // ballot + popc, one atomic per warp.  Stands in for compactifyHashKernel
 // (VoxelScene.cu:1275-1300), which lists every allocated block: blocks the
@@ -440,7 +562,12 @@ static __device__ __forceinline__ void select_blocks(const IntegArgs& a, uint32_
                 if (s.block_fresh[b]) {
                     vis = true;
                 } else if (any_valid) {
-                    if (!cull) {
+                    const int pp = parent_pixel(s, (int)b, a.W, a.H);
+                    if (pp >= 0) {
+                        int bx, by, bz;
+                        unpack_key(key, bx, by, bz);
+                        vis = parent_near(a, bx, by, bz, s.pix_world[pp]);
+                    } else if (!cull) {
                         vis = true;
                     } else {
                         int bx, by, bz;
@@ -477,6 +604,7 @@ static __device__ void integrate_block(const IntegArgs& a, int blk, unsigned lon
     const int lx = lane & 7;
     const float wx = (float)(int)((unsigned)bx * 8u + (unsigned)lx) * v;
     const float rx = wx - T[3];
+    const int ppix = parent_pixel(s, blk, a.W, a.H);
     int cnt = 0;
     unsigned long long wm = 0ull;  // sub-cubes that received a weight this frame
 #pragma unroll 1
@@ -496,7 +624,7 @@ static __device__ void integrate_block(const IntegArgs& a, int blk, unsigned lon
             const float sx = cxp * a.fx / czp + a.cx;
             const float sy = cyp * a.fy / czp + a.cy;
             const int ix = __float2int_rz(sx + 0.5f), iy = __float2int_rz(sy + 0.5f);
-            pix[j] = (ix >= 0 && ix < a.W && iy >= 0 && iy < a.H) ? iy * a.W + ix : -1;
+            pix[j] = ppix >= 0 ? ppix : ((ix >= 0 && ix < a.W && iy >= 0 && iy < a.H) ? iy * a.W + ix : -1);
         }
         float4 P[kIntegBatch];
 #pragma unroll

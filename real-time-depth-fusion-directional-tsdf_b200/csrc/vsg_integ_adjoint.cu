@@ -65,6 +65,16 @@ __global__ void __launch_bounds__(kIbWarps * 32) k_integrate_backward(IntegBackA
         if (key == kKeyEmpty || key == kKeyTomb) continue;
         int bx, by, bz;
         unpack_key(key, bx, by, bz);
+        // the block's stored parent pixel, as the forward chose it
+        // (VoxelScene.cu:1015-1035)
+        int ppix = -1;
+        if (const unsigned long long pt = s.block_parent[b]) {
+            const int px = (int)(pt & 0xFFFFu), py = (int)((pt >> 16) & 0xFFFFu);
+            if (px < a.W && py < a.H) {
+                const size_t q = (size_t)py * a.W + px;
+                if (a.pm[3 * q] != 0.0f || a.pm[3 * q + 1] != 0.0f || a.pm[3 * q + 2] != 0.0f) ppix = (int)q;
+            }
+        }
         const int lx = lane & 7;
         const float wx = (float)(int)((unsigned)bx * 8u + (unsigned)lx) * v;
         const float rx = wx - T[3];
@@ -81,8 +91,8 @@ __global__ void __launch_bounds__(kIbWarps * 32) k_integrate_backward(IntegBackA
             const float sx = cxp * a.fx / czp + a.cx;
             const float sy = cyp * a.fy / czp + a.cy;
             const int ix = __float2int_rz(sx + 0.5f), iy = __float2int_rz(sy + 0.5f);
-            if (!(ix >= 0 && ix < a.W && iy >= 0 && iy < a.H)) continue;
-            const size_t pix = (size_t)iy * a.W + ix;
+            if (ppix < 0 && !(ix >= 0 && ix < a.W && iy >= 0 && iy < a.H)) continue;
+            const size_t pix = ppix >= 0 ? (size_t)ppix : (size_t)iy * a.W + ix;
             const float p0 = a.pm[3 * pix], p1 = a.pm[3 * pix + 1], p2 = a.pm[3 * pix + 2];
             if (p0 == 0.0f && p1 == 0.0f && p2 == 0.0f) continue;
             // depthPos_world and cameraDist, as the allocation kernel forms them

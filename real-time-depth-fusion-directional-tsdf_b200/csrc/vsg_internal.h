@@ -61,7 +61,7 @@ struct Renderer {
 int scene_alloc_device(Scene* sc);
 void scene_free_device(Scene* sc);
 int scene_reset_device(Scene* sc, cudaStream_t st);
-int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H, float trunc,
+int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, const float* nm, int W, int H, float trunc,
                     const float* pose, float fx, float fy, float cx, float cy, cudaStream_t st);
 int ensure_pixel_buffers(Scene* sc, size_t npx);
 int scene_integrate_with_pixels(Scene* sc, const float* pm, const uint8_t* rgb, int W, int H, float trunc,

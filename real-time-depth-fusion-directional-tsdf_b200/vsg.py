@@ -19,12 +19,14 @@ VSG_OK = 0
 STATUS = {0: "VSG_OK", 1: "VSG_ERR_INVALID_ARG", 2: "VSG_ERR_NOT_ALLOCATED", 3: "VSG_ERR_CUDA",
           4: "VSG_ERR_OUT_OF_MEMORY", 5: "VSG_ERR_TOO_LARGE"}
 FLAG_HEAP_EXHAUSTED, FLAG_CHAIN_EXHAUSTED, FLAG_COORD_RANGE, FLAG_INSERT_RETRY, FLAG_MARCH_LIMIT = 1, 2, 4, 8, 16
+FLAG_PARENT_OVERFLOW = 32
 
 # every symbol include/vsg.h declares
 EXPORTS = [
     "vsg_params_default", "vsg_scene_create", "vsg_scene_destroy", "vsg_scene_reset", "vsg_scene_params",
-    "vsg_integrate", "vsg_integrate_noalloc", "vsg_scene_stats", "vsg_scene_export", "vsg_renderer_create", "vsg_renderer_destroy",
+    "vsg_integrate", "vsg_integrate_noalloc", "vsg_scene_set_alloc_method", "vsg_scene_stats", "vsg_scene_export", "vsg_renderer_create", "vsg_renderer_destroy",
     "vsg_render", "vsg_render_hostpose", "vsg_renderer_outputs", "vsg_renderer_download",
+    "vsg_renderer_save_ply",
     "vsg_timing_enable", "vsg_timing_read", "vsg_timing_reset", "vsg_version",
     "vsg_batch_create", "vsg_batch_destroy", "vsg_batch_step", "vsg_batch_autotune",
     "vsg_mc_output_create", "vsg_mc_output_destroy", "vsg_mc_run", "vsg_mc_triangle_count",
@@ -94,6 +96,7 @@ def lib() -> ctypes.CDLL:
         L.vsg_scene_params.argtypes = [_P, ctypes.POINTER(Params)]
         L.vsg_integrate.argtypes = [_P, _P, _P, _P, _I, _I, _F, _P, _F, _F, _F, _F, _P]
         L.vsg_integrate_noalloc.argtypes = [_P, _P, _P, _P, _I, _I, _F, _P, _F, _F, _F, _F, _P]
+        L.vsg_scene_set_alloc_method.argtypes = [_P, _I]
         L.vsg_scene_stats.argtypes = [_P, ctypes.POINTER(Stats)]
         L.vsg_scene_export.argtypes = [_P, _P, _P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
         L.vsg_renderer_create.argtypes = [_I, _I, ctypes.POINTER(_P)]
@@ -142,6 +145,7 @@ def lib() -> ctypes.CDLL:
         L.vsg_scene_lookup_blocks.argtypes = [_P, _P, ctypes.c_uint32, _P]
         L.vsg_render_backward.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, _P, _P, _P, _F,
                                           ctypes.POINTER(ctypes.c_uint32), _P]
+        L.vsg_renderer_save_ply.argtypes = [_P, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
         L.vsg_render_pose_normal_equations.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, _P, _F, _P,
                                                        ctypes.POINTER(ctypes.c_uint32), _P]
         L.vsg_render_normals.argtypes = [_P, _P, _P, _F, _F, _F, _F, _P, ctypes.POINTER(ctypes.c_uint32), _P]
@@ -309,6 +313,11 @@ class Scene:
 
     def reset(self, stream=None):
         check("vsg_scene_reset", self.L.vsg_scene_reset(self.h, _stream(stream)))
+
+    def set_alloc_method(self, method: int):
+        """1: camera-z band (Method 1, default); 2: camera and normal rays with
+        parent pixels (Method 2, VoxelScene.cu:768-912)."""
+        check("vsg_scene_set_alloc_method", self.L.vsg_scene_set_alloc_method(self.h, int(method)))
 
     def integrate(self, pointmap, rgb, normals, width, height, truncation, pose, fx, fy, cx, cy, stream=None):
         T = np.ascontiguousarray(np.asarray(pose, np.float32).reshape(16))
@@ -498,6 +507,13 @@ class Renderer:
 
         return torch.as_tensor(_DeviceArray(self.outputs()["depth"], (self.height, self.width), "<f4"),
                                device="cuda")
+
+    def save_ply(self, path: str) -> int:
+        """RayCastRender::savePointCloudPLY: ASCII PLY of the last render's
+        hits with 8-bit colour; returns the number of points written."""
+        n = ctypes.c_int64()
+        check("vsg_renderer_save_ply", self.L.vsg_renderer_save_ply(self.h, str(path).encode(), ctypes.byref(n)))
+        return int(n.value)
 
     def outputs(self) -> dict:
         ps = [_P() for _ in range(4)]

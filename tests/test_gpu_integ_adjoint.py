@@ -18,8 +18,10 @@ def _ctz(x):
     return np.clip(np.trunc(x), -2147483648.0, 2147483647.0).astype(np.int64)
 
 
-def _retrace(coords, T, pm, K):
-    """Float32 retrace of the forward's per-voxel projection and tests.
+def _retrace(coords, T, pm, K, parents=None):
+    """Float32 retrace of the forward's per-voxel projection and tests; a
+    block with a parent tag (normal-direction allocation) whose pixel is in
+    the image and holds a point uses that pixel for all its voxels.
     Returns per voxel (n, 512): updated mask, pixel index, negative flag and
     the float32 voxel centre."""
     f32 = np.float32
@@ -41,6 +43,14 @@ def _retrace(coords, T, pm, K):
     ix, iy = _ctz(sx + f32(0.5)), _ctz(sy + f32(0.5))
     inb = (ix >= 0) & (ix < K.width) & (iy >= 0) & (iy < K.height)
     pix = np.where(inb, iy * K.width + ix, 0)
+    if parents is not None:
+        px = (parents & 0xFFFF).astype(np.int64)
+        py = ((parents >> 16) & 0xFFFF).astype(np.int64)
+        pp = np.where((parents != 0) & (px < K.width) & (py < K.height), py * K.width + px, -1)
+        flat = pm.reshape(-1, 3)
+        pp = np.where((pp >= 0) & np.any(flat[np.maximum(pp, 0)] != 0, -1), pp, -1)
+        inb = np.where(pp[:, None] >= 0, True, inb)
+        pix = np.where(pp[:, None] >= 0, pp[:, None], pix)
     p = pm.reshape(-1, 3)[pix]
     valid = inb & np.any(p != 0, -1)
     P = [((T[4 * r] * p[..., 0] + T[4 * r + 1] * p[..., 1]) + T[4 * r + 2] * p[..., 2]) + T[4 * r + 3] for r in range(3)]
@@ -55,19 +65,29 @@ def _retrace(coords, T, pm, K):
     return upd, pix, neg, np.stack([wx, wy, wz], -1).astype(np.float64)
 
 
-def test_integration_gradient_matches_central_differences(cuda, synth_mod):
+@pytest.mark.parametrize("alloc_method", [1, 2])
+def test_integration_gradient_matches_central_differences(cuda, synth_mod, oracle_mod, alloc_method):
     import vsg
 
     fr, K = synth_mod.tabletop_stream(8, 4, 160, 120)
     sc = vsg.Scene(voxel_size=VOXEL, truncation=TRUNC, hash_num_slots=20011, num_sdf_blocks=40000)
+    sc.set_alloc_method(alloc_method)
+    orc = oracle_mod.OracleScene(VOXEL)  # lock-step oracle: the blocks' parent pixels
+    orc.set_alloc_method(alloc_method)
     for f in fr[:3]:
         pm, rgb, nm = (cuda.from_numpy(x).cuda() for x in (f.pointmap, f.rgb, f.normals))
         sc.integrate(pm, rgb, nm, K.width, K.height, TRUNC, f.pose, K.fx, K.fy, K.cx, K.cy)
+        orc.integrate(f.pointmap, f.rgb, TRUNC, f.pose, K.fx, K.fy, K.cx, K.cy, normals=f.normals)
     c0, v0 = sc.export()
     f = fr[3]
     pm, rgb, nm = (cuda.from_numpy(x).cuda() for x in (f.pointmap, f.rgb, f.normals))
     sc.integrate(pm, rgb, nm, K.width, K.height, TRUNC, f.pose, K.fx, K.fy, K.cx, K.cy)
+    orc.integrate(f.pointmap, f.rgb, TRUNC, f.pose, K.fx, K.fy, K.cx, K.cy, normals=f.normals)
     c1, v1 = sc.export()
+    oc, _ = orc.export(with_voxels=False)
+    assert np.array_equal(oc, c1)
+    parents = orc.export_parents()
+    assert (parents != 0).any() == (alloc_method == 2)
     # volume before the frame on the block set after it (new blocks start empty)
     before = {tuple(c): i for i, c in enumerate(c0.tolist())}
     old = np.zeros((len(c1), 512, 8), np.uint8)
@@ -80,7 +100,7 @@ def test_integration_gradient_matches_central_differences(cuda, synth_mod):
     new_w = v1.reshape(-1, 512, 8)[..., 7].astype(np.float64)
     new_sdf = np.ascontiguousarray(v1.reshape(-1, 512, 8)[..., :4]).view(np.float32)[..., 0]
 
-    upd, pix, neg, w = _retrace(c1, f.pose, f.pointmap, K)
+    upd, pix, neg, w = _retrace(c1, f.pose, f.pointmap, K, parents)
     # the retrace reproduces the forward's decisions exactly
     assert np.array_equal(new_w != old_w, upd)
     assert np.all(new_w[upd] == np.minimum(255, old_w[upd] + 1))

@@ -24,17 +24,20 @@ def _upload(torch, f):
 
 
 def _run_stream(torch, oracle_mod, frames, K, trunc=0.02, voxel=0.004, slots=200000, blocks=200000,
-                render_every=1, check_every=1, min_d=0.2, max_d=3.0, **scene_kw):
+                render_every=1, check_every=1, min_d=0.2, max_d=3.0, alloc_method=1, **scene_kw):
     import vsg
 
     sc = vsg.Scene(voxel_size=voxel, hash_num_slots=slots, num_sdf_blocks=blocks, truncation=trunc, **scene_kw)
     rr = vsg.Renderer(K.width, K.height)
     orc = oracle_mod.OracleScene(voxel)
+    if alloc_method != 1:
+        sc.set_alloc_method(alloc_method)
+        orc.set_alloc_method(alloc_method)
     reports = []
     for i, f in enumerate(frames):
         pm, rgb, nm = _upload(torch, f)
         sc.integrate(pm, rgb, nm, K.width, K.height, trunc, f.pose, K.fx, K.fy, K.cx, K.cy)
-        ost = orc.integrate(f.pointmap, f.rgb, trunc, f.pose, K.fx, K.fy, K.cx, K.cy)
+        ost = orc.integrate(f.pointmap, f.rgb, trunc, f.pose, K.fx, K.fy, K.cx, K.cy, normals=f.normals)
         rep = {"frame": i, "oracle": ost}
         if i % check_every == 0 or i == len(frames) - 1:
             gc, gv = sc.export()
@@ -160,3 +163,57 @@ def test_room_1280x720_2mm(cuda, oracle_mod, synth_mod):
     want = {k: o[k][rows[0]:rows[1]] for k in ("depth", "position", "color", "normal")}
     r = compare_renders(band, want, DEPTH_TOL)
     assert r["bit_exact_all"] and r["hits_gpu"] > 0.5 * r["pixels"], r
+
+
+@pytest.mark.parametrize("wh,frames,slots", [((160, 120), 6, 200000), ((320, 240), 3, 200000),
+                                             ((160, 120), 4, 257)])
+def test_normal_direction_allocation(cuda, oracle_mod, synth_mod, wh, frames, slots):
+    """Method 2 (allocBlocksFromDepthMapMethod2Kernel, VoxelScene.cu:768-912,
+    and the parent-pixel integration branch, :1015-1035): volumes bit-exact
+    against the oracle frame by frame, renders within tolerance."""
+    fr, K = synth_mod.tabletop_stream(2, frames, wh[0], wh[1])
+    reports = _run_stream(cuda, oracle_mod, fr, K, alloc_method=2, slots=slots)
+    _assert_reports(reports)
+    assert all(r["volume"]["bit_exact"] for r in reports if "volume" in r)
+    # the mode allocates a different block set than the camera-z band
+    one = _run_stream(cuda, oracle_mod, fr[:1], K, slots=slots)
+    assert one[0]["oracle"]["blocks"] != reports[0]["oracle"]["blocks"]
+
+
+def test_normal_direction_allocation_mixed_resolutions(cuda, oracle_mod, synth_mod):
+    """Parents recorded at one resolution and checked against the next
+    frame's image bounds (VoxelScene.cu:1019-1021): alternating 320x240 and
+    160x120 frames of one scene, volumes bit-exact against the oracle."""
+    import vsg
+
+    big, Kb = synth_mod.tabletop_stream(4, 4, 320, 240)
+    small, Ks = synth_mod.tabletop_stream(4, 4, 160, 120)
+    sc = vsg.Scene(voxel_size=0.004, hash_num_slots=200000, num_sdf_blocks=200000, truncation=0.02)
+    sc.set_alloc_method(2)
+    orc = oracle_mod.OracleScene(0.004)
+    orc.set_alloc_method(2)
+    for i in range(4):
+        f, K = (big[i], Kb) if i % 2 == 0 else (small[i], Ks)
+        pm, rgb, nm = _upload(cuda, f)
+        sc.integrate(pm, rgb, nm, K.width, K.height, 0.02, f.pose, K.fx, K.fy, K.cx, K.cy)
+        orc.integrate(f.pointmap, f.rgb, 0.02, f.pose, K.fx, K.fy, K.cx, K.cy, normals=f.normals)
+        gc, gv = sc.export()
+        oc, ov = orc.export()
+        v = compare_volumes(gc, gv, oc, ov["raw"])
+        assert v["same_blocks"] and v["bit_exact"], (i, v)
+        assert sc.stats()["flags"] == 0
+    sc.close()
+
+
+def test_normal_direction_allocation_refused_where_unsupported(cuda, synth_mod):
+    import vsg
+
+    fr, K = synth_mod.tabletop_stream(0, 1, 64, 48)
+    sc = vsg.Scene(voxel_size=0.004, hash_num_slots=20011, num_sdf_blocks=20000, truncation=0.02)
+    sc.set_alloc_method(2)
+    pm, rgb, nm = _upload(cuda, fr[0])
+    with pytest.raises(vsg.VsgError):
+        sc.integrate_noalloc(pm, rgb, nm, K.width, K.height, 0.02, fr[0].pose, K.fx, K.fy, K.cx, K.cy)
+    with pytest.raises(vsg.VsgError):
+        sc.set_alloc_method(3)
+    sc.close()

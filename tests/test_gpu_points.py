@@ -77,3 +77,46 @@ def test_points_capacity_empty_and_ply(cuda, synth_mod, oracle_mod, tmp_path):
     assert lines[0] == "ply" and "element vertex 100" in lines and lines.index("end_header") == 13
     body = np.array([[float(x) for x in ln.split()] for ln in lines[14:]])
     assert body.shape == (100, 9) and np.all((body[:, 6:] >= 0) & (body[:, 6:] <= 255))
+
+
+def test_raycast_point_cloud_ply(cuda, synth_mod, tmp_path):
+    """vsg_renderer_save_ply (RayCastRender::savePointCloudPLY,
+    RayCastRender.cpp:221-302) writes exactly the reference's text for the
+    render's outputs: hits with depth in (0, 1e9) and finite positions, "%g"
+    coordinates, colour clamped and rounded to 0..255; no file when nothing
+    was hit."""
+    import vsg
+
+    fr, K = synth_mod.tabletop_stream(1, 3, 160, 120)
+    sc = _scene(vsg, cuda, synth_mod, 1, 160, 120, 3)
+    rr = vsg.Renderer(160, 120)
+    rr.render(sc, fr[-1].pose, K.fx, K.fy, K.cx, K.cy, 0.2, 3.0)
+    out = rr.download()
+    path = tmp_path / "sub" / "cloud.ply"
+    n = rr.save_ply(str(path))
+    D, P, C = out["depth"].ravel(), out["position"].reshape(-1, 4), out["color"].reshape(-1, 4)
+    ok = np.isfinite(D) & (D > 0) & (np.abs(D) < 1e9) & np.isfinite(P[:, :3]).all(1)
+    assert n == int(ok.sum()) > 1000
+
+    def ch(v):
+        if not np.isfinite(v):
+            return 255
+        return int(np.float32(min(max(v, np.float32(0)), np.float32(1))) * np.float32(255) + np.float32(0.5))
+
+    lines = ["ply", "format ascii 1.0", "comment Generated by RayCastRender", f"element vertex {n}",
+             "property float x", "property float y", "property float z", "property uchar red",
+             "property uchar green", "property uchar blue", "end_header"]
+    for i in np.nonzero(ok)[0]:
+        p, c = P[i], C[i]
+        lines.append("%g %g %g %d %d %d" % (p[0], p[1], p[2], ch(c[0]), ch(c[1]), ch(c[2])))
+    assert path.read_text() == "\n".join(lines) + "\n"
+    # a view that hits nothing writes no file
+    away = np.array(fr[-1].pose, np.float32)
+    away[:3, 3] += 100.0
+    rr.render(sc, away, K.fx, K.fy, K.cx, K.cy, 0.2, 3.0)
+    empty = tmp_path / "none.ply"
+    with pytest.raises(vsg.VsgError):
+        rr.save_ply(str(empty))
+    assert not empty.exists()
+    rr.close()
+    sc.close()
