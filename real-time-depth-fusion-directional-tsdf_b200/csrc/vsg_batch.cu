@@ -74,7 +74,7 @@ __global__ void k_batch_frame_begin(const BatchHeader* h, const IntegArgs* integ
 __global__ void __launch_bounds__(kTile* kTile) k_batch_alloc(const BatchHeader* h, const AllocArgs* args) {
     const int i = scene_of(h->alloc_prefix, h->n, blockIdx.x);
     const uint32_t t = blockIdx.x - h->alloc_prefix[i];
-    alloc_tile(args[i], (int)(t % (uint32_t)h->alloc_tiles_x[i]), (int)(t / (uint32_t)h->alloc_tiles_x[i]));
+    alloc_tile<false>(args[i], (int)(t % (uint32_t)h->alloc_tiles_x[i]), (int)(t / (uint32_t)h->alloc_tiles_x[i]));
 }
 
 __global__ void __launch_bounds__(256) k_batch_select(const BatchHeader* h, const IntegArgs* args) {

@@ -37,7 +37,10 @@ namespace vsg {
 // allocation
 // ====================================================================
 
-__global__ void __launch_bounds__(kTile* kTile) k_alloc(AllocArgs a) { alloc_tile(a, blockIdx.x, blockIdx.y); }
+template <bool kByNormal>
+__global__ void __launch_bounds__(kTile* kTile) k_alloc(AllocArgs a) {
+    alloc_tile<kByNormal>(a, blockIdx.x, blockIdx.y);
+}
 
 __global__ void __launch_bounds__(256) k_parents(SceneDev s) {
     apply_parents(s, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
@@ -215,8 +218,12 @@ int scene_integrate(Scene* sc, const float* pm, const uint8_t* rgb, const float*
     aa.pose = P;
     dim3 grid((W + kTile - 1) / kTile, (H + kTile - 1) / kTile);
     timing_begin(sc, kSlotAlloc, st);
-    k_alloc<<<grid, kTile * kTile, 0, st>>>(aa);
-    if (by_normal) k_parents<<<sc->sm_count * 2, 256, 0, st>>>(sc->dev);
+    if (by_normal) {
+        k_alloc<true><<<grid, kTile * kTile, 0, st>>>(aa);
+        k_parents<<<sc->sm_count * 2, 256, 0, st>>>(sc->dev);
+    } else {
+        k_alloc<false><<<grid, kTile * kTile, 0, st>>>(aa);
+    }
     timing_end(sc, kSlotAlloc, st);
     IntegArgs ia;
     ia.s = sc->dev;
@@ -263,7 +270,7 @@ int scene_integrate_with_pixels(Scene* sc, const float* pm, const uint8_t* rgb, 
     aa.trunc = trunc;
     aa.pose = P;
     dim3 grid((W + kTile - 1) / kTile, (H + kTile - 1) / kTile);
-    k_alloc<<<grid, kTile * kTile, 0, st>>>(aa);
+    k_alloc<false><<<grid, kTile * kTile, 0, st>>>(aa);
     IntegArgs ia;
     ia.s = dev;
     ia.W = W;

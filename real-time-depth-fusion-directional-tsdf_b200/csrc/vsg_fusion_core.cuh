@@ -312,6 +312,9 @@ static __device__ void dda_ray(const SceneDev& s, unsigned long long* set, uint3
 }
 
 // One 16x16 pixel tile (tile_x, tile_y) per CTA of kTile*kTile threads.
+// kByNormal: Method 2 rays (the scene's alloc_method == 2), else Method 1;
+// separate instantiations keep Method 1's register budget as it was.
+template <bool kByNormal>
 static __device__ __forceinline__ void alloc_tile(const AllocArgs& a, int tile_x, int tile_y) {
     __shared__ unsigned long long set[kSetCap];
     __shared__ unsigned long long list[kSetCap];
@@ -320,7 +323,7 @@ static __device__ __forceinline__ void alloc_tile(const AllocArgs& a, int tile_x
     __shared__ uint32_t s_zmin, s_zmax, s_nonfinite, s_valid;
     const int tid = threadIdx.x;
     const SceneDev& s = a.s;
-    const bool by_normal = s.alloc_method == 2;
+    constexpr bool by_normal = kByNormal;
     for (int i = tid; i < kSetCap; i += blockDim.x) {
         set[i] = kKeyEmpty;
         if (by_normal) set_tag[i] = 0u;
@@ -360,7 +363,7 @@ static __device__ __forceinline__ void alloc_tile(const AllocArgs& a, int tile_x
         s.pix_rgb[pi] = (uint32_t)__ldg(a.rgb + 3 * pi) | ((uint32_t)__ldg(a.rgb + 3 * pi + 1) << 8) |
                         ((uint32_t)__ldg(a.rgb + 3 * pi + 2) << 16);
         const float cx = a.pose.T[3], cy = a.pose.T[7], cz = a.pose.T[11];
-        if (!by_normal) {
+        if constexpr (!by_normal) {
             // allocBlocksFromDepthMapMethod1Kernel, VoxelScene.cu:547-633:
             // the camera-space segment p.z -+ truncation
             if (!(p2 <= 1e-6f)) {
