@@ -184,6 +184,32 @@ VSG_API int vsg_scene_set_alloc_method(vsg_scene* s, int method);
  * cross product of the right and lower neighbours' offsets, interior pixels
  * with d > 0, else (0,0,0).  depth: device float[w*h]; pointmap, normals:
  * device float3[w*h].  Stream-ordered. */
+/* Point cloud -> depth / point / normal / colour maps on the GPU
+ * (CustomDepthMapGenerator::generateFromPointCloud,
+ * CustomDepthMapGenerator.cpp:81-222, perspective projection :550-556).
+ * A point with z > 0 and min_depth <= z <= max_depth projects to
+ * u = x fx / z + cx, v = y fy / z + cy; inside [0, w) x [0, h) it lands on
+ * pixel (floor u, floor v).  mode VSG_SPLAT_LAST: the reference's order --
+ * the last point in input order wins the pixel, whose normal and colour are
+ * those of the last point landing there that has one (index < n_normals,
+ * index < n_colors); VSG_SPLAT_NEAREST: the nearest point wins (the later
+ * one on equal z) with its own normal and colour (zeros when it has none),
+ * the z-buffer of CUDADepthMapData.cu:9-53 without its race.  Pixels
+ * without a point hold 0.  With n_normals == 0 the normal map is the
+ * generator's fallback over the depth map (:163-209).  Pass min_depth 0 and
+ * max_depth INFINITY for the reference's generator, which has no range.
+ * points, normals: device float3; colors: device uchar3; outputs (device,
+ * each may be NULL): depth float[w*h], pointmap and normalmap float3[w*h],
+ * colormap uchar3[w*h].  n_points < 2^32 - 1 (else VSG_ERR_TOO_LARGE).
+ * *n_valid (host, may be NULL) receives the pixels that got a point and
+ * then the call synchronises; otherwise stream-ordered.  A work buffer of
+ * 20 bytes per pixel comes from the stream-ordered allocator. */
+enum { VSG_SPLAT_LAST = 0, VSG_SPLAT_NEAREST = 1 };
+VSG_API int vsg_splat_points(const float* points, int64_t n_points, const float* normals, int64_t n_normals,
+                             const uint8_t* colors, int64_t n_colors, int w, int h, float fx, float fy, float cx,
+                             float cy, float min_depth, float max_depth, int mode, float* depth, float* pointmap,
+                             float* normalmap, uint8_t* colormap, int64_t* n_valid, vsg_stream_t stream);
+
 VSG_API int vsg_depth_to_pointmap(const float* depth, int w, int h, float fx, float fy, float cx, float cy,
                                   float* pointmap, float* normals, vsg_stream_t stream);
 

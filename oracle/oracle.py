@@ -55,6 +55,8 @@ def lib():
         L.orc_integrate_nm.argtypes = [_p, _p, _p, _p, _i, _i, _f, _p, _f, _f, _f, _f, _p]
         L.orc_set_alloc_method.argtypes = [_p, _i]
         L.orc_export_parents.argtypes = [_p, _p]
+        L.orc_splat_points.argtypes = [_p, _i64, _p, _i64, _p, _i64, _i, _i, _f, _f, _f, _f, _f, _f, _i, _p, _p,
+                                       _p, _p]
         L.orc_render.argtypes = [_p, _i, _i, _p, _p, _f, _f, _f, _f, _f, _f, _p, _p, _p, _p, _p]
         L.orc_render_rows.argtypes = [_p, _i, _i, _i, _i, _p, _p, _f, _f, _f, _f, _f, _f, _p, _p, _p,
                                       _p, _p]
@@ -321,3 +323,23 @@ def set_threads(n: int):
 
 def max_threads() -> int:
     return int(lib().orc_max_threads())
+
+
+def splat_points(points, width, height, fx, fy, cx, cy, normals=None, colors=None, mode=0, min_depth=0.0,
+                 max_depth=float("inf")) -> dict:
+    """CustomDepthMapGenerator::generateFromPointCloud restated on the CPU
+    (orc_splat_points): depth (H,W), pointmap / normalmap (H,W,3), colormap
+    (H,W,3) uint8."""
+    L = lib()
+    pts = _f32(points).reshape(-1, 3)
+    nrm = _f32(normals).reshape(-1, 3) if normals is not None else None
+    col = np.ascontiguousarray(colors, dtype=np.uint8).reshape(-1, 3) if colors is not None else None
+    depth = np.zeros((height, width), np.float32)
+    pm = np.zeros((height, width, 3), np.float32)
+    nm = np.zeros((height, width, 3), np.float32)
+    cm = np.zeros((height, width, 3), np.uint8)
+    L.orc_splat_points(_ptr(pts), len(pts), _ptr(nrm) if nrm is not None else None,
+                       len(nrm) if nrm is not None else 0, _ptr(col) if col is not None else None,
+                       len(col) if col is not None else 0, int(width), int(height), _f(fx), _f(fy), _f(cx), _f(cy),
+                       _f(min_depth), _f(max_depth), int(mode), _ptr(depth), _ptr(pm), _ptr(nm), _ptr(cm))
+    return {"depth": depth, "pointmap": pm, "normalmap": nm, "colormap": cm}

@@ -1092,6 +1092,76 @@ void orc_render_brackets(const orc_scene* s, int W, int H, const float* cam, con
     }
 }
 
+/* ------------------------------------------------------ point-cloud splat */
+
+/* CustomDepthMapGenerator::generateFromPointCloud (CustomDepthMapGenerator.
+ * cpp:81-222): sequential loop over the points (mode 0: every accepted point
+ * overwrites its pixel, its normal / colour only when it has one); mode 1
+ * keeps the nearest point (the later one on equal z) with its own normal and
+ * colour.  Normals from the depth map when n_nrm == 0 (:163-209).  Outputs
+ * are zero-initialised here; any may be NULL except depth. */
+void orc_splat_points(const float* pts, int64_t n, const float* nrm, int64_t n_nrm, const uint8_t* col,
+                      int64_t n_col, int W, int H, float fx, float fy, float cx, float cy, float zmin, float zmax,
+                      int mode, float* depth, float* pm, float* nm, uint8_t* cm) {
+    const int64_t npx = (int64_t)W * H;
+    int64_t* win = (int64_t*)malloc(sizeof(int64_t) * (npx ? npx : 1));
+    for (int64_t p = 0; p < npx; p++) win[p] = -1;
+    memset(depth, 0, sizeof(float) * npx);
+    if (pm) memset(pm, 0, sizeof(float) * 3 * npx);
+    if (nm) memset(nm, 0, sizeof(float) * 3 * npx);
+    if (cm) memset(cm, 0, 3 * npx);
+    for (int64_t i = 0; i < n; i++) {
+        const float x = pts[3 * i], y = pts[3 * i + 1], z = pts[3 * i + 2];
+        if (z <= 0.0f) continue; /* :114 */
+        if (z < zmin || z > zmax) continue;
+        const float u = (x * fx / z) + cx; /* :553-556 */
+        const float v = (y * fy / z) + cy;
+        if (!(u >= 0.0f && u < (float)W && v >= 0.0f && v < (float)H)) continue; /* :586-587 */
+        const int px = (int)floorf(u), py = (int)floorf(v);
+        if (px < 0 || py < 0 || px >= W || py >= H) continue; /* :142 */
+        const int64_t p = (int64_t)py * W + px;
+        if (mode == 1 && win[p] >= 0 && pts[3 * win[p] + 2] < z) continue;
+        win[p] = i;
+        depth[p] = z;
+        if (pm) {
+            pm[3 * p] = x;
+            pm[3 * p + 1] = y;
+            pm[3 * p + 2] = z;
+        }
+        if (nm) {
+            if (i < n_nrm) memcpy(nm + 3 * p, nrm + 3 * i, 12);
+            else if (mode == 1) memset(nm + 3 * p, 0, 12);
+        }
+        if (cm) {
+            if (i < n_col) memcpy(cm + 3 * p, col + 3 * i, 3);
+            else if (mode == 1) memset(cm + 3 * p, 0, 3);
+        }
+    }
+    if (nm && n_nrm == 0) {
+        for (int y = 1; y < H - 1; y++)
+            for (int x = 1; x < W - 1; x++) {
+                const int64_t i = (int64_t)y * W + x;
+                const float d = depth[i];
+                if (!(d > 0.0f)) continue;
+                const float dr = depth[i + 1], dd = depth[i + W];
+                const float c[3] = {((float)x - cx) * d / fx, ((float)y - cy) * d / fy, d};
+                const float r[3] = {((float)(x + 1) - cx) * dr / fx, ((float)y - cy) * dr / fy, dr};
+                const float w[3] = {((float)x - cx) * dd / fx, ((float)(y + 1) - cy) * dd / fy, dd};
+                const float a0 = r[0] - c[0], a1 = r[1] - c[1], a2 = r[2] - c[2];
+                const float b0 = w[0] - c[0], b1 = w[1] - c[1], b2 = w[2] - c[2];
+                const float n0 = a1 * b2 - a2 * b1, n1 = a2 * b0 - a0 * b2, n2 = a0 * b1 - a1 * b0;
+                const float len = sqrtf(n0 * n0 + n1 * n1 + n2 * n2);
+                if (len > 0.0f) {
+                    const float inv = 1.0f / len;
+                    nm[3 * i] = n0 * inv;
+                    nm[3 * i + 1] = n1 * inv;
+                    nm[3 * i + 2] = n2 * inv;
+                }
+            }
+    }
+    free(win);
+}
+
 /* ------------------------------------------------------- export / import */
 
 static int cmp_key3(const void* a, const void* b) {

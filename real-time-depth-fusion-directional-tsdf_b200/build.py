@@ -24,7 +24,7 @@ OBJ_DIR = os.path.join(HERE, "_build")
 
 SOURCES = ["vsg_fusion.cu", "vsg_raycast.cu", "vsg_capi.cu", "vsg_noalloc.cu", "vsg_batch.cu", "vsg_mc.cu",
            "vsg_stream.cu", "vsg_points.cu",
-           "vsg_adjoint.cu", "vsg_depthmap.cu", "vsg_integ_adjoint.cu"]
+           "vsg_adjoint.cu", "vsg_depthmap.cu", "vsg_integ_adjoint.cu", "vsg_splat.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",

@@ -15,12 +15,11 @@
 #include <cuda_runtime.h>
 
 #include "../../include/vsg.h"
+#include "vsg_normals.cuh"
 
 namespace {
 
-__device__ __forceinline__ float3 backproject(float x, float y, float d, float fx, float fy, float cx, float cy) {
-    return make_float3((x - cx) * d / fx, (y - cy) * d / fy, d);
-}
+using vsg::backproject;
 
 __global__ void k_depth_to_maps(const float* __restrict__ depth, int W, int H, float fx, float fy, float cx,
                                 float cy, float* __restrict__ pm, float* __restrict__ nm) {
@@ -35,21 +34,7 @@ __global__ void k_depth_to_maps(const float* __restrict__ depth, int W, int H, f
     pm[3 * i + 1] = p.y;
     pm[3 * i + 2] = p.z;
     if (!nm) return;
-    float3 n = make_float3(0.0f, 0.0f, 0.0f);
-    if (x >= 1 && x < W - 1 && y >= 1 && y < H - 1 && d > 0.0f) {
-        const float dr = depth[i + 1], dd = depth[i + W];
-        const float3 c = backproject((float)x, (float)y, d, fx, fy, cx, cy);
-        const float3 r = backproject((float)(x + 1), (float)y, dr, fx, fy, cx, cy);
-        const float3 w = backproject((float)x, (float)(y + 1), dd, fx, fy, cx, cy);
-        const float ax = r.x - c.x, ay = r.y - c.y, az = r.z - c.z;
-        const float bx = w.x - c.x, by = w.y - c.y, bz = w.z - c.z;
-        const float3 cr = make_float3(ay * bz - az * by, az * bx - ax * bz, ax * by - ay * bx);
-        const float len = sqrtf(cr.x * cr.x + cr.y * cr.y + cr.z * cr.z);
-        if (len > 0.0f) {
-            const float inv = 1.0f / len;
-            n = make_float3(cr.x * inv, cr.y * inv, cr.z * inv);
-        }
-    }
+    const float3 n = vsg::depth_normal(depth, W, H, x, y, fx, fy, cx, cy);
     nm[3 * i + 0] = n.x;
     nm[3 * i + 1] = n.y;
     nm[3 * i + 2] = n.z;

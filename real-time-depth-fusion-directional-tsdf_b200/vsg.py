@@ -36,7 +36,7 @@ EXPORTS = [
     "vsg_points_create", "vsg_points_destroy", "vsg_extract_points", "vsg_points_count", "vsg_points_buffers",
     "vsg_points_download", "vsg_points_save_ply",
     "vsg_renderer_record", "vsg_render_backward", "vsg_render_normals", "vsg_scene_lookup_blocks",
-    "vsg_depth_to_pointmap", "vsg_integrate_backward", "vsg_render_pose_normal_equations",
+    "vsg_depth_to_pointmap", "vsg_integrate_backward", "vsg_render_pose_normal_equations", "vsg_splat_points",
 ]
 
 
@@ -139,6 +139,9 @@ def lib() -> ctypes.CDLL:
         L.vsg_points_download.argtypes = [_P, _P, _P, _P, ctypes.POINTER(ctypes.c_int64)]
         L.vsg_points_save_ply.argtypes = [_P, ctypes.c_char_p]
         L.vsg_renderer_record.argtypes = [_P, _I]
+        _i64 = ctypes.c_int64
+        L.vsg_splat_points.argtypes = [_P, _i64, _P, _i64, _P, _i64, _I, _I, _F, _F, _F, _F, _F, _F, _I, _P, _P, _P,
+                                       _P, ctypes.POINTER(_i64), _P]
         L.vsg_depth_to_pointmap.argtypes = [_P, _I, _I, _F, _F, _F, _F, _P, _P, _P]
         L.vsg_integrate_backward.argtypes = [_P, _P, _I, _I, _F, _P, _F, _F, _F, _F, _P, _P, _P,
                                              ctypes.POINTER(ctypes.c_uint32), _P]
@@ -238,6 +241,35 @@ def render_depth(scene, renderer, pose, fx, fy, cx, cy, min_depth, max_depth, mi
             return out.to(device=ctx.dev, dtype=ctx.dtype)
 
     return _Render.apply(pose)
+
+
+SPLAT_LAST, SPLAT_NEAREST = 0, 1
+
+
+def splat_points(points, width, height, fx, fy, cx, cy, normals=None, colors=None, mode: int = SPLAT_LAST,
+                 min_depth: float = 0.0, max_depth: float = float("inf"), stream=None) -> dict:
+    """CustomDepthMapGenerator::generateFromPointCloud on the GPU
+    (vsg_splat_points): points (N,3) float32, normals (M,3) float32 and
+    colors (K,3) uint8 device tensors (M, K may be shorter than N or None).
+    Returns device tensors depth (H,W), pointmap and normalmap (H,W,3),
+    colormap (H,W,3) uint8, and the number of pixels that got a point."""
+    import torch
+
+    dev = torch.device("cuda")
+    depth = torch.empty((height, width), dtype=torch.float32, device=dev)
+    pm = torch.empty((height, width, 3), dtype=torch.float32, device=dev)
+    nm = torch.empty((height, width, 3), dtype=torch.float32, device=dev)
+    cm = torch.empty((height, width, 3), dtype=torch.uint8, device=dev)
+    n_valid = ctypes.c_int64()
+    pts = points.contiguous()
+    nrm = normals.contiguous() if normals is not None else None
+    col = colors.contiguous() if colors is not None else None
+    check("vsg_splat_points", lib().vsg_splat_points(
+        _dptr(pts), int(pts.shape[0]), _dptr(nrm), int(nrm.shape[0]) if nrm is not None else 0, _dptr(col),
+        int(col.shape[0]) if col is not None else 0, int(width), int(height), _F(fx), _F(fy), _F(cx), _F(cy),
+        _F(min_depth), _F(max_depth), int(mode), _dptr(depth), _dptr(pm), _dptr(nm), _dptr(cm),
+        ctypes.byref(n_valid), _stream(stream)))
+    return {"depth": depth, "pointmap": pm, "normalmap": nm, "colormap": cm, "n_valid": int(n_valid.value)}
 
 
 def se3_exp(xi) -> np.ndarray:
