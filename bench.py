@@ -278,6 +278,7 @@ def run_ours(args):
     line["surface_points"] = points_measure(sc, peak)
     line["streaming"] = stream_measure(sc)
     line["adjoint"] = adjoint_measure(sc, frames, K)
+    line["splat"] = splat_measure(frames, K, peak)
     if not args.no_e2e:
         line["e2e"] = e2e(args, frames, K, sc, rr)
     if not args.no_batched:
@@ -317,6 +318,51 @@ def mc_measure(sc, peak: float, reps: int = 10) -> dict:
     gbs = alg / (ms * 1e-3) / 1e9
     return {"triangles": n, "blocks_with_weight": weighted, "ms_per_launch": ms, "alg_bytes": alg,
             "achieved_gbs": gbs, "frac_of_peak": gbs / peak, "launches_timed": int(kcnt[4])}
+
+
+def splat_measure(frames, K, peak: float, reps: int = 10) -> dict:
+    """Point-cloud splat (vsg_splat_points, last-wins as the reference's
+    generator): the valid points of four stream frames seen from the first
+    frame's camera, with normals and colours, onto 640x480.  Device time per
+    call from CUDA events (the call's work buffer comes from the stream-
+    ordered pool).  Bytes = 27 per point read (point, normal, colour) + 31
+    per pixel written (depth, point, normal, colour) + the 16-byte per-pixel
+    winner words written and read once."""
+    import torch
+
+    import vsg
+
+    T0 = np.asarray(frames[0].pose, np.float64)
+    pts, nrm, col = [], [], []
+    for f in frames[:4]:
+        m = np.any(f.pointmap != 0, -1)
+        M = np.linalg.inv(T0) @ np.asarray(f.pose, np.float64)
+        pts.append((f.pointmap[m].astype(np.float64) @ M[:3, :3].T + M[:3, 3]).astype(np.float32))
+        nrm.append((f.normals[m].astype(np.float64) @ M[:3, :3].T).astype(np.float32))
+        col.append(f.rgb[m])
+    P, N, C = (torch.from_numpy(np.concatenate(x)).cuda() for x in (pts, nrm, col))
+    W, H = K.width, K.height
+    out = None
+    for _ in range(3):
+        out = vsg.splat_points(P, W, H, K.fx, K.fy, K.cx, K.cy, normals=N, colors=C)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    bufs = {k: out[k] for k in ("depth", "pointmap", "normalmap", "colormap")}
+    L = vsg.lib()
+    for _ in range(reps):
+        vsg.check("vsg_splat_points", L.vsg_splat_points(
+            P.data_ptr(), P.shape[0], N.data_ptr(), N.shape[0], C.data_ptr(), C.shape[0], W, H, K.fx, K.fy, K.cx,
+            K.cy, 0.0, float("inf"), vsg.SPLAT_LAST, bufs["depth"].data_ptr(), bufs["pointmap"].data_ptr(),
+            bufs["normalmap"].data_ptr(), bufs["colormap"].data_ptr(), None, None))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    n = int(P.shape[0])
+    alg = n * 27 + W * H * (31 + 16 * 2)
+    gbs = alg / (ms * 1e-3) / 1e9
+    return {"points": n, "pixels_hit": out["n_valid"], "ms_per_call": ms, "mpoints_per_s": n / ms / 1e3,
+            "alg_bytes": alg, "achieved_gbs": gbs, "frac_of_peak": gbs / peak}
 
 
 def points_measure(sc, peak: float, reps: int = 10) -> dict:
