@@ -245,6 +245,58 @@ def random_walk_poses(n: int, seed: int, step_m: float = 0.005, step_deg: float 
 ROOM_K = Intrinsics(1280, 720, 910.0, 910.0, 639.5, 359.5)
 
 
+def corridor_scene(seed: int, length: float = 10.0, n_prims: int = 300) -> Scene:
+    """length x 2.5 x 2.5 m corridor (x in [0, length], y in [0, 2.5], z in
+    [-1.25, 1.25]) viewed from inside, with n_prims boxes and spheres
+    (sides / radii 0.05-0.3 m) along the walls, |z| >= 0.45 so the centre
+    line stays clear."""
+    rng = np.random.default_rng(seed)
+    boxes, spheres = [], []
+    for i in range(n_prims):
+        side = 1.0 if rng.random() < 0.5 else -1.0
+        x = rng.uniform(0.2, length - 0.2)
+        y = rng.uniform(0.0, 2.3)
+        z = side * rng.uniform(0.75, 1.1)
+        if i % 2 == 0:
+            s = rng.uniform(0.05, 0.3, 3)
+            boxes.append((np.array([x, y, z]) - s / 2, np.array([x, y, z]) + s / 2))
+        else:
+            spheres.append((np.array([x, y, z]), rng.uniform(0.05, 0.3)))
+    return Scene(planes=[], spheres=spheres, boxes=boxes, room=((0.0, 0.0, -1.25), (length, 2.5, 1.25)))
+
+
+def corridor_poses(n: int, length: float = 10.0, margin: float = 0.8) -> list:
+    """Walk along the corridor's centre line and back at 1.25 m height: the
+    first half faces +x from x = margin to length - margin, the second half
+    returns facing -x; the gaze swings +-20 degrees sideways and +-5 degrees
+    vertically."""
+    poses = []
+    half = max(n // 2, 1)
+    for i in range(n):
+        back = i >= half
+        s = (i - half) / max(n - half - 1, 1) if back else i / max(half - 1, 1)
+        x = (length - margin) - s * (length - 2 * margin) if back else margin + s * (length - 2 * margin)
+        yaw = math.radians(20.0) * math.sin(2 * math.pi * i / 60.0)
+        pitch = math.radians(5.0) * math.sin(2 * math.pi * i / 45.0)
+        fwd = -1.0 if back else 1.0
+        eye = np.array([x, 1.25, 0.0])
+        d = np.array([fwd * math.cos(yaw), math.sin(pitch), math.sin(yaw)])
+        poses.append(look_at(eye, eye + d))
+    return poses
+
+
+def corridor_stream(seed: int = 3, frames: int = 2000, width: int = 640, height: int = 480,
+                    length: float = 10.0, n_prims: int = 300, frame_ids=None) -> tuple[list, Intrinsics]:
+    """Corridor workload: there-and-back walk (corridor_poses) through
+    corridor_scene, sensor range 0.2-4 m."""
+    scene = corridor_scene(seed, length, n_prims)
+    K = TABLETOP_K if (width, height) == (640, 480) else scaled_intrinsics(TABLETOP_K, width, height)
+    poses = corridor_poses(frames, length)
+    ids = range(frames) if frame_ids is None else frame_ids
+    return [render_frame(scene, K, poses[i], np.random.default_rng([seed, i]), zmin=0.2, zmax=4.0,
+                         color_top=2.5) for i in ids], K
+
+
 def room_stream(seed: int = 1, frames: int = 300, width: int = 1280, height: int = 720,
                 frame_ids=None) -> tuple[list, Intrinsics]:
     """Larger single stream: seeded room, random-walk trajectory."""
@@ -287,28 +339,41 @@ def render_frame_torch(scene: Scene, K: Intrinsics, pose: np.ndarray, seed: int 
         ok = (den < -1e-9) & (t > 0) & (t < tbest)
         tbest = torch.where(ok, t, tbest)
         nbest = torch.where(ok[:, None], nr.expand_as(nbest), nbest)
-    for (c, r) in scene.spheres:
-        ct = torch.as_tensor(np.asarray(c), dtype=dt, device=device)
-        oc = o - ct
-        b = dw @ oc
-        disc = b * b - (oc @ oc - r * r)
-        t = -b - torch.sqrt(torch.clamp(disc, min=0.0))
-        ok = (disc > 0) & (t > 0) & (t < tbest)
-        tbest = torch.where(ok, t, tbest)
-        hp = o + dw * t[:, None]
-        nbest = torch.where(ok[:, None], (hp - ct) / r, nbest)
-    for (lo, hi) in scene.boxes:
+    # spheres and boxes in batches of primitives (nearest hit; the first
+    # primitive on equal distances, as the sequential loop)
+    if scene.spheres:
+        C = torch.as_tensor(np.array([c for c, _ in scene.spheres], np.float64), dtype=dt, device=device)
+        Rr = torch.as_tensor(np.array([r for _, r in scene.spheres], np.float64), dtype=dt, device=device)
+        for k0 in range(0, C.shape[0], 64):
+            Ck, Rk = C[k0:k0 + 64], Rr[k0:k0 + 64]
+            oc = o[None, :] - Ck                                   # (P,3)
+            b = dw @ oc.T                                          # (N,P)
+            disc = b * b - ((oc * oc).sum(1) - Rk * Rk)[None, :]
+            t = -b - torch.sqrt(torch.clamp(disc, min=0.0))
+            t = torch.where((disc > 0) & (t > 0), t, torch.full_like(t, float("inf")))
+            tk, ik = t.min(dim=1)
+            ok = tk < tbest
+            tbest = torch.where(ok, tk, tbest)
+            hp = o + dw * tk[:, None]
+            nbest = torch.where(ok[:, None], (hp - Ck[ik]) / Rk[ik][:, None], nbest)
+    if scene.boxes:
+        LO = torch.as_tensor(np.array([lo for lo, _ in scene.boxes], np.float64), dtype=dt, device=device)
+        HI = torch.as_tensor(np.array([hi for _, hi in scene.boxes], np.float64), dtype=dt, device=device)
         inv = 1.0 / torch.where(dw.abs() < 1e-9, torch.full_like(dw, 1e-9), dw)
-        t0 = (torch.as_tensor(np.asarray(lo), dtype=dt, device=device) - o) * inv
-        t1 = (torch.as_tensor(np.asarray(hi), dtype=dt, device=device) - o) * inv
-        tmin, tmax = torch.minimum(t0, t1), torch.maximum(t0, t1)
-        tn, tf = tmin.max(dim=1).values, tmax.min(dim=1).values
-        ok = (tn <= tf) & (tn > 0) & (tn < tbest)
-        tbest = torch.where(ok, tn, tbest)
-        ax = tmin.argmax(dim=1)
-        nn = torch.zeros_like(nbest)
-        nn.scatter_(1, ax[:, None], -torch.sign(dw.gather(1, ax[:, None])))
-        nbest = torch.where(ok[:, None], nn, nbest)
+        for k0 in range(0, LO.shape[0], 16):
+            t0 = (LO[None, k0:k0 + 16] - o) * inv[:, None, :]    # (N,P,3)
+            t1 = (HI[None, k0:k0 + 16] - o) * inv[:, None, :]
+            tmin, tmax = torch.minimum(t0, t1), torch.maximum(t0, t1)
+            tn, tf = tmin.max(dim=2).values, tmax.min(dim=2).values
+            tn = torch.where((tn <= tf) & (tn > 0), tn, torch.full_like(tn, float("inf")))
+            tk, ik = tn.min(dim=1)
+            ok = tk < tbest
+            tbest = torch.where(ok, tk, tbest)
+            tm = tmin[torch.arange(tmin.shape[0], device=device), ik]   # (N,3) of the winning box
+            ax = tm.argmax(dim=1)
+            nn = torch.zeros_like(nbest)
+            nn.scatter_(1, ax[:, None], -torch.sign(dw.gather(1, ax[:, None])))
+            nbest = torch.where(ok[:, None], nn, nbest)
     if scene.room is not None:
         inv = 1.0 / torch.where(dw.abs() < 1e-9, torch.full_like(dw, 1e-9), dw)
         t0 = (torch.as_tensor(np.asarray(scene.room[0]), dtype=dt, device=device) - o) * inv
