@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-scans", type=int, default=64)
+    ap.add_argument("--no-corridor", action="store_true")
+    ap.add_argument("--corridor-frames", type=int, default=400)
     return ap.parse_args()
 
 
@@ -279,6 +281,8 @@ def run_ours(args):
     line["streaming"] = stream_measure(sc)
     line["adjoint"] = adjoint_measure(sc, frames, K)
     line["splat"] = splat_measure(frames, K, peak)
+    if not args.no_corridor:
+        line["corridor"] = corridor_measure(args.corridor_frames)
     if not args.no_e2e:
         line["e2e"] = e2e(args, frames, K, sc, rr)
     if not args.no_batched:
@@ -318,6 +322,81 @@ def mc_measure(sc, peak: float, reps: int = 10) -> dict:
     gbs = alg / (ms * 1e-3) / 1e9
     return {"triangles": n, "blocks_with_weight": weighted, "ms_per_launch": ms, "alg_bytes": alg,
             "achieved_gbs": gbs, "frac_of_peak": gbs / peak, "launches_timed": int(kcnt[4])}
+
+
+def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r_in: float = 3.0) -> dict:
+    """Corridor workload (10 x 2.5 x 2.5 m, 300 primitives, 640x480, 4 mm,
+    500 000 buckets / blocks): a there-and-back walk of n_frames, frames
+    generated on the device.  Pass 1, at the true poses, per frame: stream
+    out every block farther than r_out from a point 1.5 m ahead of the
+    camera, stream in the stored chunks (0.5 m) within r_in of it, integrate,
+    ray cast -- wall clock per frame (the streaming calls synchronise).
+    Pass 2 tracks instead: each frame's pose is estimated by track_steps
+    Gauss-Newton steps (vsg.refine_pose) of its depth against the model from
+    a constant-velocity prediction, then streamed and integrated at the
+    estimate; reported with the trajectory error against the true poses."""
+    import torch
+
+    import synth
+    import vsg
+
+    scene = synth.corridor_scene(3)
+    K = synth.TABLETOP_K
+    W, H = K.width, K.height
+    poses = synth.corridor_poses(n_frames)
+    frames = [synth.render_frame_torch(scene, K, P, seed=i, zmax=4.0, color_top=2.5) for i, P in enumerate(poses)]
+    torch.cuda.synchronize()
+
+    def run(track: bool):
+        sc = vsg.Scene(voxel_size=VOXEL, truncation=TRUNC, hash_num_slots=500000, num_sdf_blocks=500000)
+        rr = vsg.Renderer(W, H)
+        store = vsg.Store((0.5, 0.5, 0.5))
+        est = []
+        n_out = n_in = peak_res = 0
+        track_ms = 0.0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i, (pm, rgb, nm) in enumerate(frames):
+            T = poses[i].astype(np.float64)
+            if track and i >= 1:
+                pred = est[-1] @ (np.linalg.inv(est[-2]) @ est[-1]) if i >= 2 else est[-1]
+                target = torch.where(pm[..., 2] > 0, pm[..., 2], torch.full_like(pm[..., 2], 1e10))
+                t1 = time.perf_counter()
+                T, _ = vsg.refine_pose(sc, rr, target, pred, K.fx, K.fy, K.cx, K.cy, MIN_D, 4.0,
+                                       steps=track_steps)
+                track_ms += (time.perf_counter() - t1) * 1e3
+            est.append(T)
+            T32 = T.astype(np.float32)
+            c = (T32[:3, 3] + np.float32(1.5) * T32[:3, 2]).astype(np.float32)
+            n_out += sc.stream_out(store, c, r_out)
+            n_in += sc.stream_in(store, c, r_in)[0]
+            sc.integrate(pm, rgb, nm, W, H, TRUNC, T32, K.fx, K.fy, K.cx, K.cy)
+            rr.render(sc, T32, K.fx, K.fy, K.cx, K.cy, MIN_D, 4.0)
+            if i % 20 == 0:
+                peak_res = max(peak_res, sc.stats()["allocated_blocks"])
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        st = sc.stats()
+        out = {"frames_per_s_wall": n_frames / wall, "ms_per_frame_wall": wall * 1e3 / n_frames,
+               "blocks_streamed_out": n_out, "blocks_streamed_in": n_in,
+               "resident_blocks_peak": max(peak_res, st["allocated_blocks"]),
+               "stored_blocks_end": int(store.info()[0]), "flags": st["flags"]}
+        if track:
+            terr = [float(np.linalg.norm(e[:3, 3] - p[:3, 3])) for e, p in zip(est, poses)]
+            rerr = [float(np.degrees(np.arccos(np.clip((np.trace(e[:3, :3].T @ p[:3, :3]) - 1) / 2, -1, 1))))
+                    for e, p in zip(est, poses)]
+            out.update({"gn_steps_per_frame": track_steps, "track_ms_per_frame": track_ms / max(n_frames - 1, 1),
+                        "trans_err_mean_m": float(np.mean(terr)), "trans_err_max_m": float(np.max(terr)),
+                        "rot_err_mean_deg": float(np.mean(rerr)), "rot_err_max_deg": float(np.max(rerr))})
+        sc.close()
+        rr.close()
+        return out
+
+    res = {"frames": n_frames, "size": "640x480", "slots": 500000, "r_out_m": r_out, "r_in_m": r_in,
+           "chunk_m": 0.5, "fusion": run(False), "tracking": run(True)}
+    del frames
+    torch.cuda.empty_cache()
+    return res
 
 
 def splat_measure(frames, K, peak: float, reps: int = 10) -> dict:

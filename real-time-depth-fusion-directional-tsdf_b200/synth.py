@@ -266,21 +266,22 @@ def corridor_scene(seed: int, length: float = 10.0, n_prims: int = 300) -> Scene
 
 
 def corridor_poses(n: int, length: float = 10.0, margin: float = 0.8) -> list:
-    """Walk along the corridor's centre line and back at 1.25 m height: the
-    first half faces +x from x = margin to length - margin, the second half
-    returns facing -x; the gaze swings +-20 degrees sideways and +-5 degrees
+    """Walk along the corridor's centre line and back at 1.25 m height: x
+    follows margin + (length - 2 margin)(1 - cos 2 pi u)/2 over u in [0, 1]
+    (smooth, at rest at both ends and at the far end); the heading turns
+    from +x to -x between u = 0.4 and 0.6 (smoothstep) while the camera is
+    nearly at rest, and the gaze swings +-20 degrees sideways and +-5 degrees
     vertically."""
     poses = []
-    half = max(n // 2, 1)
     for i in range(n):
-        back = i >= half
-        s = (i - half) / max(n - half - 1, 1) if back else i / max(half - 1, 1)
-        x = (length - margin) - s * (length - 2 * margin) if back else margin + s * (length - 2 * margin)
-        yaw = math.radians(20.0) * math.sin(2 * math.pi * i / 60.0)
+        u = i / max(n - 1, 1)
+        x = margin + (length - 2 * margin) * (1.0 - math.cos(2 * math.pi * u)) / 2.0
+        w = min(max((u - 0.4) / 0.2, 0.0), 1.0)
+        heading = math.pi * w * w * (3.0 - 2.0 * w)
+        yaw = heading + math.radians(20.0) * math.sin(2 * math.pi * i / 60.0)
         pitch = math.radians(5.0) * math.sin(2 * math.pi * i / 45.0)
-        fwd = -1.0 if back else 1.0
         eye = np.array([x, 1.25, 0.0])
-        d = np.array([fwd * math.cos(yaw), math.sin(pitch), math.sin(yaw)])
+        d = np.array([math.cos(yaw) * math.cos(pitch), math.sin(pitch), math.sin(yaw) * math.cos(pitch)])
         poses.append(look_at(eye, eye + d))
     return poses
 
