@@ -333,8 +333,9 @@ def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r
     ray cast -- wall clock per frame (the streaming calls synchronise).
     Pass 2 tracks instead: each frame's pose is estimated by track_steps
     Gauss-Newton steps (vsg.refine_pose) of its depth against the model from
-    a constant-velocity prediction, then streamed and integrated at the
-    estimate; reported with the trajectory error against the true poses."""
+    a constant-velocity prediction (residuals within 2 m and at incidence
+    |cos| >= 0.5), then streamed and integrated at the estimate; reported
+    with the trajectory error against the true poses."""
     import torch
 
     import synth
@@ -362,8 +363,8 @@ def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r
                 pred = est[-1] @ (np.linalg.inv(est[-2]) @ est[-1]) if i >= 2 else est[-1]
                 target = torch.where(pm[..., 2] > 0, pm[..., 2], torch.full_like(pm[..., 2], 1e10))
                 t1 = time.perf_counter()
-                T, _ = vsg.refine_pose(sc, rr, target, pred, K.fx, K.fy, K.cx, K.cy, MIN_D, 4.0,
-                                       steps=track_steps)
+                T, _ = vsg.refine_pose(sc, rr, target, pred, K.fx, K.fy, K.cx, K.cy, MIN_D, 2.0,
+                                       steps=track_steps, min_incidence=0.5)
                 track_ms += (time.perf_counter() - t1) * 1e3
             est.append(T)
             T32 = T.astype(np.float32)

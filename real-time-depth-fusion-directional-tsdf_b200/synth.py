@@ -287,15 +287,16 @@ def corridor_poses(n: int, length: float = 10.0, margin: float = 0.8) -> list:
 
 
 def corridor_stream(seed: int = 3, frames: int = 2000, width: int = 640, height: int = 480,
-                    length: float = 10.0, n_prims: int = 300, frame_ids=None) -> tuple[list, Intrinsics]:
+                    length: float = 10.0, n_prims: int = 300, frame_ids=None,
+                    noise: bool = True) -> tuple[list, Intrinsics]:
     """Corridor workload: there-and-back walk (corridor_poses) through
     corridor_scene, sensor range 0.2-4 m."""
     scene = corridor_scene(seed, length, n_prims)
     K = TABLETOP_K if (width, height) == (640, 480) else scaled_intrinsics(TABLETOP_K, width, height)
     poses = corridor_poses(frames, length)
     ids = range(frames) if frame_ids is None else frame_ids
-    return [render_frame(scene, K, poses[i], np.random.default_rng([seed, i]), zmin=0.2, zmax=4.0,
-                         color_top=2.5) for i in ids], K
+    return [render_frame(scene, K, poses[i], np.random.default_rng([seed, i]) if noise else None, zmin=0.2,
+                         zmax=4.0, color_top=2.5) for i in ids], K
 
 
 def room_stream(seed: int = 1, frames: int = 300, width: int = 1280, height: int = 720,

@@ -290,27 +290,53 @@ def se3_exp(xi) -> np.ndarray:
     return out
 
 
+def _unit_rays(width, height, fx, fy, cx, cy):
+    """(H,W,3) unit camera-space ray directions on the device, float32."""
+    import torch
+
+    v, u = torch.meshgrid(torch.arange(height, device="cuda", dtype=torch.float32),
+                          torch.arange(width, device="cuda", dtype=torch.float32), indexing="ij")
+    cd = torch.stack([(u - cx) / fx, (v - cy) / fy, torch.ones_like(u)], -1)
+    return cd / cd.norm(dim=-1, keepdim=True)
+
+
 def refine_pose(scene, renderer, target_depth, pose, fx, fy, cx, cy, min_depth, max_depth, steps: int = 8,
-                huber: float = 0.01, damping: float = 1e-6, min_weight_sum: float = 0.5):
+                huber: float = 0.01, damping: float = 1e-6, min_weight_sum: float = 0.5,
+                max_residual=(0.2, 0.05), min_incidence: float = 0.0):
     """Gauss-Newton alignment of a camera pose to a target depth image (H,W
     device float32, misses >= 1e9) through the ray cast: each step renders at
     the current pose, forms residuals (rendered - target) on pixels hit in
     both with Huber weights (1 inside `huber` metres, huber/|r| outside),
     solves (H + damping diag(H)) xi = -b from
     vsg_render_pose_normal_equations and right-multiplies the pose by
-    exp(xi).  Returns (4x4 float64 pose, per-step weighted RMS residual)."""
+    exp(xi).  Outliers (disocclusions, silhouettes) are left out: pixels
+    whose |residual| exceeds a threshold shrinking geometrically from
+    max_residual[0] to max_residual[1] over the steps.  With
+    min_incidence > 0, pixels where the model's normal (vsg_render_normals)
+    meets the ray at |cos| < min_incidence are left out too: at grazing
+    incidence the depth is steep in the pose.  Returns (4x4 float64 pose,
+    per-step weighted RMS residual)."""
     import torch
 
     T = np.asarray(pose, np.float64).reshape(4, 4).copy()
     renderer.record(True)
+    rays = _unit_rays(renderer.width, renderer.height, fx, fy, cx, cy) if min_incidence > 0 else None
+    r0, r1 = (float(max_residual[0]), float(max_residual[1])) if max_residual is not None else (np.inf, np.inf)
     rms = []
-    for _ in range(steps):
+    for k in range(steps):
         T32 = T.astype(np.float32)
         renderer.render(scene, T32, fx, fy, cx, cy, min_depth, max_depth)
         d = renderer.depth_tensor()
         m = (d < 1e9) & (target_depth < 1e9)
+        if rays is not None:
+            n, _ = renderer.normals(scene, T32, fx, fy, cx, cy)
+            R = torch.as_tensor(T32[:3, :3], device="cuda")
+            cos = (n[..., :3] * (rays @ R.T)).sum(-1).abs()
+            m = m & (cos >= min_incidence)
         r = torch.where(m, d - target_depth, torch.zeros_like(d))
         a = r.abs()
+        tau = r0 * (r1 / r0) ** (k / max(steps - 1, 1)) if np.isfinite(r0) else np.inf
+        m = m & (a <= tau)
         w = torch.where(m, torch.where(a <= huber, torch.ones_like(a), huber / a.clamp_min(huber)),
                         torch.zeros_like(a))
         Hm, b, _ = renderer.pose_normal_equations(scene, T32, fx, fy, cx, cy, r, w, min_weight_sum)
