@@ -276,15 +276,23 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind},
             "clocks": clk.summary()}
-    line["marching_cubes"] = mc_measure(sc, peak)
-    line["surface_points"] = points_measure(sc, peak)
-    line["streaming"] = stream_measure(sc)
-    line["adjoint"] = adjoint_measure(sc, frames, K)
-    line["splat"] = splat_measure(frames, K, peak)
-    if not args.no_corridor:
-        line["corridor"] = corridor_measure(args.corridor_frames)
+    # side measurements after the timed step; a failure is recorded in the
+    # line instead of losing it
+    def side(name, fn, *a):
+        try:
+            line[name] = fn(*a)
+        except Exception as exc:  # noqa: BLE001
+            line[name] = {"error": f"{type(exc).__name__}: {exc}"}
+
+    side("marching_cubes", mc_measure, sc, peak)
+    side("surface_points", points_measure, sc, peak)
+    side("streaming", stream_measure, sc)
+    side("adjoint", adjoint_measure, sc, frames, K)
+    side("splat", splat_measure, frames, K, peak)
     if not args.no_e2e:
         line["e2e"] = e2e(args, frames, K, sc, rr)
+    if not args.no_corridor:
+        side("corridor", corridor_measure, args.corridor_frames)
     if not args.no_batched:
         line["batched"] = run_batched(args, dist)
     if not args.no_cpu and rank == 0:
@@ -326,7 +334,7 @@ def mc_measure(sc, peak: float, reps: int = 10) -> dict:
 
 def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r_in: float = 3.0) -> dict:
     """Corridor workload (10 x 2.5 x 2.5 m, 300 primitives, 640x480, 4 mm,
-    500 000 buckets / blocks): a there-and-back walk of n_frames, frames
+    500 000 buckets, 1 000 000 pool blocks): a there-and-back walk of n_frames, frames
     generated on the device.  Pass 1, at the true poses, per frame: stream
     out every block farther than r_out from a point 1.5 m ahead of the
     camera, stream in the stored chunks (0.5 m) within r_in of it, integrate,
@@ -349,7 +357,8 @@ def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r
     torch.cuda.synchronize()
 
     def run(track: bool):
-        sc = vsg.Scene(voxel_size=VOXEL, truncation=TRUNC, hash_num_slots=500000, num_sdf_blocks=500000)
+        sc = vsg.Scene(voxel_size=VOXEL, truncation=TRUNC, hash_num_slots=500000, num_sdf_blocks=1000000,
+                       max_chain_nodes=1000000)
         rr = vsg.Renderer(W, H)
         store = vsg.Store((0.5, 0.5, 0.5))
         est = []
@@ -393,7 +402,8 @@ def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r
         rr.close()
         return out
 
-    res = {"frames": n_frames, "size": "640x480", "slots": 500000, "r_out_m": r_out, "r_in_m": r_in,
+    res = {"frames": n_frames, "size": "640x480", "slots": 500000, "pool_blocks": 1000000, "r_out_m": r_out,
+           "r_in_m": r_in,
            "chunk_m": 0.5, "fusion": run(False), "tracking": run(True)}
     del frames
     torch.cuda.empty_cache()
