@@ -334,7 +334,7 @@ def mc_measure(sc, peak: float, reps: int = 10) -> dict:
 
 def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r_in: float = 3.0) -> dict:
     """Corridor workload (10 x 2.5 x 2.5 m, 300 primitives, 640x480, 4 mm,
-    500 000 buckets, 1 000 000 pool blocks): a there-and-back walk of n_frames, frames
+    500 000 buckets, 2 000 000 pool blocks): a there-and-back walk of n_frames, frames
     generated on the device.  Pass 1, at the true poses, per frame: stream
     out every block farther than r_out from a point 1.5 m ahead of the
     camera, stream in the stored chunks (0.5 m) within r_in of it, integrate,
@@ -357,12 +357,12 @@ def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r
     torch.cuda.synchronize()
 
     def run(track: bool):
-        sc = vsg.Scene(voxel_size=VOXEL, truncation=TRUNC, hash_num_slots=500000, num_sdf_blocks=1000000,
-                       max_chain_nodes=1000000)
+        sc = vsg.Scene(voxel_size=VOXEL, truncation=TRUNC, hash_num_slots=500000, num_sdf_blocks=2000000,
+                       max_chain_nodes=2000000)
         rr = vsg.Renderer(W, H)
         store = vsg.Store((0.5, 0.5, 0.5))
         est = []
-        n_out = n_in = peak_res = 0
+        n_out = n_in = peak_res = refused = 0
         track_ms = 0.0
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -379,7 +379,12 @@ def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r
             T32 = T.astype(np.float32)
             c = (T32[:3, 3] + np.float32(1.5) * T32[:3, 2]).astype(np.float32)
             n_out += sc.stream_out(store, c, r_out)
-            n_in += sc.stream_in(store, c, r_in)[0]
+            try:
+                n_in += sc.stream_in(store, c, r_in)[0]
+            except vsg.VsgError as exc:
+                if exc.code != 5:  # VSG_ERR_TOO_LARGE: the pool cannot take them; nothing moved
+                    raise
+                refused += 1
             sc.integrate(pm, rgb, nm, W, H, TRUNC, T32, K.fx, K.fy, K.cx, K.cy)
             rr.render(sc, T32, K.fx, K.fy, K.cx, K.cy, MIN_D, 4.0)
             if i % 20 == 0:
@@ -390,7 +395,7 @@ def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r
         out = {"frames_per_s_wall": n_frames / wall, "ms_per_frame_wall": wall * 1e3 / n_frames,
                "blocks_streamed_out": n_out, "blocks_streamed_in": n_in,
                "resident_blocks_peak": max(peak_res, st["allocated_blocks"]),
-               "stored_blocks_end": int(store.info()[0]), "flags": st["flags"]}
+               "stored_blocks_end": int(store.info()[0]), "stream_in_refused": refused, "flags": st["flags"]}
         if track:
             terr = [float(np.linalg.norm(e[:3, 3] - p[:3, 3])) for e, p in zip(est, poses)]
             rerr = [float(np.degrees(np.arccos(np.clip((np.trace(e[:3, :3].T @ p[:3, :3]) - 1) / 2, -1, 1))))
@@ -402,7 +407,7 @@ def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r
         rr.close()
         return out
 
-    res = {"frames": n_frames, "size": "640x480", "slots": 500000, "pool_blocks": 1000000, "r_out_m": r_out,
+    res = {"frames": n_frames, "size": "640x480", "slots": 500000, "pool_blocks": 2000000, "r_out_m": r_out,
            "r_in_m": r_in,
            "chunk_m": 0.5, "fusion": run(False), "tracking": run(True)}
     del frames
