@@ -302,7 +302,8 @@ def _unit_rays(width, height, fx, fy, cx, cy):
 
 def refine_pose(scene, renderer, target_depth, pose, fx, fy, cx, cy, min_depth, max_depth, steps: int = 8,
                 huber: float = 0.01, damping: float = 1e-6, min_weight_sum: float = 0.5,
-                max_residual=(0.2, 0.05), min_incidence: float = 0.0):
+                max_residual=(0.2, 0.05), min_incidence: float = 0.0, min_pixels: int = 500,
+                max_step=(0.1, 0.1)):
     """Gauss-Newton alignment of a camera pose to a target depth image (H,W
     device float32, misses >= 1e9) through the ray cast: each step renders at
     the current pose, forms residuals (rendered - target) on pixels hit in
@@ -314,7 +315,9 @@ def refine_pose(scene, renderer, target_depth, pose, fx, fy, cx, cy, min_depth, 
     max_residual[0] to max_residual[1] over the steps.  With
     min_incidence > 0, pixels where the model's normal (vsg_render_normals)
     meets the ray at |cos| < min_incidence are left out too: at grazing
-    incidence the depth is steep in the pose.  Returns (4x4 float64 pose,
+    incidence the depth is steep in the pose.  The iteration stops when
+    fewer than min_pixels pixels carry weight; a step longer than max_step
+    (radians, metres) is shortened to it.  Returns (4x4 float64 pose,
     per-step weighted RMS residual)."""
     import torch
 
@@ -339,12 +342,16 @@ def refine_pose(scene, renderer, target_depth, pose, fx, fy, cx, cy, min_depth, 
         m = m & (a <= tau)
         w = torch.where(m, torch.where(a <= huber, torch.ones_like(a), huber / a.clamp_min(huber)),
                         torch.zeros_like(a))
+        if int(m.sum()) < min_pixels:
+            break
         Hm, b, _ = renderer.pose_normal_equations(scene, T32, fx, fy, cx, cy, r, w, min_weight_sum)
         rms.append(float(torch.sqrt((w * r * r).sum() / w.sum().clamp_min(1e-30))))
         A = Hm + damping * np.diag(np.diag(Hm))
         if not np.all(np.isfinite(A)) or np.linalg.matrix_rank(A) < 6:
             break
-        T = T @ se3_exp(-np.linalg.solve(A, b))
+        xi = -np.linalg.solve(A, b)
+        s = max(np.linalg.norm(xi[:3]) / max_step[0], np.linalg.norm(xi[3:]) / max_step[1], 1.0)
+        T = T @ se3_exp(xi / s)
     return T, rms
 
 
