@@ -258,6 +258,7 @@ int vsg_renderer_create(int w, int h, vsg_renderer** out) {
     R.w = w;
     R.h = h;
     cudaGetDevice(&R.device);
+    cudaDeviceGetAttribute(&R.sm_count, cudaDevAttrMultiProcessorCount, R.device);
     const size_t n = (size_t)w * h;
     // RayCastRender::initialize, RayCastRender.cpp:88-118
     if (cudaMalloc(&R.depth, n * sizeof(float)) != cudaSuccess || cudaMalloc(&R.position, n * sizeof(float4)) != cudaSuccess ||

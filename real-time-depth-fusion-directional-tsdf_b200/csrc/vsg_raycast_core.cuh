@@ -189,13 +189,33 @@ static __device__ __forceinline__ bool trilinear(const SceneDev& s, float px, fl
     return true;
 }
 
-// One ray: pixel (x, y) of the scene in a (in the image).  Warps should
-// cover 8x4 pixel tiles of one scene.
-static __device__ __forceinline__ void render_pixel(const RenderArgs& a, int x, int y) {
-    const SceneDev& s = a.s;
-    // numActiveBlocks == 0 leaves the outputs untouched (RayCastRender.cu:552-555)
-    if (*(volatile int*)&s.ctr->free_count >= s.num_blocks) return;
-    float T[12];
+// The march state of one ray (traverseCoarseGridSimpleSampleAll,
+// RayCastRender.cu:276-398, with the refinement of
+// findIntersectionBisection, :229-271, run as modes 1..3 of the same loop).
+struct RayState {
+    RayInv R;          // origin (the camera) and inverse direction
+    float wdx, wdy, wdz;
+    float d2r, rc, re;
+    float lastSdf, lastAlpha;
+    float ba, bad, bb, bbd, bc, mdist;
+    TapCache tc;
+    int steps;         // FP32 chain additions so far (iteration guard)
+    int mode;          // 0 = march, 1..3 = regula-falsi step
+    bool lastValid;
+    uint32_t rgb;
+    uint32_t n_full, n_skip, n_jump, n_single;
+    float out_depth;
+    float4 out_pos, out_col;
+    bool hit;
+};
+
+// Does the launch march at all?  minDepth / maxDepth of 0 or MINF leave
+// every output at MINF (renderKernel, RayCastRender.cu:463-470).
+static __device__ __forceinline__ bool march_enabled(const RenderArgs& a) {
+    return !(a.minD == 0 || a.minD == kMinf) && !(a.maxD == 0 || a.maxD == kMinf);
+}
+
+static __device__ __forceinline__ void load_pose(const RenderArgs& a, float T[12]) {
     if (a.pose_dev) {
 #pragma unroll
         for (int i = 0; i < 12; ++i) T[i] = __ldg(a.pose_dev + i);
@@ -203,8 +223,11 @@ static __device__ __forceinline__ void render_pixel(const RenderArgs& a, int x, 
 #pragma unroll
         for (int i = 0; i < 12; ++i) T[i] = a.pose.T[i];
     }
-    const size_t pi = (size_t)y * a.W + x;
-    // renderKernel, RayCastRender.cu:447-500
+}
+
+// renderKernel, RayCastRender.cu:447-500: the ray of pixel (x, y) and the
+// start of its march.
+static __device__ __forceinline__ void ray_setup(const RenderArgs& a, const float T[12], int x, int y, RayState& r) {
     float cdx = ((float)x - a.cx) / a.fx, cdy = ((float)y - a.cy) / a.fy, cdz = 1.0f;
     const float cl = sqrtf(cdx * cdx + cdy * cdy + cdz * cdz);
     if (cl > 1e-6f) {
@@ -221,181 +244,208 @@ static __device__ __forceinline__ void render_pixel(const RenderArgs& a, int x, 
         wdy /= wl;
         wdz /= wl;
     }
-    float out_depth = kMinf;
-    float4 out_pos = make_float4(kMinf, kMinf, kMinf, kMinf);
-    float4 out_col = make_float4(kMinf, kMinf, kMinf, kMinf);
-    bool hit = false;
-    const float minD = a.minD, maxD = a.maxD;
-    if (!(minD == 0 || minD == kMinf) && !(maxD == 0 || maxD == kMinf)) {
-        // traverseCoarseGridSimpleSampleAll, RayCastRender.cu:276-398
-        const float ox = a.camx, oy = a.camy, oz = a.camz;
-        const float v = s.voxel;
-        float lastSdf = 0.0f, lastAlpha = 0.0f;
-        bool lastValid = false;
-        const float d2r = 1.0f / cdz;
-        float rc = d2r * fmaxf(minD, minD);
-        const float re = d2r * fminf(maxD, maxD);
+    r.wdx = wdx;
+    r.wdy = wdy;
+    r.wdz = wdz;
+    r.out_depth = kMinf;
+    r.out_pos = make_float4(kMinf, kMinf, kMinf, kMinf);
+    r.out_col = make_float4(kMinf, kMinf, kMinf, kMinf);
+    r.hit = false;
+    r.lastSdf = 0.0f;
+    r.lastAlpha = 0.0f;
+    r.lastValid = false;
+    r.d2r = 1.0f / cdz;
+    r.rc = r.d2r * fmaxf(a.minD, a.minD);
+    r.re = r.d2r * fminf(a.maxD, a.maxD);
+    r.R.ox = a.camx;
+    r.R.oy = a.camy;
+    r.R.oz = a.camz;
+    r.R.hx = fabsf(wdx) > 1e-12f;
+    r.R.hy = fabsf(wdy) > 1e-12f;
+    r.R.hz = fabsf(wdz) > 1e-12f;
+    r.R.ix = r.R.hx ? 1.0f / wdx : 0.0f;
+    r.R.iy = r.R.hy ? 1.0f / wdy : 0.0f;
+    r.R.iz = r.R.hz ? 1.0f / wdz : 0.0f;
+    r.tc.bx = 0x7FFFFFFF;
+    r.tc.by = r.tc.bz = r.tc.span = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) r.tc.set(i, -1);
+    r.steps = 0;
+    r.mode = 0;
+    r.ba = r.bad = r.bb = r.bbd = r.bc = r.mdist = 0.0f;
+    r.rgb = 0u;
+    r.n_full = r.n_skip = r.n_jump = r.n_single = 0u;
+}
+
+// One iteration of the march: a skip jump, a march sample or a
+// regula-falsi sample.  Returns true when the ray is done.
+static __device__ __forceinline__ bool ray_step(const RenderArgs& a, RayState& r, size_t pi) {
+    const SceneDev& s = a.s;
+    const float v = s.voxel;
+    const float ox = r.R.ox, oy = r.R.oy, oz = r.R.oz;
+    float st;  // ray parameter of the sample to evaluate
+    if (r.mode == 0) {
+        if (!(r.rc < r.re)) return true;
+        if (r.steps >= kMaxMarch) {
+            atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_MARCH_LIMIT);
+            return true;
+        }
         const float C = (float)kBlock * v, C2 = 2.0f * v, C8 = 64.0f * v;
         const float invC2 = 1.0f / C2;
-        RayInv R;
-        R.ox = ox;
-        R.oy = oy;
-        R.oz = oz;
-        R.hx = fabsf(wdx) > 1e-12f;
-        R.hy = fabsf(wdy) > 1e-12f;
-        R.hz = fabsf(wdz) > 1e-12f;
-        R.ix = R.hx ? 1.0f / wdx : 0.0f;
-        R.iy = R.hy ? 1.0f / wdy : 0.0f;
-        R.iz = R.hz ? 1.0f / wdz : 0.0f;
-        TapCache tc;
-        tc.bx = 0x7FFFFFFF;
-        tc.by = tc.bz = tc.span = 0;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) tc.set(i, -1);
-        int steps = 0;  // FP32 chain additions so far (iteration guard)
-        uint32_t n_full = 0u, n_skip = 0u, n_jump = 0u, n_single = 0u;
         const float m = 1e-4f;  // keep skipped samples this far inside their cell
-        // one loop for the march and the regula-falsi steps, so a single
-        // trilinear evaluation site serves both (mode 0 = march, 1..3 =
-        // step k of findIntersectionBisection, RayCastRender.cu:229-271)
-        int mode = 0;
-        float ba = 0.0f, bad = 0.0f, bb = 0.0f, bbd = 0.0f, bc = 0.0f, mdist = 0.0f;
-        uint32_t rgb = 0u;
-#pragma unroll 1
-        while (true) {
-            float st;  // ray parameter of the sample to evaluate
-            if (mode == 0) {
-                if (!(rc < re)) break;
-                if (steps >= kMaxMarch) {
-                    atomicOr(&s.ctr->flags, (uint32_t)VSG_FLAG_MARCH_LIMIT);
-                    break;
-                }
-                const float spx = ox + rc * wdx, spy = oy + rc * wdy, spz = oz + rc * wdz;
-                // global sub-cube (2 voxels) of the sample, its block cell and super-cell
-                const int qx = __float2int_rd(spx * invC2), qy = __float2int_rd(spy * invC2),
-                          qz = __float2int_rd(spz * invC2);
-                float tlo = 0.0f, thi = 0.0f;
-                bool cell = false;
-                const int k = s.bidx_log2;
-                const uint32_t sb = grid_bit(qx >> 5, qy >> 5, qz >> 5, k - 3);
-                if (!((__ldg(s.sup + (sb >> 5)) >> (sb & 31)) & 1u)) {
-                    cell_interval(R, qx >> 5, qy >> 5, qz >> 5, C8, tlo, thi);  // 64-voxel cell
-                    cell = true;
-                } else {
-                    const unsigned long long w = __ldg(s.dwm + bidx_cell(qx >> 2, qy >> 2, qz >> 2, k));
-                    if (w == 0ull) {
-                        cell_interval(R, qx >> 2, qy >> 2, qz >> 2, C, tlo, thi);  // 8-voxel cell
-                        cell = true;
-                    } else if (!((w >> ((((qz & 3) << 2) | (qy & 3)) << 2 | (qx & 3))) & 1ull)) {
-                        cell_interval(R, qx, qy, qz, C2, tlo, thi);  // 2-voxel cell
-                        cell = true;
-                    }
-                }
-                if (cell) {
-                    if (rc > tlo + m && rc < thi - m) {
-                        const int before = steps;
-                        rc = vsg_chain_advance(rc, v * 0.5f, fminf(thi - m, re), kMaxMarch - steps, &steps);
-                        n_skip += (uint32_t)(steps - before);
-                        ++n_jump;
-                        lastValid = false;
-                        continue;
-                    }
-                    ++n_single;  // too close to the cell boundary to trust the test
-                }
-                st = rc;
-            } else {
-                st = bc;
-            }
-            float dist = 0.0f;
-            ++n_full;
-            const bool ok = trilinear(s, ox + st * wdx, oy + st * wdy, oz + st * wdz, dist, mode != 0, rgb, tc, a.touched);
-            if (mode == 0) {
-                if (ok && lastValid && lastSdf < 0.0f && dist > 0.0f) {
-                    // zero crossing: a = last sample, b = this one
-                    if (a.rec) a.rec[pi] = make_float2(lastAlpha, rc);
-                    ba = lastAlpha;
-                    bad = lastSdf;
-                    bb = rc;
-                    bbd = dist;
-                    mdist = dist;
-                    bc = ba + (bad / (bad - bbd)) * (bb - ba);  // findIntersectionLinear
-                    mode = 1;
-                    continue;
-                }
-                if (ok) {
-                    lastSdf = dist;
-                    lastAlpha = rc;
-                }
-                lastValid = ok;
-                rc += v * 0.5f;
-                ++steps;
-            } else {
-                bool finished = !ok, success = false;
-                if (ok) {
-                    if (bad * dist > 0.0f) {
-                        ba = bc;
-                        bad = dist;
-                    } else {
-                        bb = bc;
-                        bbd = dist;
-                    }
-                    if (mode == 3) {
-                        finished = true;
-                        success = true;
-                    } else {
-                        bc = ba + (bad / (bad - bbd)) * (bb - ba);
-                        ++mode;
-                    }
-                }
-                if (finished) {
-                    const float th = v * 3;  // RayCastRender.cu:362-365
-                    if (success && fabsf(lastSdf - mdist) < th && fabsf(mdist) < th) {
-                        const float alpha = bc;
-                        out_depth = alpha / d2r;
-                        out_pos = make_float4(ox + alpha * wdx, oy + alpha * wdy, oz + alpha * wdz, 1.0f);
-                        out_col = make_float4((float)(rgb & 0xFFu) / 255.0f, (float)((rgb >> 8) & 0xFFu) / 255.0f,
-                                              (float)((rgb >> 16) & 0xFFu) / 255.0f, 1.0f);
-                        hit = true;
-                        break;
-                    }
-                    // not accepted: the march continues after the crossing sample
-                    lastSdf = mdist;
-                    lastAlpha = rc;
-                    lastValid = true;
-                    rc += v * 0.5f;
-                    ++steps;
-                    mode = 0;
-                }
+        const float spx = ox + r.rc * r.wdx, spy = oy + r.rc * r.wdy, spz = oz + r.rc * r.wdz;
+        // global sub-cube (2 voxels) of the sample, its block cell and super-cell
+        const int qx = __float2int_rd(spx * invC2), qy = __float2int_rd(spy * invC2), qz = __float2int_rd(spz * invC2);
+        float tlo = 0.0f, thi = 0.0f;
+        bool cell = false;
+        const int k = s.bidx_log2;
+        const uint32_t sb = grid_bit(qx >> 5, qy >> 5, qz >> 5, k - 3);
+        if (!((__ldg(s.sup + (sb >> 5)) >> (sb & 31)) & 1u)) {
+            cell_interval(r.R, qx >> 5, qy >> 5, qz >> 5, C8, tlo, thi);  // 64-voxel cell
+            cell = true;
+        } else {
+            const unsigned long long w = __ldg(s.dwm + bidx_cell(qx >> 2, qy >> 2, qz >> 2, k));
+            if (w == 0ull) {
+                cell_interval(r.R, qx >> 2, qy >> 2, qz >> 2, C, tlo, thi);  // 8-voxel cell
+                cell = true;
+            } else if (!((w >> ((((qz & 3) << 2) | (qy & 3)) << 2 | (qx & 3))) & 1ull)) {
+                cell_interval(r.R, qx, qy, qz, C2, tlo, thi);  // 2-voxel cell
+                cell = true;
             }
         }
-        const unsigned am = __activemask();
-        const unsigned hm = __ballot_sync(am, hit);
-        const uint32_t it = n_full + n_jump;
-        const uint32_t it_max = __reduce_max_sync(am, it);
-        uint32_t nf = n_full, ns = n_skip, nj = n_jump, n1 = n_single, ni = it;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            nf += __shfl_xor_sync(am, nf, o);
-            ns += __shfl_xor_sync(am, ns, o);
-            nj += __shfl_xor_sync(am, nj, o);
-            n1 += __shfl_xor_sync(am, n1, o);
-            ni += __shfl_xor_sync(am, ni, o);
+        if (cell) {
+            if (r.rc > tlo + m && r.rc < thi - m) {
+                const int before = r.steps;
+                r.rc = vsg_chain_advance(r.rc, v * 0.5f, fminf(thi - m, r.re), kMaxMarch - r.steps, &r.steps);
+                r.n_skip += (uint32_t)(r.steps - before);
+                ++r.n_jump;
+                r.lastValid = false;
+                return false;
+            }
+            ++r.n_single;  // too close to the cell boundary to trust the test
         }
-        if ((threadIdx.x & 31) == (__ffs(am) - 1)) {
-            atomicAdd(&s.frame->hits, (uint32_t)__popc(hm));
-            atomicAdd(&s.frame->misses, (uint32_t)(__popc(am) - __popc(hm)));
-            atomicAdd(&s.frame->samples_full, nf);
-            atomicAdd(&s.frame->samples_skipped, ns);
-            atomicAdd(&s.frame->jumps, nj);
-            atomicAdd(&s.frame->singles, n1);
-            atomicAdd(&s.frame->lane_iters, ni);
-            atomicAdd(&s.frame->warp_iters, it_max);
+        st = r.rc;
+    } else {
+        st = r.bc;
+    }
+    float dist = 0.0f;
+    ++r.n_full;
+    const bool ok = trilinear(s, ox + st * r.wdx, oy + st * r.wdy, oz + st * r.wdz, dist, r.mode != 0, r.rgb, r.tc,
+                              a.touched);
+    if (r.mode == 0) {
+        if (ok && r.lastValid && r.lastSdf < 0.0f && dist > 0.0f) {
+            // zero crossing: a = last sample, b = this one
+            if (a.rec) a.rec[pi] = make_float2(r.lastAlpha, r.rc);
+            r.ba = r.lastAlpha;
+            r.bad = r.lastSdf;
+            r.bb = r.rc;
+            r.bbd = dist;
+            r.mdist = dist;
+            r.bc = r.ba + (r.bad / (r.bad - r.bbd)) * (r.bb - r.ba);  // findIntersectionLinear
+            r.mode = 1;
+            return false;
+        }
+        if (ok) {
+            r.lastSdf = dist;
+            r.lastAlpha = r.rc;
+        }
+        r.lastValid = ok;
+        r.rc += v * 0.5f;
+        ++r.steps;
+        return false;
+    }
+    bool finished = !ok, success = false;
+    if (ok) {
+        if (r.bad * dist > 0.0f) {
+            r.ba = r.bc;
+            r.bad = dist;
+        } else {
+            r.bb = r.bc;
+            r.bbd = dist;
+        }
+        if (r.mode == 3) {
+            finished = true;
+            success = true;
+        } else {
+            r.bc = r.ba + (r.bad / (r.bad - r.bbd)) * (r.bb - r.ba);
+            ++r.mode;
         }
     }
-    a.depth[pi] = out_depth;
-    a.pos[pi] = out_pos;
-    a.col[pi] = out_col;
+    if (finished) {
+        const float th = v * 3;  // RayCastRender.cu:362-365
+        if (success && fabsf(r.lastSdf - r.mdist) < th && fabsf(r.mdist) < th) {
+            const float alpha = r.bc;
+            r.out_depth = alpha / r.d2r;
+            r.out_pos = make_float4(ox + alpha * r.wdx, oy + alpha * r.wdy, oz + alpha * r.wdz, 1.0f);
+            r.out_col = make_float4((float)(r.rgb & 0xFFu) / 255.0f, (float)((r.rgb >> 8) & 0xFFu) / 255.0f,
+                                    (float)((r.rgb >> 16) & 0xFFu) / 255.0f, 1.0f);
+            r.hit = true;
+            return true;
+        }
+        // not accepted: the march continues after the crossing sample
+        r.lastSdf = r.mdist;
+        r.lastAlpha = r.rc;
+        r.lastValid = true;
+        r.rc += v * 0.5f;
+        ++r.steps;
+        r.mode = 0;
+    }
+    return false;
+}
+
+static __device__ __forceinline__ void ray_write(const RenderArgs& a, const RayState& r, size_t pi) {
+    a.depth[pi] = r.out_depth;
+    a.pos[pi] = r.out_pos;
+    a.col[pi] = r.out_col;
     a.nrm[pi] = make_float4(kMinf, kMinf, kMinf, kMinf);
+}
+
+// Warp-summed march statistics of the active lanes into the frame counters.
+static __device__ __forceinline__ void add_stats(const SceneDev& s, unsigned am, uint32_t hits, uint32_t rays,
+                                                 uint32_t nf, uint32_t ns, uint32_t nj, uint32_t n1, uint32_t ni,
+                                                 uint32_t witer) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        hits += __shfl_xor_sync(am, hits, o);
+        rays += __shfl_xor_sync(am, rays, o);
+        nf += __shfl_xor_sync(am, nf, o);
+        ns += __shfl_xor_sync(am, ns, o);
+        nj += __shfl_xor_sync(am, nj, o);
+        n1 += __shfl_xor_sync(am, n1, o);
+        ni += __shfl_xor_sync(am, ni, o);
+    }
+    if ((threadIdx.x & 31) == (__ffs(am) - 1)) {
+        atomicAdd(&s.frame->hits, hits);
+        atomicAdd(&s.frame->misses, rays - hits);
+        atomicAdd(&s.frame->samples_full, nf);
+        atomicAdd(&s.frame->samples_skipped, ns);
+        atomicAdd(&s.frame->jumps, nj);
+        atomicAdd(&s.frame->singles, n1);
+        atomicAdd(&s.frame->lane_iters, ni);
+        atomicAdd(&s.frame->warp_iters, witer);
+    }
+}
+
+// One ray: pixel (x, y) of the scene in a (in the image).  Warps should
+// cover 8x4 pixel tiles of one scene.
+static __device__ __forceinline__ void render_pixel(const RenderArgs& a, int x, int y) {
+    const SceneDev& s = a.s;
+    // numActiveBlocks == 0 leaves the outputs untouched (RayCastRender.cu:552-555)
+    if (*(volatile int*)&s.ctr->free_count >= s.num_blocks) return;
+    float T[12];
+    load_pose(a, T);
+    const size_t pi = (size_t)y * a.W + x;
+    RayState r;
+    ray_setup(a, T, x, y, r);
+    if (march_enabled(a)) {
+#pragma unroll 1
+        while (!ray_step(a, r, pi)) {
+        }
+        const unsigned am = __activemask();
+        const uint32_t it = r.n_full + r.n_jump;
+        add_stats(s, am, r.hit ? 1u : 0u, 1u, r.n_full, r.n_skip, r.n_jump, r.n_single, it, __reduce_max_sync(am, it));
+    }
+    ray_write(a, r, pi);
 }
 
 static __device__ __forceinline__ void render_begin(FrameCounters* f) {
