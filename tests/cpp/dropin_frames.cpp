@@ -5,8 +5,11 @@
 // matrix, download the depth.  After the frames it extracts the surface with
 // the marching-cubes launchers (MarchingCubes.h:34-58) and streams blocks
 // out to host memory and back with VoxelStreamingManager, then renders the
-// last pose again.  Test harness: frames come from binary files written by
-// the Python test, depths are written back for comparison.
+// last pose again.  The last frame's render and surface points go to PLY
+// files.  Built with -DUSE_NORMAL_DIR_ALLOC it runs the reference's
+// normal-direction allocation (Method 2).  Test harness: frames come from
+// binary files written by the Python test, depths are written back for
+// comparison.
 //
 //   dropin_frames DIR NFRAMES W H FX FY CX CY VOXEL TRUNC SLOTS BLOCKS MIND MAXD
 #include <cstdio>
@@ -79,6 +82,12 @@ int main(int argc, char** argv) {
         renderer.render(&scene, cam, d_T, fx, fy, cx, cy, minD, maxD);
         renderer.downloadDepthFloat(depth.data());
         if (!write_file(dir + "/depth_" + id + ".bin", depth.data(), n * 4)) return 6;
+        if (i == nframes - 1) {
+            // the exporters the reference's main loop calls (voxelSG.cpp:656-673)
+            if (!renderer.savePointCloudPLY(dir + "/cloud.ply")) return 8;
+            std::printf("surface_points=%d\n", renderer.extractSurfacePoints(&scene, -0.1f, 0.1f, 5));
+            if (!renderer.saveExtractedSurfacePointsPLY(dir + "/surface.ply")) return 9;
+        }
     }
     std::printf("frames=%u free=%u\n", scene.getNumIntegratedFrames(), scene.getHeapFreeCount());
     // marching cubes as the reference's launchers are called

@@ -16,7 +16,8 @@ PKG = os.path.join(ROOT, "real-time-depth-fusion-directional-tsdf_b200")
 CUDA = "/usr/local/cuda"
 
 
-def test_cpp_dropin_matches_binding(cuda, synth_mod, tmp_path):
+@pytest.mark.parametrize("method", [1, 2])
+def test_cpp_dropin_matches_binding(cuda, synth_mod, tmp_path, method):
     import vsg
 
     W, H, N = 160, 120, 3
@@ -28,7 +29,8 @@ def test_cpp_dropin_matches_binding(cuda, synth_mod, tmp_path):
         f.normals.astype(np.float32).tofile(os.path.join(d, f"nm_{i}.bin"))
         f.pose.astype(np.float32).tofile(os.path.join(d, f"pose_{i}.bin"))
     exe = os.path.join(d, "dropin_frames")
-    subprocess.run(["g++", "-O2", "-std=c++17", "-o", exe, os.path.join(ROOT, "tests", "cpp", "dropin_frames.cpp"),
+    defs = ["-DUSE_NORMAL_DIR_ALLOC"] if method == 2 else []
+    subprocess.run(["g++", "-O2", "-std=c++17", *defs, "-o", exe, os.path.join(ROOT, "tests", "cpp", "dropin_frames.cpp"),
                     "-I", os.path.join(ROOT, "include"), "-I", f"{CUDA}/include", "-L", PKG, "-lvsg",
                     f"-Wl,-rpath,{PKG}", "-L", f"{CUDA}/lib64", "-lcudart"], check=True)
     r = subprocess.run([exe, d, str(N), str(W), str(H), str(K.fx), str(K.fy), str(K.cx), str(K.cy), "0.004", "0.02",
@@ -36,6 +38,7 @@ def test_cpp_dropin_matches_binding(cuda, synth_mod, tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     assert f"frames={N}" in r.stdout
     sc = vsg.Scene(voxel_size=0.004, truncation=0.02, hash_num_slots=20011, num_sdf_blocks=40000)
+    sc.set_alloc_method(method)
     rr = vsg.Renderer(W, H)
     for i, f in enumerate(fr):
         pm = cuda.from_numpy(f.pointmap).cuda()
@@ -47,6 +50,14 @@ def test_cpp_dropin_matches_binding(cuda, synth_mod, tmp_path):
         got = np.fromfile(os.path.join(d, f"depth_{i}.bin"), np.float32).reshape(H, W)
         assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), i
         assert (got < 1e9).sum() > 0.5 * W * H
+    # the exporters of the last frame
+    ply = tmp_path / "cloud_binding.ply"
+    rr.save_ply(str(ply))
+    assert (tmp_path / "cloud.ply").read_text() == ply.read_text()
+    pts = vsg.SurfacePoints(1_000_000)
+    pts.extract(sc, -0.1, 0.1, 5)
+    assert f"surface_points={pts.count()}" in r.stdout
+    assert (tmp_path / "surface.ply").read_text().count("\n") == pts.count() + 14
     mc = vsg.MarchingCubes(250000)
     mc.run(sc, voxel_size=0.004)
     assert f"triangles={min(mc.count(), 2**31 - 1)}" in r.stdout
