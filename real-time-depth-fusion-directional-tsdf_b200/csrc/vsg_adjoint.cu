@@ -533,13 +533,24 @@ __global__ void __launch_bounds__(128) k_pose_normal_equations(BackArgs a) {
     }
 }
 
-// Sum nv values (nv <= 32) over n partial records in a fixed order.
+// Sum nv values (nv <= 32) over n partial records in a fixed order (four
+// independent accumulators per lane keep four loads in flight).
 __global__ void k_reduce_records(const double* partials, int n, int nv, double* out) {
     __shared__ double red[32][33];
     const int i = threadIdx.x / 32, lane = threadIdx.x % 32;
     double s = 0.0;
-    if (i < nv)
-        for (int k = lane; k < n; k += 32) s += partials[(size_t)k * nv + i];
+    if (i < nv) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int k = lane;
+        for (; k + 96 < n; k += 128) {
+            s0 += partials[(size_t)k * nv + i];
+            s1 += partials[(size_t)(k + 32) * nv + i];
+            s2 += partials[(size_t)(k + 64) * nv + i];
+            s3 += partials[(size_t)(k + 96) * nv + i];
+        }
+        for (; k < n; k += 32) s0 += partials[(size_t)k * nv + i];
+        s = (s0 + s1) + (s2 + s3);
+    }
     red[i][lane] = s;
     __syncthreads();
     if (lane == 0 && i < nv) {
