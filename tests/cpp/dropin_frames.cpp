@@ -85,7 +85,7 @@ int main(int argc, char** argv) {
         if (i == nframes - 1) {
             // the exporters the reference's main loop calls (voxelSG.cpp:656-673)
             if (!renderer.savePointCloudPLY(dir + "/cloud.ply")) return 8;
-            std::printf("surface_points=%d\n", renderer.extractSurfacePoints(&scene, -0.1f, 0.1f, 5));
+            std::printf("surface_points=%d\n", renderer.extractSurfacePoints(&scene, -0.1f, 0.1f, 1));
             if (!renderer.saveExtractedSurfacePointsPLY(dir + "/surface.ply")) return 9;
         }
     }

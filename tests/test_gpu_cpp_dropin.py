@@ -55,7 +55,7 @@ def test_cpp_dropin_matches_binding(cuda, synth_mod, tmp_path, method):
     rr.save_ply(str(ply))
     assert (tmp_path / "cloud.ply").read_text() == ply.read_text()
     pts = vsg.SurfacePoints(1_000_000)
-    pts.extract(sc, -0.1, 0.1, 5)
+    pts.extract(sc, -0.1, 0.1, 1)
     assert f"surface_points={pts.count()}" in r.stdout
     assert (tmp_path / "surface.ply").read_text().count("\n") == pts.count() + 14
     mc = vsg.MarchingCubes(250000)
