@@ -49,7 +49,9 @@ def test_cpp_dropin_matches_binding(cuda, synth_mod, tmp_path, method):
         ref = rr.download()["depth"]
         got = np.fromfile(os.path.join(d, f"depth_{i}.bin"), np.float32).reshape(H, W)
         assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), i
-        assert (got < 1e9).sum() > 0.5 * W * H
+        # Method 2 allocates only where its 2 cm rays cross a block boundary, so
+        # its early frames hit fewer pixels
+        assert (got < 1e9).sum() > (0.5 if method == 1 else 0.1) * W * H
     # the exporters of the last frame
     ply = tmp_path / "cloud_binding.ply"
     rr.save_ply(str(ply))
