@@ -115,6 +115,17 @@ def make_stream(args):
     return frames, K
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(frames, K, budget_s: float = 20.0) -> dict:
     """Oracle (CPU restatement, OpenMP) on a bounded sample of the stream:
     all frames integrated, a band of rows ray cast per frame."""
@@ -140,7 +151,7 @@ def cpu_baseline(frames, K, budget_s: float = 20.0) -> dict:
         if t_int + t_ren > budget_s:
             break
     fps = n / (t_int + t_ren)
-    return {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
+    return {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port", "cpu": cpu_model(),
             "sample": f"{n} frames integrated in full; ray cast on {rows} central rows per frame, "
                       f"scaled to {K.height} rows"}
 
@@ -162,7 +173,7 @@ def run_reference(args):
             "config": {"workload": WORKLOAD, "frames": args.frames, "sample": r["sample"]},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "frames/s", "cores": r["cores"], "kind": "port",
-                             "sample": r["sample"]},
+                             "cpu": r["cpu"], "sample": r["sample"]},
             "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
