@@ -219,3 +219,48 @@ def test_normal_direction_allocation_refused_where_unsupported(cuda, synth_mod):
     with pytest.raises(vsg.VsgError):
         sc.set_alloc_method(3)
     sc.close()
+
+
+def test_ragged_and_invalid_inputs(cuda, oracle_mod, synth_mod):
+    """An image size that fills no tile evenly (157x113), then the same frames
+    with NaN, infinite, behind-camera and zero points mixed in, then an
+    all-zero frame: volumes bit-exact against the oracle after every frame,
+    renders within tolerance, and the coordinate-range flag raised exactly
+    when the oracle drops out-of-range blocks (VoxelScene.cu:547-633 lets NaN
+    depths through its z test, as the oracle does)."""
+    import vsg
+
+    fr, K = synth_mod.tabletop_stream(6, 4, 157, 113)
+    rng = np.random.default_rng(9)
+    frames = [fr[0], fr[1]]
+    for f in fr[2:]:
+        pm = f.pointmap.copy()
+        u = rng.random(pm.shape[:2])
+        pm[u < 0.05] = np.nan
+        pm[(u >= 0.05) & (u < 0.07)] = np.inf
+        neg = (u >= 0.07) & (u < 0.10)
+        pm[neg, 2] = -pm[neg, 2]
+        pm[(u >= 0.10) & (u < 0.20)] = 0.0
+        frames.append(type(f)(pointmap=pm, rgb=f.rgb, normals=f.normals, depth=f.depth, pose=f.pose))
+    z = fr[0]
+    frames.append(type(z)(pointmap=np.zeros_like(z.pointmap), rgb=z.rgb, normals=z.normals, depth=z.depth,
+                          pose=fr[3].pose))
+    sc = vsg.Scene(voxel_size=0.004, hash_num_slots=20011, num_sdf_blocks=60000, truncation=0.02)
+    rr = vsg.Renderer(K.width, K.height)
+    orc = oracle_mod.OracleScene(0.004)
+    for i, f in enumerate(frames):
+        pm, rgb, nm = _upload(cuda, f)
+        sc.integrate(pm, rgb, nm, K.width, K.height, 0.02, f.pose, K.fx, K.fy, K.cx, K.cy)
+        orc.integrate(f.pointmap, f.rgb, 0.02, f.pose, K.fx, K.fy, K.cx, K.cy)
+        gc, gv = sc.export()
+        oc, ov = orc.export()
+        v = compare_volumes(gc, gv, oc, ov["raw"])
+        assert v["same_blocks"] and v["bit_exact"], (i, v)
+        drops = orc.L.orc_coord_range_drops(orc.h)
+        assert bool(sc.stats()["flags"] & vsg.FLAG_COORD_RANGE) == (drops > 0), (i, drops)
+        assert sc.stats()["flags"] & ~vsg.FLAG_COORD_RANGE == 0
+        rr.render(sc, f.pose, K.fx, K.fy, K.cx, K.cy, 0.2, 3.0)
+        o = orc.render(K.width, K.height, f.pose, K.fx, K.fy, K.cx, K.cy, 0.2, 3.0)
+        assert compare_renders(rr.download(), o, DEPTH_TOL)["frac_within_tol"] >= DEPTH_FRAC, i
+    sc.close()
+    rr.close()
