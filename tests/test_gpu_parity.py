@@ -264,3 +264,41 @@ def test_ragged_and_invalid_inputs(cuda, oracle_mod, synth_mod):
         assert compare_renders(rr.download(), o, DEPTH_TOL)["frac_within_tol"] >= DEPTH_FRAC, i
     sc.close()
     rr.close()
+
+
+def test_render_call_forms(cuda, oracle_mod, synth_mod):
+    """RayCastRender::render's argument forms (RayCastRender.cpp:123-183,
+    RayCastRender.cu:500-505): a device pose gives the host-pose result bit
+    for bit; a camera position apart from the pose's translation is honoured
+    as the reference honours it (the oracle with the same camera); a minimum
+    or maximum depth of 0 or MINF leaves every output at MINF."""
+    import vsg
+
+    fr, K = synth_mod.tabletop_stream(8, 3, 160, 120)
+    sc = vsg.Scene(voxel_size=0.004, hash_num_slots=20011, num_sdf_blocks=60000, truncation=0.02)
+    orc = oracle_mod.OracleScene(0.004)
+    for f in fr:
+        pm, rgb, nm = _upload(cuda, f)
+        sc.integrate(pm, rgb, nm, K.width, K.height, 0.02, f.pose, K.fx, K.fy, K.cx, K.cy)
+        orc.integrate(f.pointmap, f.rgb, 0.02, f.pose, K.fx, K.fy, K.cx, K.cy)
+    rr = vsg.Renderer(K.width, K.height)
+    T = np.asarray(fr[-1].pose, np.float32)
+    rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, 0.2, 3.0)
+    host = rr.download()
+    Td = cuda.from_numpy(np.ascontiguousarray(T.reshape(16))).cuda()
+    rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, 0.2, 3.0, pose_dev=Td.data_ptr())
+    dev = rr.download()
+    for k in ("depth", "position", "color", "normal"):
+        assert np.array_equal(host[k].view(np.uint32), dev[k].view(np.uint32)), k
+    cam = (T[:3, 3] + np.array([0.01, -0.02, 0.015], np.float32)).astype(np.float32)
+    rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, 0.2, 3.0, cam_pos=cam)
+    want = orc.render(K.width, K.height, T, K.fx, K.fy, K.cx, K.cy, 0.2, 3.0, cam=cam)
+    r = compare_renders(rr.download(), want, DEPTH_TOL)
+    assert r["bit_exact_all"], r
+    for lo, hi in ((0.0, 3.0), (1e10, 3.0), (0.2, 0.0), (0.2, 1e10)):
+        rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, lo, hi)
+        out = rr.download()
+        for k in ("depth", "position", "color", "normal"):
+            assert np.all(out[k] == np.float32(1e10)), (lo, hi, k)
+    sc.close()
+    rr.close()
