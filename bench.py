@@ -378,6 +378,7 @@ def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r
         store = vsg.Store((0.5, 0.5, 0.5))
         est = []
         n_out = n_in = peak_res = refused = 0
+        t_out = t_in = t_fuse = 0.0
         track_ms = 0.0
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -393,15 +394,22 @@ def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r
             est.append(T)
             T32 = T.astype(np.float32)
             c = (T32[:3, 3] + np.float32(1.5) * T32[:3, 2]).astype(np.float32)
+            ta = time.perf_counter()
             n_out += sc.stream_out(store, c, r_out)
+            tb = time.perf_counter()
             try:
                 n_in += sc.stream_in(store, c, r_in)[0]
             except vsg.VsgError as exc:
                 if exc.code != 5:  # VSG_ERR_TOO_LARGE: the pool cannot take them; nothing moved
                     raise
                 refused += 1
+            tc = time.perf_counter()
             sc.integrate(pm, rgb, nm, W, H, TRUNC, T32, K.fx, K.fy, K.cx, K.cy)
             rr.render(sc, T32, K.fx, K.fy, K.cx, K.cy, MIN_D, 4.0)
+            torch.cuda.synchronize()
+            t_out += tb - ta
+            t_in += tc - tb
+            t_fuse += time.perf_counter() - tc
             if i % 20 == 0:
                 peak_res = max(peak_res, sc.stats()["allocated_blocks"])
         torch.cuda.synchronize()
@@ -410,7 +418,9 @@ def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r
         out = {"frames": nf, "frames_per_s_wall": nf / wall, "ms_per_frame_wall": wall * 1e3 / nf,
                "blocks_streamed_out": n_out, "blocks_streamed_in": n_in,
                "resident_blocks_peak": max(peak_res, st["allocated_blocks"]),
-               "stored_blocks_end": int(store.info()[0]), "stream_in_refused": refused, "flags": st["flags"]}
+               "stored_blocks_end": int(store.info()[0]), "stream_in_refused": refused, "flags": st["flags"],
+               "ms_per_frame_stream_out": t_out * 1e3 / nf, "ms_per_frame_stream_in": t_in * 1e3 / nf,
+               "ms_per_frame_integrate_render": t_fuse * 1e3 / nf}
         if track:
             terr = [float(np.linalg.norm(e[:3, 3] - p[:3, 3])) for e, p in zip(est, poses)]
             rerr = [float(np.degrees(np.arccos(np.clip((np.trace(e[:3, :3].T @ p[:3, :3]) - 1) / 2, -1, 1))))
