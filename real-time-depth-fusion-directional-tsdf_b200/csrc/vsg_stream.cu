@@ -37,6 +37,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <memory>
 #include <unordered_map>
 #include <vector>
 
@@ -247,10 +248,17 @@ struct Coord3Hash {
 
 }  // namespace
 
+// Host voxel storage in slabs of kSlabBlocks blocks: appending a block
+// copies its 4 KiB once (no regrowth of one large array), and slabs of
+// chunks that stream back in return to the store's free list, so a long
+// run stops faulting in fresh pages.
+constexpr size_t kSlabBlocks = 16;
+
 struct Chunk {
     std::vector<std::array<int, 3>> coords;
-    std::vector<Voxel> vox;  // 512 per block
+    std::vector<Voxel*> slabs;  // block i at slabs[i / kSlabBlocks] + (i % kSlabBlocks) * 512
     std::unordered_map<std::array<int, 3>, uint32_t, Coord3Hash> index;
+    Voxel* block(size_t i) const { return slabs[i / kSlabBlocks] + (i % kSlabBlocks) * kVoxPerBlock; }
 };
 
 struct BlockStore {
@@ -258,6 +266,26 @@ struct BlockStore {
     float voxel = 0.0f;  // voxel size of the blocks held (0 = none yet)
     std::unordered_map<std::array<int, 3>, Chunk, Coord3Hash> chunks;
     uint64_t n_blocks = 0;
+    std::vector<std::unique_ptr<Voxel[]>> slab_mem;  // every slab ever made (freed with the store)
+    std::vector<Voxel*> free_slabs;
+
+    Voxel* new_slab() {
+        if (!free_slabs.empty()) {
+            Voxel* s = free_slabs.back();
+            free_slabs.pop_back();
+            return s;
+        }
+        slab_mem.emplace_back(new Voxel[kSlabBlocks * kVoxPerBlock]);
+        return slab_mem.back().get();
+    }
+    // drop a chunk, keeping its slabs for reuse
+    void erase_chunk(const std::array<int, 3>& ck) {
+        auto it = chunks.find(ck);
+        if (it == chunks.end()) return;
+        n_blocks -= it->second.coords.size();
+        for (Voxel* s : it->second.slabs) free_slabs.push_back(s);
+        chunks.erase(it);
+    }
 
     // worldToChunks, VoxelStreamingManager.cpp:905-922
     std::array<int, 3> chunk_of_world(const float p[3]) const {
@@ -289,13 +317,15 @@ struct BlockStore {
         Chunk& ch = chunks[chunk_of_block(x, y, z, voxel_size)];
         auto it = ch.index.find(key);
         if (it != ch.index.end()) {
-            Voxel* dst = ch.vox.data() + (size_t)it->second * kVoxPerBlock;
+            Voxel* dst = ch.block(it->second);
             for (int i = 0; i < kVoxPerBlock; ++i) dst[i] = merge_voxels(dst[i], v[i]);
             return;
         }
-        ch.index.emplace(key, (uint32_t)ch.coords.size());
+        const size_t i = ch.coords.size();
+        if (i % kSlabBlocks == 0) ch.slabs.push_back(new_slab());
+        ch.index.emplace(key, (uint32_t)i);
         ch.coords.push_back(key);
-        ch.vox.insert(ch.vox.end(), v, v + kVoxPerBlock);
+        std::memcpy(ch.block(i), v, kVoxPerBlock * sizeof(Voxel));
         ++n_blocks;
     }
 
@@ -562,7 +592,7 @@ int vsg_store_export(const vsg_block_store* st, int32_t* coords, uint8_t* voxels
     all.reserve(st->impl.n_blocks);
     for (const auto& kv : st->impl.chunks)
         for (size_t i = 0; i < kv.second.coords.size(); ++i)
-            all.push_back({kv.second.coords[i], kv.second.vox.data() + i * vsg::kVoxPerBlock});
+            all.push_back({kv.second.coords[i], kv.second.block(i)});
     std::sort(all.begin(), all.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
     for (size_t i = 0; i < all.size(); ++i) {
         coords[3 * i + 0] = all[i].first[0];
@@ -580,7 +610,7 @@ int vsg_store_save(const vsg_block_store* st, const char* path) {
     for (const auto& kv : st->impl.chunks)
         for (size_t i = 0; i < kv.second.coords.size(); ++i) {
             coords.push_back(kv.second.coords[i]);
-            vox.push_back(kv.second.vox.data() + i * vsg::kVoxPerBlock);
+            vox.push_back(kv.second.block(i));
         }
     return write_blocks(path, st->impl.voxel, coords, vox);
 }
@@ -656,7 +686,7 @@ int vsg_stream_in(vsg_scene* s, vsg_block_store* store, const float center[3], f
         const vsg::Chunk& ch = bs.chunks.at(ck);
         for (size_t i = 0; i < ch.coords.size(); ++i) {
             coords.push_back(ch.coords[i]);
-            vox.push_back(ch.vox.data() + i * vsg::kVoxPerBlock);
+            vox.push_back(ch.block(i));
         }
     }
     if (coords.empty()) return VSG_OK;
@@ -671,8 +701,7 @@ int vsg_stream_in(vsg_scene* s, vsg_block_store* store, const float center[3], f
     rc = vsg::insert_blocks(sc, coords, vox, st, &merged, &failed);
     if (rc != VSG_OK) return rc;
     for (const auto& ck : take) {
-        bs.n_blocks -= bs.chunks.at(ck).coords.size();
-        bs.chunks.erase(ck);
+        bs.erase_chunk(ck);
     }
     if (n_in) *n_in = (uint32_t)coords.size() - failed;
     if (n_merged) *n_merged = merged;
