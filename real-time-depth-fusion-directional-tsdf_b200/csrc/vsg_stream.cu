@@ -468,11 +468,21 @@ int insert_blocks(Scene* sc, const std::vector<std::array<int, 3>>& coords, cons
     uint32_t merged = 0, failed = 0;
     for (size_t done = 0; done < coords.size();) {
         const uint32_t n = (uint32_t)std::min<size_t>(kStageBlocks, coords.size() - done);
-        for (uint32_t i = 0; i < n; ++i) {
-            const auto& c = coords[done + i];
-            sg->h_info[i] = make_int4(c[0], c[1], c[2], -1);
-            std::memcpy(sg->h_vox + (size_t)i * kVoxPerBlock, vox[done + i], kVoxPerBlock * sizeof(Voxel));
-        }
+        // gather into the pinned staging, contiguous ranges over up to 8 host threads
+        auto gather = [&](uint32_t a, uint32_t b) {
+            for (uint32_t i = a; i < b; ++i) {
+                const auto& c = coords[done + i];
+                sg->h_info[i] = make_int4(c[0], c[1], c[2], -1);
+                std::memcpy(sg->h_vox + (size_t)i * kVoxPerBlock, vox[done + i], kVoxPerBlock * sizeof(Voxel));
+            }
+        };
+        const unsigned hw = std::thread::hardware_concurrency();
+        const unsigned nt = n < 512 ? 1u : std::min<unsigned>(hw ? hw : 1u, 8u);
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < nt; ++t) pool.emplace_back(gather, (uint32_t)((uint64_t)n * t / nt),
+                                                            (uint32_t)((uint64_t)n * (t + 1) / nt));
+        gather(0, (uint32_t)((uint64_t)n / nt));
+        for (auto& th : pool) th.join();
         if (cudaMemsetAsync(sg->d_ctr, 0, sizeof(StreamCounters), st) != cudaSuccess ||
             cudaMemcpyAsync(sg->d_info, sg->h_info, n * sizeof(int4), cudaMemcpyHostToDevice, st) != cudaSuccess ||
             cudaMemcpyAsync(sg->d_vox, sg->h_vox, (size_t)n * kVoxPerBlock * sizeof(Voxel), cudaMemcpyHostToDevice,
