@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-scans", type=int, default=64)
     ap.add_argument("--no-corridor", action="store_true")
+    ap.add_argument("--no-room", action="store_true")
     ap.add_argument("--corridor-frames", type=int, default=400)
     return ap.parse_args()
 
@@ -300,6 +301,8 @@ def run_ours(args):
     side("streaming", stream_measure, sc)
     side("adjoint", adjoint_measure, sc, frames, K)
     side("splat", splat_measure, frames, K, peak)
+    if not args.no_room:
+        side("room", room_measure, peak)
     if not args.no_e2e:
         line["e2e"] = e2e(args, frames, K, sc, rr)
     if not args.no_corridor:
@@ -438,6 +441,79 @@ def corridor_measure(n_frames: int, track_steps: int = 10, r_out: float = 4.0, r
     del frames
     torch.cuda.empty_cache()
     return res
+
+
+def room_measure(peak: float, n_frames: int = 30, reps: int = 3) -> dict:
+    """Room workload (1280x720, fx=fy=910, 2 mm voxels, truncation 0.01 m,
+    2^20 buckets and pool blocks; 4 x 3 x 2.5 m room with 40 boxes and 20
+    spheres, random-walk camera; frames generated on the device): the same
+    step as the headline (every frame integrated, then ray cast at its pose,
+    0.2-4.0 m) with the volume far beyond L2.  Frames/s over `reps` steps
+    (CUDA events), per-kernel device times and algorithmic bytes as for the
+    headline."""
+    import torch
+
+    import synth
+    import vsg
+
+    K = synth.ROOM_K
+    W, H = K.width, K.height
+    scene = synth.room_scene(1)
+    poses = synth.random_walk_poses(n_frames, 1)
+    frames = [synth.render_frame_torch(scene, K, P, seed=i, zmax=4.0, color_top=2.5) + (P.astype(np.float32),)
+              for i, P in enumerate(poses)]
+    sc = vsg.Scene(voxel_size=0.002, truncation=0.01, hash_num_slots=1 << 20, num_sdf_blocks=1 << 20)
+    rr = vsg.Renderer(W, H)
+
+    def step():
+        sc.reset()
+        for pm, rgb, nm, T in frames:
+            sc.integrate(pm, rgb, nm, W, H, 0.01, T, K.fx, K.fy, K.cx, K.cy)
+            rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, 4.0)
+
+    sc.timing(True)
+    sc.reset()
+    per = []
+    for pm, rgb, nm, T in frames:
+        sc.integrate(pm, rgb, nm, W, H, 0.01, T, K.fx, K.fy, K.cx, K.cy)
+        rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, 4.0)
+        per.append(sc.stats())
+    sc.timing(False)
+    step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    sc.timing(True)
+    sc.timing_reset()
+    step()
+    kms, kcnt = sc.timing_read()
+    sc.timing(False)
+    npx = W * H
+    upd = float(np.mean([p["frame_updated_blocks"] for p in per]))
+    new = float(np.mean([p["frame_new_blocks"] for p in per]))
+    vis = float(np.mean([p["frame_visible_blocks"] for p in per]))
+    n_ray = float(np.mean([p["render_blocks_read"] for p in per]))
+    alg = {"alloc": npx * 12 + new * 20 + vis * 16, "integrate": upd * 512 * 16 + npx * 15,
+           "render": n_ray * 512 * 5 + npx * (4 + 16 + 16 + 16)}
+    kern = {}
+    for i, nm in {0: "alloc", 1: "integrate", 2: "render"}.items():
+        kt = float(kms[i] / max(kcnt[i], 1))
+        gbs = alg[nm] / (kt * 1e-3) / 1e9
+        kern[nm] = {"ms_per_launch": kt, "alg_bytes": alg[nm], "achieved_gbs": gbs, "frac_of_peak": gbs / peak}
+    fps = n_frames * reps / (ms * 1e-3)
+    st = sc.stats()
+    sc.close()
+    rr.close()
+    del frames
+    torch.cuda.empty_cache()
+    return {"workload": f"room {n_frames}x1280x720, voxel 2mm, trunc 0.01m, 2^20 buckets/blocks",
+            "frames_per_s": fps, "mpix_per_s": fps * npx / 1e6, "blocks_end": st["allocated_blocks"],
+            "updated_blocks_per_frame": upd, "kernels": kern, "flags": st["flags"]}
 
 
 def splat_measure(frames, K, peak: float, reps: int = 10) -> dict:
