@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(256) k_batch_select(const BatchHeader* h, cons
     select_blocks(args[blockIdx.y], blockIdx.x * blockDim.x, gridDim.x * blockDim.x);
 }
 
-__global__ void __launch_bounds__(256) k_batch_integrate(const BatchHeader* h, const IntegArgs* args) {
+__global__ void __launch_bounds__(256, 4) k_batch_integrate(const BatchHeader* h, const IntegArgs* args) {
     if ((int)blockIdx.y >= h->n) return;
     integrate_work(args[blockIdx.y]);
 }

@@ -589,7 +589,7 @@ static __device__ __forceinline__ void select_blocks(const IntegArgs& a, uint32_
     }
 }
 
-constexpr int kIntegBatch = 8;  // voxels per lane with loads in flight together
+constexpr int kIntegBatch = 4;  // voxels per lane with loads in flight together
 
 // Per-voxel TSDF update, VoxelScene.cu:954-1126, for the 16 voxels lane
 // `lane` owns in block blk (idx = 32k + lane), in batches of kIntegBatch:
