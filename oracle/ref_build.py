@@ -12,8 +12,8 @@ MarchingCubes.cu with oracle/ref_shim.cu and a two-line OpenCV stand-in
                                   own, the semantics the oracle restates
 
 Nothing is copied out of the reference tree; the reference build system is
-not used.  Skipped when the reference checkout is absent (the GPU box uses
-the prebuilt files).
+not used.  Skipped when the reference checkout is absent (a machine without
+it uses the files built here).
 """
 from __future__ import annotations
 

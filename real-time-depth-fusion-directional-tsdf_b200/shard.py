@@ -6,7 +6,7 @@ scans -- shard by scan with no exchange on the data path: each rank fuses
 its own scans, and the only collectives are a barrier around the timed
 region, the maximum of the per-rank times, and an end-of-run gather of
 per-rank statistics.  These helpers are backend-agnostic (gloo on CPU for the
-tests, NCCL over NVLink on the GPU box).
+tests, NCCL over NVLink on GPUs).
 """
 from __future__ import annotations
 

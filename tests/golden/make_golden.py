@@ -135,4 +135,6 @@ def main(out_dir: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_golden.py OUT_DIR")
+    main(sys.argv[1])
