@@ -21,6 +21,8 @@
  *                         streamOut / streamIn, streamOutFindBlocksOnGPU,
  *                         streamOutCopyToChunkGrid, streamInCopyToGPUBuffer,
  *                         streamInInsertToHashTable
+ *   CustomDepthMapGenerator (CustomDepthMapGenerator.h:15-165): setCameraParams,
+ *                         setProjectionMethod, generateFromPointCloud
  * so that reference call sites compile unchanged against it.  Like the
  * reference, the methods print to stderr and return on bad input instead of
  * throwing; the only throw is GlobalParamsConfig::initialize.
@@ -35,6 +37,7 @@
 
 #include <cstdint>
 #include <iostream>
+#include <limits>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -542,4 +545,122 @@ private:
     float m_inRadius = 0.0f;
     bool m_inPending = false;
     unsigned int m_out = 0, m_in = 0;
+};
+
+/* CustomDepthMapGenerator (CustomDepthMapGenerator.h:15-165;
+ * generateFromPointCloud, CustomDepthMapGenerator.cpp:81-222): point cloud
+ * -> depth / point / normal / colour maps, computed on the GPU by
+ * vsg_splat_points in the reference's order (the last point landing on a
+ * pixel wins; a point's normal and colour are written only when it has
+ * one; without normals the depth-map fallback).  Points, normals and colours
+ * are any element types with .x/.y/.z (cv::Point3f) and operator[] (cv::Vec3b);
+ * the maps come back as std::array elements.  Only the perspective
+ * projection (PERSPECTIVE, CUSTOM_CAMERA) is implemented; ORTHOGRAPHIC
+ * prints an error and returns empty maps. */
+#include <array>
+
+class CustomDepthMapGenerator {
+public:
+    struct CameraParams {
+        float fx = 525.0f, fy = 525.0f, cx = 319.5f, cy = 239.5f;
+        float nearPlane = 0.1f, farPlane = 10.0f;
+        int width = 640, height = 480;
+    };
+    enum class ProjectionMethod { PERSPECTIVE, ORTHOGRAPHIC, CUSTOM_CAMERA };
+    struct GeneratedDepthMap {
+        std::vector<float> depthmap;                         // 0 = no point
+        std::vector<std::array<float, 3>> pointmap;          // camera space, 0 = no point
+        std::vector<std::array<float, 3>> normalmap;
+        std::vector<std::array<unsigned char, 3>> colormap;
+        int width = 0, height = 0;
+    };
+
+    void setCameraParams(const CameraParams& p) { m_cam = p; }
+    void setCameraParams(float fx, float fy, float cx, float cy, float nearPlane, float farPlane, int width,
+                         int height) {
+        m_cam.fx = fx;
+        m_cam.fy = fy;
+        m_cam.cx = cx;
+        m_cam.cy = cy;
+        m_cam.nearPlane = nearPlane;
+        m_cam.farPlane = farPlane;
+        m_cam.width = width;
+        m_cam.height = height;
+    }
+    const CameraParams& getCameraParams() const { return m_cam; }
+    void setProjectionMethod(ProjectionMethod m) { m_method = m; }
+    ProjectionMethod getProjectionMethod() const { return m_method; }
+
+    template <class P, class N, class C>
+    GeneratedDepthMap generateFromPointCloud(const std::vector<P>& points, const std::vector<N>& normals,
+                                             const std::vector<C>& colors) {
+        GeneratedDepthMap out;
+        out.width = m_cam.width;
+        out.height = m_cam.height;
+        if (m_method == ProjectionMethod::ORTHOGRAPHIC) {
+            std::cerr << "CustomDepthMapGenerator: only the perspective projection is implemented" << std::endl;
+            return out;
+        }
+        const size_t npx = (size_t)m_cam.width * (size_t)m_cam.height;
+        std::vector<float> hp(3 * points.size()), hn(3 * normals.size());
+        std::vector<unsigned char> hc(3 * colors.size());
+        for (size_t i = 0; i < points.size(); ++i) {
+            hp[3 * i] = points[i].x;
+            hp[3 * i + 1] = points[i].y;
+            hp[3 * i + 2] = points[i].z;
+        }
+        for (size_t i = 0; i < normals.size(); ++i) {
+            hn[3 * i] = normals[i].x;
+            hn[3 * i + 1] = normals[i].y;
+            hn[3 * i + 2] = normals[i].z;
+        }
+        for (size_t i = 0; i < colors.size(); ++i)
+            for (int k = 0; k < 3; ++k) hc[3 * i + k] = (unsigned char)colors[i][k];
+        float *dp = nullptr, *dn = nullptr, *dd = nullptr, *dpm = nullptr, *dnm = nullptr;
+        unsigned char *dc = nullptr, *dcm = nullptr;
+        bool ok = cudaMalloc(&dp, hp.size() * 4 + 4) == cudaSuccess &&
+                  cudaMalloc(&dn, hn.size() * 4 + 4) == cudaSuccess &&
+                  cudaMalloc(&dc, hc.size() + 4) == cudaSuccess && cudaMalloc(&dd, npx * 4) == cudaSuccess &&
+                  cudaMalloc(&dpm, npx * 12) == cudaSuccess && cudaMalloc(&dnm, npx * 12) == cudaSuccess &&
+                  cudaMalloc(&dcm, npx * 3) == cudaSuccess;
+        if (ok)
+            ok = cudaMemcpy(dp, hp.data(), hp.size() * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
+                 cudaMemcpy(dn, hn.data(), hn.size() * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
+                 cudaMemcpy(dc, hc.data(), hc.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+        int64_t nvalid = 0;
+        if (ok)
+            ok = vsg_splat_points(dp, (int64_t)points.size(), dn, (int64_t)normals.size(), dc, (int64_t)colors.size(),
+                                  m_cam.width, m_cam.height, m_cam.fx, m_cam.fy, m_cam.cx, m_cam.cy, 0.0f,
+                                  std::numeric_limits<float>::infinity(), VSG_SPLAT_LAST, dd, dpm, dnm, dcm,
+                                  &nvalid, nullptr) == VSG_OK;
+        if (ok) {
+            out.depthmap.resize(npx);
+            out.pointmap.resize(npx);
+            out.normalmap.resize(npx);
+            out.colormap.resize(npx);
+            ok = cudaMemcpy(out.depthmap.data(), dd, npx * 4, cudaMemcpyDeviceToHost) == cudaSuccess &&
+                 cudaMemcpy(out.pointmap.data(), dpm, npx * 12, cudaMemcpyDeviceToHost) == cudaSuccess &&
+                 cudaMemcpy(out.normalmap.data(), dnm, npx * 12, cudaMemcpyDeviceToHost) == cudaSuccess &&
+                 cudaMemcpy(out.colormap.data(), dcm, npx * 3, cudaMemcpyDeviceToHost) == cudaSuccess;
+        }
+        cudaFree(dp);
+        cudaFree(dn);
+        cudaFree(dc);
+        cudaFree(dd);
+        cudaFree(dpm);
+        cudaFree(dnm);
+        cudaFree(dcm);
+        if (!ok) {
+            std::cerr << "CustomDepthMapGenerator: point cloud splat failed" << std::endl;
+            out.depthmap.clear();
+            out.pointmap.clear();
+            out.normalmap.clear();
+            out.colormap.clear();
+        }
+        return out;
+    }
+
+private:
+    CameraParams m_cam;
+    ProjectionMethod m_method = ProjectionMethod::PERSPECTIVE;
 };

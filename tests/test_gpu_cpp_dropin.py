@@ -68,3 +68,44 @@ def test_cpp_dropin_matches_binding(cuda, synth_mod, tmp_path, method):
     assert f"streamed_in={n_out} " in r.stdout
     after = np.fromfile(os.path.join(d, "depth_after_stream.bin"), np.float32).reshape(H, W)
     assert np.array_equal(after.view(np.uint32), ref.view(np.uint32))
+
+
+def test_cpp_depth_map_generator_matches_binding(cuda, synth_mod, tmp_path):
+    """CustomDepthMapGenerator from the C++ header (generateFromPointCloud's
+    call shape, CustomDepthMapGenerator.cpp:81-222) gives the maps of
+    vsg.splat_points in the reference's last-point-wins order, bit for bit,
+    with a shorter normal list and no colours."""
+    import vsg
+
+    fr, K = synth_mod.tabletop_stream(5, 2, 320, 240)
+    T0 = np.asarray(fr[0].pose, np.float64)
+    pts, nrm, col = [], [], []
+    for f in fr:
+        m = np.any(f.pointmap != 0, -1)
+        M = np.linalg.inv(T0) @ np.asarray(f.pose, np.float64)
+        pts.append((f.pointmap[m].astype(np.float64) @ M[:3, :3].T + M[:3, 3]).astype(np.float32))
+        nrm.append((f.normals[m].astype(np.float64) @ M[:3, :3].T).astype(np.float32))
+        col.append(f.rgb[m])
+    P = np.concatenate(pts)
+    N = np.concatenate(nrm)[: len(P) * 2 // 3]
+    d = str(tmp_path)
+    P.tofile(os.path.join(d, "points.bin"))
+    N.tofile(os.path.join(d, "normals.bin"))
+    open(os.path.join(d, "colors.bin"), "wb").close()
+    exe = os.path.join(d, "splat_cloud")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", exe, os.path.join(ROOT, "tests", "cpp", "splat_cloud.cpp"),
+                    "-I", os.path.join(ROOT, "include"), "-I", f"{CUDA}/include", "-L", PKG, "-lvsg",
+                    f"-Wl,-rpath,{PKG}", "-L", f"{CUDA}/lib64", "-lcudart"], check=True)
+    r = subprocess.run([exe, d, str(len(P)), str(len(N)), "0", str(K.width), str(K.height), str(K.fx), str(K.fy),
+                        str(K.cx), str(K.cy)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    want = vsg.splat_points(cuda.from_numpy(P).cuda(), K.width, K.height, K.fx, K.fy, K.cx, K.cy,
+                            normals=cuda.from_numpy(N).cuda())
+    H, W = K.height, K.width
+    got = {"depth": np.fromfile(os.path.join(d, "depth.bin"), np.float32).reshape(H, W),
+           "pointmap": np.fromfile(os.path.join(d, "pointmap.bin"), np.float32).reshape(H, W, 3),
+           "normalmap": np.fromfile(os.path.join(d, "normalmap.bin"), np.float32).reshape(H, W, 3),
+           "colormap": np.fromfile(os.path.join(d, "colormap.bin"), np.uint8).reshape(H, W, 3)}
+    for k, g in got.items():
+        assert np.array_equal(g.view(np.uint8), want[k].cpu().numpy().view(np.uint8)), k
+    assert want["n_valid"] > 0.5 * W * H and not got["colormap"].any()
