@@ -9,7 +9,9 @@
  *                         truncation fields, CUDAHashData.h:27-28)
  *   VoxelScene           (VoxelScene.h:51-209): constructor, reset,
  *                         integrateFromScanData, getNumIntegratedFrames,
- *                         isAllocated, getParams, getHeapFreeCount
+ *                         isAllocated, getParams, getHeapFreeCount,
+ *                         compactifyHashEntries, printStats, saveToMesh,
+ *                         getOutputDirectory
  *   RayCastRender        (RayCastRender.h:20-124): initialize, render,
  *                         downloadResults, downloadDepthFloat, savePointCloudPLY,
  *                         getOutputDepth/Color/Normal/Positions,
@@ -36,6 +38,7 @@
 #include <vector_types.h>
 
 #include <cstdint>
+#include <cstdio>
 #include <iostream>
 #include <limits>
 #include <stdexcept>
@@ -228,6 +231,62 @@ public:
         return st.free_blocks;
     }
     bool isAllocated() const { return m_scene != nullptr; }
+    /* VoxelScene.h:97: the reference lists every allocated block here;
+     * vsg_integrate selects the blocks a frame can touch itself, so there is
+     * nothing to do between frames. */
+    void compactifyHashEntries() {}
+    /* VoxelScene.cpp:380-398 */
+    void printStats() const {
+        std::cout << "\n=== VoxelScene Stats ===" << std::endl;
+        std::cout << "Hash Slots: " << m_params.hashSlotNum << std::endl;
+        std::cout << "Bucket Size: " << m_params.slotSize << std::endl;
+        std::cout << "Total Hash Entries: " << m_params.totalHashSize << std::endl;
+        std::cout << "SDF Blocks: " << m_params.SDFBlockNum << std::endl;
+        std::cout << "Block Size: " << m_params.SDFBlockSize << "x" << m_params.SDFBlockSize << "x"
+                  << m_params.SDFBlockSize << std::endl;
+        std::cout << "Total Voxels: " << m_params.totalBlockSize << std::endl;
+        std::cout << "Integrated Frames: " << getNumIntegratedFrames() << std::endl;
+        if (m_scene) {
+            const unsigned int freeCount = getHeapFreeCount();
+            std::cout << "Free Blocks: " << freeCount << " / " << m_params.SDFBlockNum << " ("
+                      << (freeCount * 100.0 / (m_params.SDFBlockNum ? m_params.SDFBlockNum : 1)) << "%)"
+                      << std::endl;
+        }
+        std::cout << "========================\n" << std::endl;
+    }
+    /* VoxelScene.cpp:838-845 is a stub that returns false.  Here: marching
+     * cubes over the scene (iso 0, up to maxTriangles) written as an ASCII PLY
+     * mesh (vertices, then faces of three consecutive vertices); false when
+     * the scene is empty, the file cannot be written or a call fails. */
+    bool saveToMesh(const std::string& filename, int maxTriangles = 4000000) {
+        if (!m_scene || maxTriangles <= 0) return false;
+        vsg_mc_output* mc = nullptr;
+        if (vsg_mc_output_create(maxTriangles, &mc) != VSG_OK) return false;
+        bool ok = vsg_mc_run(m_scene, mc, 0.0f, m_params.voxelSize, nullptr) == VSG_OK;
+        int64_t n = 0;
+        std::vector<float> v, nrm;
+        if (ok) ok = vsg_mc_download(mc, nullptr, nullptr, &n) == VSG_OK;
+        const int64_t k = n < maxTriangles ? n : maxTriangles;
+        if (ok && k > 0) {
+            v.resize((size_t)k * 9);
+            nrm.resize((size_t)k * 9);
+            ok = vsg_mc_download(mc, v.data(), nrm.data(), &n) == VSG_OK;
+        }
+        vsg_mc_output_destroy(mc);
+        if (!ok || k <= 0) return false;
+        FILE* f = std::fopen(filename.c_str(), "w");
+        if (!f) return false;
+        std::fprintf(f, "ply\nformat ascii 1.0\nelement vertex %lld\nproperty float x\nproperty float y\n"
+                        "property float z\nelement face %lld\nproperty list uchar int vertex_indices\nend_header\n",
+                     (long long)(3 * k), (long long)k);
+        for (int64_t i = 0; i < 3 * k; ++i) std::fprintf(f, "%g %g %g\n", v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+        for (int64_t t = 0; t < k; ++t)
+            std::fprintf(f, "3 %lld %lld %lld\n", (long long)(3 * t), (long long)(3 * t + 1), (long long)(3 * t + 2));
+        return std::fclose(f) == 0;
+    }
+    /* VoxelScene.h:148: the reference's per-run log directory; logs are not
+     * written here, so this is the current directory. */
+    std::string getOutputDirectory() const { return "."; }
     Params& getParams() { return m_params; }
     const Params& getParams() const { return m_params; }
     vsg_scene* handle() const { return m_scene; }

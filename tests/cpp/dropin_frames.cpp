@@ -98,6 +98,9 @@ int main(int argc, char** argv) {
     runMarchingCubesCUDA(scene.getHashData(), scene.getParams(), mcParams, mcOut);
     std::printf("triangles=%d\n", copyMarchingCubesTriangleCount(mcOut));
     freeMarchingCubesOutput(mcOut);
+    scene.compactifyHashEntries();
+    scene.printStats();
+    if (!scene.saveToMesh(dir + "/mesh.ply")) return 10;
     // stream far blocks out, then everything back in, and render the last pose again
     VoxelStreamingManager streaming(scene, params, vec3f(0.1f, 0.1f, 0.1f), vec3i(513, 513, 513),
                                     vec3i(-256, -256, -256), 2000, false);

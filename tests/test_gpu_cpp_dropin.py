@@ -63,6 +63,9 @@ def test_cpp_dropin_matches_binding(cuda, synth_mod, tmp_path, method):
     mc = vsg.MarchingCubes(250000)
     mc.run(sc, voxel_size=0.004)
     assert f"triangles={min(mc.count(), 2**31 - 1)}" in r.stdout
+    assert f"Integrated Frames: {N}" in r.stdout
+    head = (tmp_path / "mesh.ply").read_text().splitlines()[:10]
+    assert f"element vertex {3 * mc.count()}" in head and f"element face {mc.count()}" in head
     n_out = sc.stream_out(vsg.Store((0.1, 0.1, 0.1)), (0.0, 0.1, 0.0), 0.25)
     assert n_out > 0 and f"streamed_out={n_out} " in r.stdout
     assert f"streamed_in={n_out} " in r.stdout
