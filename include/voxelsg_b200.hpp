@@ -37,6 +37,8 @@
 #include <cuda_runtime.h>
 #include <vector_types.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <iostream>
@@ -522,10 +524,20 @@ public:
                           const vec3i& gridDimensions, const vec3i& minGridPos, unsigned int initialChunkListSize,
                           bool streamingEnabled)
         : m_scene(&sceneHashRef), m_params(params) {
-        (void)gridDimensions;
-        (void)minGridPos;
+        initialize(voxelExtends, gridDimensions, minGridPos, initialChunkListSize, streamingEnabled);
+    }
+    /* VoxelStreamingManager.cpp:136-166: a fresh, empty chunk grid.  The
+     * store has no grid bounds; the dimensions only serve the chunk helpers
+     * below. */
+    void initialize(const vec3f& voxelExtends, const vec3i& gridDimensions, const vec3i& minGridPos,
+                    unsigned int initialChunkListSize, bool streamingEnabled) {
         (void)initialChunkListSize;
         (void)streamingEnabled;
+        if (m_store) vsg_store_destroy(m_store);
+        m_store = nullptr;
+        m_ext = voxelExtends;
+        m_dims = gridDimensions;
+        m_min = minGridPos;
         const float e[3] = {voxelExtends.x, voxelExtends.y, voxelExtends.z};
         if (vsg_store_create(e, &m_store) != VSG_OK) {
             std::cerr << "VoxelStreamingManager: invalid chunk extents" << std::endl;
@@ -538,8 +550,12 @@ public:
     VoxelStreamingManager(const VoxelStreamingManager&) = delete;
     VoxelStreamingManager& operator=(const VoxelStreamingManager&) = delete;
 
+    /* the calls below are synchronous: no auxiliary thread, no critical section */
     void startMultiThreading() {}
     void stopMultiThreading() {}
+    void startAuxiliaryThread() {}
+    void initializeCriticalSection() {}
+    void deleteCriticalSection() {}
 
     void streamOut(VoxelScene& scene, const float3& cameraPos, float radius) {
         m_scene = &scene;
@@ -571,9 +587,17 @@ public:
         m_inRadius = radius;
         m_inPending = true;
     }
+    /* Takes the chunks chosen by the last streamInCopyToGPUBuffer, or, as
+     * the reference's auxiliary thread would choose them, those around
+     * posCamera_ within radius_ (voxelSG.cpp:528-551). */
     void streamInInsertToHashTable(bool multiThreaded) {
         (void)multiThreaded;
-        if (!ready() || !m_inPending) return;
+        if (!ready()) return;
+        if (!m_inPending) {
+            if (!(radius_ > 0.0f)) return;
+            m_inCenter = posCamera_;
+            m_inRadius = radius_;
+        }
         m_inPending = false;
         const float c[3] = {m_inCenter.x, m_inCenter.y, m_inCenter.z};
         uint32_t n = 0, merged = 0;
@@ -588,6 +612,76 @@ public:
     unsigned int getNumStreamedOut() const { return m_out; }
     unsigned int getNumStreamedIn() const { return m_in; }
     vsg_block_store* store() const { return m_store; }
+
+    /* VoxelStreamingManager.cpp:836-903: file blocks given as the streaming
+     * records (SDFBlockInfo array, SDFBlock array of 12-byte VoxelData). */
+    void updateChunkGrid(const int* blockInfos, const int* blocks, unsigned int nSDFBlocks) {
+        if (!m_store) return;
+        if (vsg_store_add_records(m_store, m_params.voxelSize, reinterpret_cast<const int32_t*>(blockInfos),
+                                  reinterpret_cast<const uint8_t*>(blocks), nSDFBlocks) != VSG_OK)
+            std::cerr << "VoxelStreamingManager: updateChunkGrid failed" << std::endl;
+    }
+    /* VoxelStreamingManager.cpp:993-1140: the number of stored blocks a
+     * stream-in around posCamera within radius takes (no chunk-grid bounds). */
+    unsigned int streamInFindChunk(const vec3f& posCamera, float radius, bool useParts) {
+        (void)useParts;
+        uint64_t nb = 0;
+        const float c[3] = {posCamera.x, posCamera.y, posCamera.z};
+        if (!m_store || vsg_store_count(m_store, c, radius, &nb, nullptr) != VSG_OK) nb = 0;
+        m_counter = (unsigned int)nb;
+        return m_counter;
+    }
+    void clearSDFBlockCounter() { m_counter = 0; }
+    unsigned int getSDFBlockCounter() const { return m_counter; }
+
+    /* chunk helpers, VoxelStreamingManager.cpp:194-212, 905-991 */
+    vec3i worldToChunks(const vec3f& posWorld) const {
+        const float p[3] = {posWorld.x / m_ext.x, posWorld.y / m_ext.y, posWorld.z / m_ext.z};
+        int c[3];
+        for (int i = 0; i < 3; ++i) {
+            const float s = p[i] > 0.0f ? 1.0f : (p[i] < 0.0f ? -1.0f : 0.0f);
+            c[i] = static_cast<int>(p[i] + s * 0.5f);
+        }
+        return vec3i(c[0], c[1], c[2]);
+    }
+    bool isValidChunk(const vec3i& chunk) const {
+        return chunk.x >= m_min.x && chunk.y >= m_min.y && chunk.z >= m_min.z && chunk.x < m_min.x + m_dims.x &&
+               chunk.y < m_min.y + m_dims.y && chunk.z < m_min.z + m_dims.z;
+    }
+    unsigned int linearizeChunkPos(const vec3i& chunkPos) const {
+        return (unsigned int)((chunkPos.z - m_min.z) * m_dims.x * m_dims.y + (chunkPos.y - m_min.y) * m_dims.x +
+                              (chunkPos.x - m_min.x));
+    }
+    vec3i delinearizeChunkIndex(unsigned int idx) const {
+        const unsigned int dx = (unsigned int)m_dims.x, dxy = (unsigned int)(m_dims.x * m_dims.y);
+        return vec3i(m_min.x + (int)(idx % dx), m_min.y + (int)((idx % dxy) / dx), m_min.z + (int)(idx / dxy));
+    }
+    vec3i meterToNumberOfChunksCeil(float radius) const {
+        return vec3i((int)std::ceil(radius / m_ext.x), (int)std::ceil(radius / m_ext.y), (int)std::ceil(radius / m_ext.z));
+    }
+    bool isChunkInSphere(const vec3i& chunk, const vec3f& center, float radius) const {
+        const float wx = chunk.x * m_ext.x, wy = chunk.y * m_ext.y, wz = chunk.z * m_ext.z;
+        const float ext = std::max(std::max(m_ext.x, m_ext.y), m_ext.z);
+        const float r = 0.5f * ext * std::sqrt(3.0f);
+        const float dx = wx - center.x, dy = wy - center.y, dz = wz - center.z;
+        return std::sqrt(dx * dx + dy * dy + dz * dz) - r <= radius;
+    }
+    bool isInsideRadius(const float3& blockWorldCenter, const float3& cameraPos, float radius) const {
+        const float dx = blockWorldCenter.x - cameraPos.x, dy = blockWorldCenter.y - cameraPos.y,
+                    dz = blockWorldCenter.z - cameraPos.z;
+        return dx * dx + dy * dy + dz * dz <= radius * radius;
+    }
+    float3 blockCoordToWorld(const int3& blockCoord) const {
+        const float s = (float)SDF_BLOCK_SIZE * m_params.voxelSize;
+        return make_float3(blockCoord.x * s, blockCoord.y * s, blockCoord.z * s);
+    }
+
+    /* runtime fields the reference's main loop sets (VoxelStreamingManager.h:287-292) */
+    vec3f posCamera_;
+    float radius_ = 0.0f;
+    bool s_terminateThread = false;
+    unsigned int m_frameNumber = 0;
+    std::string m_outputDirectory;
 
 private:
     bool ready() const {
@@ -604,6 +698,9 @@ private:
     float m_inRadius = 0.0f;
     bool m_inPending = false;
     unsigned int m_out = 0, m_in = 0;
+    unsigned int m_counter = 0;
+    vec3f m_ext;
+    vec3i m_dims, m_min;
 };
 
 /* CustomDepthMapGenerator (CustomDepthMapGenerator.h:15-165;

@@ -410,6 +410,20 @@ VSG_API int vsg_store_export(const vsg_block_store* st, int32_t* coords, uint8_t
  * 30-76) after a 32-byte header; load merges the file into the store. */
 VSG_API int vsg_store_save(const vsg_block_store* st, const char* path);
 VSG_API int vsg_store_load(vsg_block_store* st, const char* path);
+/* How many stored blocks (in how many chunks) a vsg_stream_in with this
+ * centre and radius would take (VoxelStreamingManager::streamInFindChunk,
+ * VoxelStreamingManager.cpp:993-1140, which returns the block count);
+ * radius < 0: everything stored. */
+VSG_API int vsg_store_count(const vsg_block_store* st, const float center[3], float radius, uint64_t* n_blocks,
+                            uint64_t* n_chunks);
+/* File n host blocks given in the reference's streaming records
+ * (VoxelStreamingManager::updateChunkGrid, VoxelStreamingManager.cpp:836-903):
+ * infos = n SDFBlockInfo {int3 pos, int ptr} (4 int32 each), voxels = n
+ * SDFBlock of 512 12-byte VoxelData {uchar3 colour, uchar weight, float sdf,
+ * 2 flag bytes, 2 pad}; blocks already stored merge as in stream-out.
+ * voxel_size must match the blocks already held. */
+VSG_API int vsg_store_add_records(vsg_block_store* st, float voxel_size, const int32_t* infos,
+                                  const uint8_t* voxels, uint64_t n);
 /* Move every block whose corner lies at distance >= radius from center into
  * the store (deleted from the scene, pool blocks freed). */
 VSG_API int vsg_stream_out(vsg_scene* s, vsg_block_store* st, const float center[3], float radius, uint32_t* n_out,

@@ -655,6 +655,33 @@ int vsg_store_info(const vsg_block_store* st, uint64_t* n_blocks, uint64_t* n_ch
     return VSG_OK;
 }
 
+int vsg_store_count(const vsg_block_store* st, const float center[3], float radius, uint64_t* n_blocks,
+                    uint64_t* n_chunks) {
+    if (!st || (!center && radius >= 0.0f)) return VSG_ERR_INVALID_ARG;
+    const float zero[3] = {0.0f, 0.0f, 0.0f};
+    const std::vector<std::array<int, 3>> take = st->impl.chunks_for(center ? center : zero, radius);
+    uint64_t nb = 0;
+    for (const auto& ck : take) nb += st->impl.chunks.at(ck).coords.size();
+    if (n_blocks) *n_blocks = nb;
+    if (n_chunks) *n_chunks = take.size();
+    return VSG_OK;
+}
+
+int vsg_store_add_records(vsg_block_store* st, float voxel_size, const int32_t* infos, const uint8_t* voxels,
+                          uint64_t n) {
+    if (!st || !(voxel_size > 0.0f) || (n && (!infos || !voxels))) return VSG_ERR_INVALID_ARG;
+    if (n == 0) return VSG_OK;
+    if (st->impl.n_blocks && st->impl.voxel != voxel_size) return VSG_ERR_INVALID_ARG;
+    st->impl.voxel = voxel_size;
+    std::vector<vsg::Voxel> blk(vsg::kVoxPerBlock);
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint8_t* src = voxels + i * (uint64_t)vsg::kVoxPerBlock * 12u;
+        for (int v = 0; v < vsg::kVoxPerBlock; ++v) blk[v] = from_ref_voxel(src + 12 * v);
+        st->impl.add(infos[4 * i], infos[4 * i + 1], infos[4 * i + 2], blk.data(), voxel_size);
+    }
+    return VSG_OK;
+}
+
 int vsg_store_export(const vsg_block_store* st, int32_t* coords, uint8_t* voxels, uint64_t max_blocks,
                      uint64_t* n_out) {
     if (!st || !n_out) return VSG_ERR_INVALID_ARG;

@@ -32,7 +32,7 @@ EXPORTS = [
     "vsg_mc_output_create", "vsg_mc_output_destroy", "vsg_mc_run", "vsg_mc_triangle_count",
     "vsg_mc_output_buffers", "vsg_mc_download",
     "vsg_store_create", "vsg_store_destroy", "vsg_store_info", "vsg_store_export", "vsg_store_save",
-    "vsg_store_load", "vsg_stream_out", "vsg_stream_in", "vsg_scene_save", "vsg_scene_load",
+    "vsg_store_load", "vsg_store_count", "vsg_store_add_records", "vsg_stream_out", "vsg_stream_in", "vsg_scene_save", "vsg_scene_load",
     "vsg_points_create", "vsg_points_destroy", "vsg_extract_points", "vsg_points_count", "vsg_points_buffers",
     "vsg_points_download", "vsg_points_save_ply",
     "vsg_renderer_record", "vsg_render_backward", "vsg_render_normals", "vsg_scene_lookup_blocks",
@@ -127,6 +127,8 @@ def lib() -> ctypes.CDLL:
         L.vsg_store_export.argtypes = [_P, _P, _P, ctypes.c_uint64, _u64p]
         L.vsg_store_save.argtypes = [_P, ctypes.c_char_p]
         L.vsg_store_load.argtypes = [_P, ctypes.c_char_p]
+        L.vsg_store_count.argtypes = [_P, _P, _F, _u64p, _u64p]
+        L.vsg_store_add_records.argtypes = [_P, _F, _P, _P, ctypes.c_uint64]
         L.vsg_stream_out.argtypes = [_P, _P, _P, _F, _u32p, _P]
         L.vsg_stream_in.argtypes = [_P, _P, _P, _F, _u32p, _u32p, _P]
         L.vsg_scene_save.argtypes = [_P, ctypes.c_char_p]
@@ -636,6 +638,22 @@ class Store:
 
     def load(self, path: str):
         check("vsg_store_load", self.L.vsg_store_load(self.h, str(path).encode()))
+
+    def count(self, center=None, radius: float = -1.0) -> tuple[int, int]:
+        """(blocks, chunks) a stream-in with this centre and radius would take."""
+        c = np.ascontiguousarray(np.asarray(center if center is not None else (0, 0, 0), np.float32).reshape(3))
+        nb, nc = ctypes.c_uint64(), ctypes.c_uint64()
+        check("vsg_store_count", self.L.vsg_store_count(self.h, _hptr(c), _F(radius), ctypes.byref(nb),
+                                                        ctypes.byref(nc)))
+        return int(nb.value), int(nc.value)
+
+    def add_records(self, voxel_size: float, infos, ref_voxels):
+        """File blocks given in the reference's records: infos (n,4) int32
+        {x, y, z, ptr}, ref_voxels (n, 512*12) uint8 VoxelData."""
+        infos = np.ascontiguousarray(infos, np.int32).reshape(-1, 4)
+        ref_voxels = np.ascontiguousarray(ref_voxels, np.uint8).reshape(len(infos), -1)
+        check("vsg_store_add_records", self.L.vsg_store_add_records(self.h, _F(voxel_size), _hptr(infos),
+                                                                    _hptr(ref_voxels), len(infos)))
 
 
 class SurfacePoints:

@@ -108,3 +108,43 @@ def test_store_rejects_bad_files(tmp_path):
         st.load(str(tmp_path / "missing.vsgb"))
     with pytest.raises(vsg.VsgError):
         vsg.Store((0.0, 1.0, 1.0))
+
+
+def test_store_records_and_counts(oracle_mod):
+    """vsg_store_add_records files the reference's streaming records like a
+    checkpoint file does (merging repeats), and vsg_store_count reports the
+    blocks and chunks a stream-in would take, as the oracle's chunk grid
+    (ChunkStore.take) chooses them."""
+    import vsg
+
+    rng = np.random.default_rng(8)
+    coords, vox = _blocks(rng, 300)
+    rec = np.zeros((len(coords), 512, 12), np.uint8)
+    v = vox.reshape(len(coords), 512, 8)
+    rec[:, :, 0:3] = v[:, :, 4:7]
+    rec[:, :, 3] = v[:, :, 7]
+    rec[:, :, 4:8] = v[:, :, 0:4]
+    infos = np.concatenate([coords, -np.ones((len(coords), 1), np.int32)], 1)
+    ext = (0.5, 0.5, 0.5)
+    st = vsg.Store(ext)
+    st.add_records(0.004, infos, rec.reshape(len(coords), -1))
+    gc, gv = st.export()
+    order = np.lexsort((coords[:, 2], coords[:, 1], coords[:, 0]))
+    assert np.array_equal(gc, coords[order]) and np.array_equal(gv, vox[order])
+    # the same records again merge voxel by voxel
+    st.add_records(0.004, infos, rec.reshape(len(coords), -1))
+    oc = oracle_mod.ChunkStore(0.004, ext)
+    oc.add(coords, vox)
+    oc.add(coords, vox)
+    _, gv2 = st.export()
+    _, ov2 = oc.export()
+    assert np.array_equal(gv2, ov2)
+    for center, radius in (((0.0, 0.0, 0.0), 1.0), ((0.5, -0.3, 0.2), 2.5), ((5.0, 5.0, 5.0), 0.5)):
+        nb, nc = st.count(center, radius)
+        fresh = oracle_mod.ChunkStore(0.004, ext)  # take() removes what it returns
+        fresh.add(coords, vox)
+        tc, _ = fresh.take(center, radius)
+        assert nb == len(tc), (center, radius)
+    assert st.count(None, -1.0)[0] == len(coords)
+    with pytest.raises(vsg.VsgError):
+        st.add_records(0.008, infos[:1], rec[:1].reshape(1, -1))
