@@ -107,8 +107,12 @@ int main(int argc, char** argv) {
     streaming.streamOutFindBlocksOnGPU(vec3f(0.0f, 0.1f, 0.0f), 0.25f, false, false);
     streaming.streamOutCopyToChunkGrid(false);
     std::printf("streamed_out=%u free=%u\n", streaming.getNumStreamedOut(), scene.getHeapFreeCount());
-    streaming.streamInCopyToGPUBuffer(vec3f(0.0f, 0.1f, 0.0f), 100.0f, false, false);
-    streaming.streamInInsertToHashTable(false);
+    // stream-in as the reference's main loop drives it: the sphere in
+    // posCamera_ / radius_, then the insert (voxelSG.cpp:528-551)
+    std::printf("found=%u\n", streaming.streamInFindChunk(vec3f(0.0f, 0.1f, 0.0f), 100.0f, false));
+    streaming.posCamera_ = vec3f(0.0f, 0.1f, 0.0f);
+    streaming.radius_ = 100.0f;
+    streaming.streamInInsertToHashTable(true);
     std::printf("streamed_in=%u free=%u\n", streaming.getNumStreamedIn(), scene.getHeapFreeCount());
     {
         vsg::Mat4f T;

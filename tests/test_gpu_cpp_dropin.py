@@ -68,7 +68,7 @@ def test_cpp_dropin_matches_binding(cuda, synth_mod, tmp_path, method):
     assert f"element vertex {3 * mc.count()}" in head and f"element face {mc.count()}" in head
     n_out = sc.stream_out(vsg.Store((0.1, 0.1, 0.1)), (0.0, 0.1, 0.0), 0.25)
     assert n_out > 0 and f"streamed_out={n_out} " in r.stdout
-    assert f"streamed_in={n_out} " in r.stdout
+    assert f"found={n_out}" in r.stdout and f"streamed_in={n_out} " in r.stdout
     after = np.fromfile(os.path.join(d, "depth_after_stream.bin"), np.float32).reshape(H, W)
     assert np.array_equal(after.view(np.uint32), ref.view(np.uint32))
 
