@@ -86,28 +86,137 @@ struct vec3i {
     vec3i() = default;
     vec3i(int a, int b, int c) : x(a), y(b), z(c) {}
 };
+struct vec4f {
+    float x = 0.0f, y = 0.0f, z = 0.0f, w = 0.0f;
+    vec4f() = default;
+    vec4f(float a, float b, float c, float d) : x(a), y(b), z(c), w(d) {}
+};
 #endif
 
 /* The knobs the fusion path reads, with the reference's code defaults. */
 class GlobalParamsConfig {
 public:
+    /* Every knob of globalPramasConfig.h:55-170 with the defaults of
+     * globalParamasConfig.cpp:8-402.  The fusion path reads the SDF, hash,
+     * marching-cubes and streaming knobs; the sensor, texture, rendering,
+     * tracking and recording knobs belong to parts of the reference outside
+     * this library and are kept only so that code setting them compiles. */
+    std::string g_data_name;
+    unsigned int g_sensorIdx = 0;
+    std::string g_sceneName;
+    std::string g_binaryDumpSensorFile0;
+    unsigned int g_optimizationIdx = 0;
+    int g_gain = 1;
+    int g_exposure = 200;
+    bool g_autoExposureEnabled = false;
+    bool g_autoWhiteBalanceEnabled = false;
+    bool g_renderToFile = false;
+    bool g_voxelRenderingEnabled = false;
+    unsigned int g_texKeyFrames = 4;
+    int g_nVideoFrame = 900;
+    int g_startFrame = 0;
+    unsigned int g_texPoolPatchWidth = 4;
+    unsigned int g_texPoolNumPatches = 1000000;
+    unsigned int g_numTextureTileWidth = 1024;
+    unsigned int g_texIntegrationWeightMax = 255;
+    unsigned int g_texIntegrationWeightSample = 30;
+    float g_erodeSigmaStretch = 2.0f;
+    unsigned int g_erodeIterStretchBox = 0;
+    unsigned int g_erodeIterStretchGauss = 0;
+    unsigned int g_erodeIterOccDepth = 6;
+    float g_texAngleThreshold_depth = 0.05f;
+    float g_texAngleThreshold_update = 0.5f;
+    float g_screenBoundaryWidth = 40.0f;
+    float g_sigmaAngle = 0.5f;
+    float g_sigmaDepth = 0.5f;
+    float g_sigmaArea = 1.0f;
+    unsigned int g_windowWidth = 640;
+    unsigned int g_windowHeight = 480;
+    unsigned int g_adapterWidth = 640;
+    unsigned int g_adapterHeight = 480;
+    float g_sensorDepthMax = 3.0f;
+    float g_sensorDepthMin = 0.4f;
+    bool g_enableColorCropping = false;
+    unsigned int g_colorCropX = 320;
+    unsigned int g_colorCropY = 272;
+    unsigned int g_colorCropWidth = 640;
+    unsigned int g_colorCropHeight = 480;
     float g_SDFVoxelSize = 0.1f;          /* globalParamasConfig.cpp:28 */
+    float g_SDFMarchingCubeThreshFactor = 10.0f;
     float g_SDFTruncation = 0.25f;        /* :38 */
     float g_SDFTruncationScale = 0.01f;   /* :44 */
     float g_SDFMaxIntegrationDistance = 3.0f;
+    unsigned int g_SDFIntegrationWeightSample = 3;
     unsigned int g_SDFIntegrationWeightMax = 255;
     unsigned int g_hashNumSlots = 10000;  /* :61 */
     unsigned int g_hashNumSDFBlocks = 10000; /* :65 */
+    unsigned int g_hashMaxCollisionLinkedListSize = 5;
     unsigned int g_hashSlotSize = HASH_BUCKET_SIZE;
     unsigned int g_hashNumBuckets = 10000; /* = g_hashNumSlots, :74 */
     float g_SDFRayIncrementFactor = 0.8f;
+    float g_SDFRayThresSampleDistFactor = 50.5f;
+    float g_SDFRayThresDistFactor = 50.0f;
+    bool g_SDFUseGradients = false;
+    bool g_binaryDumpSensorUseTrajectory = false;
+    bool g_binaryDumpSensorUseTrajectoryOnlyInit = false;
+    float g_depthSigmaD = 2.0f;
+    float g_depthSigmaR = 0.1f;
+    bool g_depthFilter = true;
+    float g_colorSigmaD = 1.0f;
+    float g_colorSigmaR = 0.08f;
+    bool g_colorFilter = false;
+    vec4f g_materialAmbient = vec4f(0.75f, 0.65f, 0.5f, 1.0f);
+    vec4f g_materialSpecular = vec4f(1.0f, 1.0f, 1.0f, 1.0f);
+    vec4f g_materialDiffuse = vec4f(1.0f, 0.9f, 0.7f, 1.0f);
+    float g_materialShininess = 16.0f;
+    vec4f g_lightAmbient = vec4f(0.4f, 0.4f, 0.4f, 1.0f);
+    vec4f g_lightDiffuse = vec4f(0.6f, 0.52944f, 0.4566f, 0.6f);
+    vec4f g_lightSpecular = vec4f(0.3f, 0.3f, 0.3f, 1.0f);
+    vec3f g_lightDirection = vec3f(0.0f, -1.0f, 2.0f);
+    unsigned int g_RnderMode = 1;
+    bool g_useColorForRendering = false;
+    bool g_playData = true;
+    float g_renderingDepthDiscontinuityThresLin = 0.001f;
+    float g_rmappingDepthDiscontinuityThresLin = 0.0f;
+    float g_renderingDepthDiscontinuityThresOffset = 0.012f;
+    float g_remappingDepthDiscontinuityThresOffset = 0.0f;
+    bool g_bUseCameraCalibration = false;
     unsigned int g_marchingCubesMaxNumTriangles = 250000; /* :379 */
-    float g_streamingRadius = 4.0f;       /* :136 */
     bool g_streamingEnabled = true;       /* :119 */
     vec3f g_streamingVoxelExtents = vec3f(1.0f, 1.0f, 1.0f);        /* :124 */
     vec3i g_streamingGridDimensions = vec3i(513, 513, 513);         /* :127 */
     vec3i g_streamingMinGridPos = vec3i(-256, -256, -256);          /* :130 */
     unsigned int g_streamingInitialChunkListSize = 2000;            /* :133 */
+    float g_streamingRadius = 4.0f;       /* :136 */
+    vec3f g_streamingPos = vec3f(0.0f, 0.0f, 3.0f);
+    unsigned int g_streamingOutParts = 80;
+    bool g_recordData = false;
+    bool g_recordCompression = true;
+    std::string g_recordDataFile = "Dump/test.sens";
+    bool g_reconstructionEnabled = true;
+    bool g_offlineProcessing = false;
+    bool g_integrationEnabled = true;
+    bool g_trackingEnabled = true;
+    bool g_timingsDetailledEnabled = false;
+    bool g_timingsDetailledEnabledOurs = false;
+    bool g_timingsTotalEnabled = false;
+    bool g_garbageCollectionEnabled = false;
+    unsigned int g_garbageCollectionStarve = 15;
+    int g_warpingMode = 0;
+    int g_depth_map_H = 400;
+    int g_depth_map_W = 480;
+    int g_maxDirectionalSlots = 0;
+    float g_directionThresholdCosine = 0.0f;
+    float g_weightMax = 0.0f;
+
+    /* globalParamasConfig.cpp:8-402 */
+    void setDefault() { *this = GlobalParamsConfig(); }
+    void print() const {
+        std::cout << "GlobalParamsConfig: voxel " << g_SDFVoxelSize << " m, truncation " << g_SDFTruncation
+                  << " m (scale " << g_SDFTruncationScale << "), hash slots " << g_hashNumSlots << ", SDF blocks "
+                  << g_hashNumSDFBlocks << ", marching cubes max triangles " << g_marchingCubesMaxNumTriangles
+                  << ", streaming " << (g_streamingEnabled ? "on" : "off") << std::endl;
+    }
 
     static GlobalParamsConfig& getInstance() {
         static GlobalParamsConfig s;
