@@ -37,6 +37,8 @@ def lib(nofma: bool = True):
         L.ref_voxel_bytes.restype = _I
         L.ref_integrate_dev.restype = _F
         L.ref_integrate_dev.argtypes = [_P, _P, _P, _P, _I, _I, _F, _P, _P, _F, _F, _F, _F]
+        L.ref_integrate_m2.restype = _I
+        L.ref_integrate_m2.argtypes = L.ref_integrate.argtypes
         L.ref_render_dev.restype = _F
         L.ref_render_dev.argtypes = [_P, _I, _I, _P, _P, _F, _F, _F, _F, _F, _F, _P, _P, _P, _P]
         _libs[nofma] = L
@@ -57,10 +59,11 @@ class RefScene:
             self.L.ref_destroy(self.h)
             self.h = None
 
-    def integrate(self, pm_dev, rgb_dev, nm_dev, W, H, trunc, pose, fx, fy, cx, cy):
+    def integrate(self, pm_dev, rgb_dev, nm_dev, W, H, trunc, pose, fx, fy, cx, cy, method: int = 1):
+        """method 2: the normal-direction allocation (USE_NORMAL_DIR_ALLOC)."""
         T = np.ascontiguousarray(np.asarray(pose, np.float32).reshape(16))
-        rc = self.L.ref_integrate(self.h, pm_dev, rgb_dev, nm_dev, W, H, _F(trunc), T.ctypes.data, _F(fx), _F(fy),
-                                  _F(cx), _F(cy))
+        fn = self.L.ref_integrate_m2 if method == 2 else self.L.ref_integrate
+        rc = fn(self.h, pm_dev, rgb_dev, nm_dev, W, H, _F(trunc), T.ctypes.data, _F(fx), _F(fy), _F(cx), _F(cy))
         assert rc == 0, rc
 
     def render(self, W, H, pose, fx, fy, cx, cy, min_d, max_d, fill=1e10):

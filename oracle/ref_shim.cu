@@ -80,6 +80,25 @@ int ref_integrate(void* h, const float* pm, const uint8_t* rgb, const float* nm,
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
 }
 
+// The same with the reference's normal-direction allocation, as its build
+// with USE_NORMAL_DIR_ALLOC calls it (VoxelScene.cu:1693-1715).
+int ref_integrate_m2(void* h, const float* pm, const uint8_t* rgb, const float* nm, int W, int H, float trunc,
+                     const float* T_host, float fx, float fy, float cx, float cy) {
+    RefScene* s = static_cast<RefScene*>(h);
+    float* d_T = nullptr;
+    if (cudaMalloc(&d_T, 16 * sizeof(float)) != cudaSuccess) return 1;
+    cudaMemcpy(d_T, T_host, 16 * sizeof(float), cudaMemcpyHostToDevice);
+    const float3 cam = make_float3(T_host[3], T_host[7], T_host[11]);
+    allocBlocksFromDepthMapMethod2CUDA(s->hash, s->params, reinterpret_cast<const float3*>(pm),
+                                       reinterpret_cast<const float3*>(nm), W, H, trunc, cam, d_T);
+    compactifyHashCUDA(s->hash, s->params);
+    integrateDepthMapIntoBlocksCUDA(s->hash, s->params, reinterpret_cast<const float3*>(pm),
+                                    reinterpret_cast<const uchar3*>(rgb), reinterpret_cast<const float3*>(nm), W, H,
+                                    trunc, cam, d_T, fx, fy, cx, cy);
+    cudaFree(d_T);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+}
+
 // main's ray-cast block (voxelSG.cpp:575-618): outputs to host buffers
 // (depth float[W*H], position / colour / normal float4[W*H]).
 int ref_render(void* h, int W, int H, const float* T_host, float fx, float fy, float cx, float cy, float minD,

@@ -83,3 +83,100 @@ def test_reference_kernels_match_oracle_and_cuda_path(cuda, oracle_mod, synth_mo
         assert cmp["frac_within_tol"] >= 0.995, cmp
     rnf.close()
     rfm.close()
+
+
+def _sparse(frames, step=6):
+    """Keep the points of a lattice of pixels only, so that the normal rays of
+    different pixels cross different blocks."""
+    out = []
+    for f in frames:
+        keep = np.zeros(f.pointmap.shape[:2], bool)
+        keep[step // 2::step, step // 2::step] = True
+        pm = np.where(keep[..., None], f.pointmap, 0).astype(np.float32)
+        nm = np.where(keep[..., None], f.normals, 0).astype(np.float32)
+        out.append(type(f)(pointmap=pm, rgb=f.rgb, normals=nm, depth=f.depth, pose=f.pose))
+    return out
+
+
+def _normal_ray_parents_unique(L, frames, voxel, trunc):
+    """True if in every frame each block lies on the normal ray of at most one
+    pixel (the reference keeps whichever pixel's write lands last)."""
+    from test_oracle_method2 import _norm, _rot, _xform
+
+    f32 = np.float32
+    for f in frames:
+        T = np.asarray(f.pose, f32).reshape(16)
+        owner = {}
+        for y, x in zip(*np.nonzero(np.any(f.pointmap != 0, -1))):
+            p = [f32(c) for c in f.pointmap[y, x]]
+            nc = [f32(c) for c in f.normals[y, x]]
+            nl = _norm(nc)
+            if nl < f32(0.1):
+                continue
+            nw = _rot(T, [c / nl for c in nc])
+            nl = _norm(nw)
+            if nl > f32(1e-6):
+                nw = [c / nl for c in nw]
+            w = _xform(T, p)
+            e = np.array([w[k] - f32(nw[k] * f32(trunc)) for k in range(3)], f32)
+            out = np.zeros(3 * 1024, np.int32)
+            import ctypes
+
+            n = L.orc_dda_blocks(np.asarray(w, f32).ctypes.data_as(ctypes.c_void_p), e.ctypes.data_as(ctypes.c_void_p),
+                                 f32(voxel), out.ctypes.data_as(ctypes.c_void_p))
+            for i in range(n):
+                b = tuple(out[3 * i:3 * i + 3])
+                if owner.setdefault(b, (y, x)) != (y, x):
+                    return False
+    return True
+
+
+def test_reference_normal_direction_allocation(cuda, oracle_mod, synth_mod):
+    """The reference's Method 2 (allocBlocksFromDepthMapMethod2CUDA and the
+    parent-pixel branch of its integration, built without FMA contraction)
+    against the oracle and the CUDA path, bit for bit, on sparse frames where
+    its allocation is race-free and every block has one parent pixel per
+    frame."""
+    ref = _ref()
+    import vsg
+
+    voxel, trunc, buckets, blocks, W, H = 0.004, 0.02, 1 << 24, 20000, 64, 48
+    for s in range(21, 80):
+        frames, K = synth_mod.tabletop_stream(s, 3, W, H)
+        frames = _sparse(frames)
+        orc = oracle_mod.OracleScene(voxel)
+        orc.set_alloc_method(2)
+        prev, clash = set(), False
+        for f in frames:
+            orc.integrate(f.pointmap, f.rgb, trunc, f.pose, K.fx, K.fy, K.cx, K.cy, normals=f.normals)
+            cur = {tuple(c) for c in orc.export(with_voxels=False)[0].tolist()}
+            seen = set()
+            for c in cur - prev:
+                b = oracle_mod.bucket_hash(c[0], c[1], c[2], buckets)
+                clash |= b in seen
+                seen.add(b)
+            prev = cur
+        if not clash and _normal_ray_parents_unique(oracle_mod.lib(), frames, voxel, trunc):
+            break
+    else:
+        pytest.skip("no race-free seed")
+    rnf = ref.RefScene(buckets, blocks, voxel, trunc, nofma=True)
+    orc = oracle_mod.OracleScene(voxel)
+    orc.set_alloc_method(2)
+    sc = vsg.Scene(voxel_size=voxel, truncation=trunc, hash_num_slots=50021, num_sdf_blocks=blocks)
+    sc.set_alloc_method(2)
+    for f in frames:
+        pm, rgb, nm = (cuda.from_numpy(np.ascontiguousarray(x)).cuda() for x in (f.pointmap, f.rgb, f.normals))
+        rnf.integrate(pm.data_ptr(), rgb.data_ptr(), nm.data_ptr(), W, H, trunc, f.pose, K.fx, K.fy, K.cx, K.cy,
+                      method=2)
+        orc.integrate(f.pointmap, f.rgb, trunc, f.pose, K.fx, K.fy, K.cx, K.cy, normals=f.normals)
+        sc.integrate(pm, rgb, nm, W, H, trunc, f.pose, K.fx, K.fy, K.cx, K.cy)
+        oc, ov = orc.export()
+        c1, v1 = rnf.export()
+        res = compare_volumes(c1, v1, oc, ov["raw"])
+        assert res["same_blocks"] and res["bit_exact"], res
+        gc, gv = sc.export()
+        res = compare_volumes(gc, gv, oc, ov["raw"])
+        assert res["same_blocks"] and res["bit_exact"], res
+    assert len(oc) > 20 and (orc.export_parents() != 0).sum() > 10
+    rnf.close()
