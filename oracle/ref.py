@@ -37,6 +37,8 @@ def lib(nofma: bool = True):
         L.ref_voxel_bytes.restype = _I
         L.ref_integrate_dev.restype = _F
         L.ref_integrate_dev.argtypes = [_P, _P, _P, _P, _I, _I, _F, _P, _P, _F, _F, _F, _F]
+        L.ref_extract_points.restype = _I
+        L.ref_extract_points.argtypes = [_P, _F, _F, ctypes.c_uint, _I, _P, _P, _P]
         L.ref_integrate_m2.restype = _I
         L.ref_integrate_m2.argtypes = L.ref_integrate.argtypes
         L.ref_render_dev.restype = _F
@@ -76,6 +78,18 @@ class RefScene:
                                d.ctypes.data, p.ctypes.data, c.ctypes.data, n.ctypes.data)
         assert rc == 0, rc
         return {"depth": d, "position": p, "color": c, "normal": n}
+
+    def extract_points(self, min_sdf, max_sdf, min_weight, max_points=2_000_000):
+        """The reference's extractSurfacePointsCUDA: (positions, colours,
+        normals) (n, 4) float32 in its output order, and its count."""
+        p = np.zeros((max_points, 4), np.float32)
+        c = np.zeros((max_points, 4), np.float32)
+        n = np.zeros((max_points, 4), np.float32)
+        cnt = self.L.ref_extract_points(self.h, _F(min_sdf), _F(max_sdf), int(min_weight), max_points,
+                                        p.ctypes.data, c.ctypes.data, n.ctypes.data)
+        assert cnt >= 0, cnt
+        k = min(cnt, max_points)
+        return p[:k], c[:k], n[:k], cnt
 
     def export(self):
         """(coords (n,3) int32 sorted by x,y,z; voxel bytes (n, 4096) uint8)."""

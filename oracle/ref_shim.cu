@@ -23,6 +23,11 @@ extern "C" void rayCastRenderCUDA(CUDAHashRef& hashData, int width, int height, 
                                   float fx, float fy, float cx, float cy, float minDepth, float maxDepth,
                                   float voxelSize, int numBuckets, int bucketSize, int totalHashSize);
 
+extern "C" void extractSurfacePointsCUDA(const CUDAHashRef& hashData, const Params& params, float minSDF,
+                                         float maxSDF, unsigned int minWeight, float4* d_outputPositions,
+                                         float4* d_outputColors, float4* d_outputNormals, int maxPoints,
+                                         int* d_pointCount);
+
 namespace {
 struct RefScene {
     CUDAHashRef hash;
@@ -97,6 +102,32 @@ int ref_integrate_m2(void* h, const float* pm, const uint8_t* rgb, const float* 
                                     trunc, cam, d_T, fx, fy, cx, cy);
     cudaFree(d_T);
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+}
+
+// RayCastRender::extractSurfacePoints without its logging
+// (RayCastRender.cpp:307-368): the points to host float4 arrays of max_pts
+// entries.  Returns the reference's point count (or -1).
+int ref_extract_points(void* h, float min_sdf, float max_sdf, unsigned int min_w, int max_pts, float* pos,
+                       float* col, float* nrm) {
+    RefScene* s = static_cast<RefScene*>(h);
+    float4 *dp = nullptr, *dc = nullptr, *dn = nullptr;
+    int* dcnt = nullptr;
+    if (cudaMalloc(&dp, (size_t)max_pts * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc(&dc, (size_t)max_pts * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc(&dn, (size_t)max_pts * sizeof(float4)) != cudaSuccess || cudaMalloc(&dcnt, sizeof(int)) != cudaSuccess)
+        return -1;
+    extractSurfacePointsCUDA(s->hash, s->params, min_sdf, max_sdf, min_w, dp, dc, dn, max_pts, dcnt);
+    int n = -1;
+    cudaMemcpy(&n, dcnt, sizeof(int), cudaMemcpyDeviceToHost);
+    const int k = n < 0 ? 0 : (n < max_pts ? n : max_pts);
+    cudaMemcpy(pos, dp, (size_t)k * sizeof(float4), cudaMemcpyDeviceToHost);
+    cudaMemcpy(col, dc, (size_t)k * sizeof(float4), cudaMemcpyDeviceToHost);
+    cudaMemcpy(nrm, dn, (size_t)k * sizeof(float4), cudaMemcpyDeviceToHost);
+    cudaFree(dp);
+    cudaFree(dc);
+    cudaFree(dn);
+    cudaFree(dcnt);
+    return cudaDeviceSynchronize() == cudaSuccess ? n : -1;
 }
 
 // main's ray-cast block (voxelSG.cpp:575-618): outputs to host buffers

@@ -180,3 +180,37 @@ def test_reference_normal_direction_allocation(cuda, oracle_mod, synth_mod):
         assert res["same_blocks"] and res["bit_exact"], res
     assert len(oc) > 20 and (orc.export_parents() != 0).sum() > 10
     rnf.close()
+
+
+@pytest.mark.parametrize("args", [(-0.1, 0.1, 1), (-0.01, 0.01, 1), (-0.02, 0.02, 2)])
+def test_reference_surface_points(cuda, oracle_mod, synth_mod, args):
+    """The reference's extractSurfacePointsCUDA (kernelExtractSurfacePoints,
+    RayCastRender.cu:683-868) on the volume its own kernels built, against
+    the oracle's restatement on the oracle's (bit-identical) volume: the same
+    points, compared as multisets of their 12 floats."""
+    ref = _ref()
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_golden
+    from test_gpu_points import _rows
+
+    voxel, trunc, buckets, blocks, W, H = 0.004, 0.02, 1 << 24, 20000, 64, 48
+    for s in range(13, 63):
+        frames, K = synth_mod.tabletop_stream(s, 3, W, H)
+        if not make_golden.bucket_collision(oracle_mod, frames, K, voxel, trunc, buckets):
+            break
+    else:
+        pytest.skip("no race-free seed")
+    rnf = ref.RefScene(buckets, blocks, voxel, trunc, nofma=True)
+    orc = oracle_mod.OracleScene(voxel)
+    for f in frames:
+        pm, rgb, nm = (cuda.from_numpy(np.ascontiguousarray(x)).cuda() for x in (f.pointmap, f.rgb, f.normals))
+        rnf.integrate(pm.data_ptr(), rgb.data_ptr(), nm.data_ptr(), W, H, trunc, f.pose, K.fx, K.fy, K.cx, K.cy)
+        orc.integrate(f.pointmap, f.rgb, trunc, f.pose, K.fx, K.fy, K.cx, K.cy)
+    rP, rC, rN, rn = rnf.extract_points(*args)
+    on, oP, oC, oN = orc.extract_points(*args, 2_000_000)
+    assert rn == on > 100, (rn, on)
+    assert np.array_equal(_rows(rP, rC, rN), _rows(oP, oC, oN))
+    rnf.close()
