@@ -261,12 +261,15 @@ int vsg_renderer_create(int w, int h, vsg_renderer** out) {
     cudaDeviceGetAttribute(&R.sm_count, cudaDevAttrMultiProcessorCount, R.device);
     const size_t n = (size_t)w * h;
     // RayCastRender::initialize, RayCastRender.cpp:88-118
+    const size_t nb = (size_t)((w + 7) / 8) * ((h + 3) / 4) + (size_t)((w + 63) / 64) * ((h + 31) / 32) + 1;
     if (cudaMalloc(&R.depth, n * sizeof(float)) != cudaSuccess || cudaMalloc(&R.position, n * sizeof(float4)) != cudaSuccess ||
-        cudaMalloc(&R.color, n * sizeof(float4)) != cudaSuccess || cudaMalloc(&R.normal, n * sizeof(float4)) != cudaSuccess) {
+        cudaMalloc(&R.color, n * sizeof(float4)) != cudaSuccess || cudaMalloc(&R.normal, n * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc(&R.bounds, nb * sizeof(uint2)) != cudaSuccess) {
         cudaFree(R.depth);
         cudaFree(R.position);
         cudaFree(R.color);
         cudaFree(R.normal);
+        cudaFree(R.bounds);
         delete r;
         return VSG_ERR_OUT_OF_MEMORY;
     }
@@ -281,6 +284,7 @@ int vsg_renderer_destroy(vsg_renderer* r) {
     cudaFree(r->impl.position);
     cudaFree(r->impl.color);
     cudaFree(r->impl.normal);
+    cudaFree(r->impl.bounds);
     cudaFree(r->impl.bracket);
     cudaFree(r->impl.partials);
     cudaFree(r->impl.skipped);

@@ -49,6 +49,7 @@ struct Renderer {
     float4* position = nullptr;
     float4* color = nullptr;
     float4* normal = nullptr;
+    uint2* bounds = nullptr;  // march distance bounds per pixel tile (k_tile_bounds)
     int sm_count = 148;
     // adjoint support (vsg_renderer_record): march brackets, per-CTA pose
     // gradient partials, skipped-pixel counter

@@ -25,6 +25,11 @@ struct RenderArgs {
     float4* col;
     float4* nrm;
     float2* rec;  // non-null when recording: per pixel the march bracket of its last zero crossing
+    // Optional ray-distance bounds (k_tile_bounds): per 8x4 pixel tile, then
+    // per 64x32 pixel tile, then one entry for every pixel; .x = ~bits of the
+    // nearest, .y = bits of the farthest distance (0 / 0: no box).
+    const uint2* bounds;
+    int t1x, t2x, n1, n2;
 };
 
 // Pool indices of the blocks holding a sample's 8 trilinear taps.  The taps
@@ -277,6 +282,33 @@ static __device__ __forceinline__ void ray_setup(const RenderArgs& a, const floa
     r.n_full = r.n_skip = r.n_jump = r.n_single = 0u;
 }
 
+// Start the march at the nearest and end it after the farthest ray distance
+// at which a sample of this pixel's tile can read a weighted voxel: every
+// sample outside that range is invalid, so skipping it (the chain replayed
+// exactly) or not taking it leaves the outputs as they are.  The margin
+// covers the rounding of the sample position cam + rc * dir.
+static __device__ __forceinline__ void apply_bounds(const RenderArgs& a, int x, int y, RayState& r) {
+    const uint2 b1 = __ldg(a.bounds + (y >> 2) * a.t1x + (x >> 3));
+    const uint2 b2 = __ldg(a.bounds + a.n1 + (y >> 5) * a.t2x + (x >> 6));
+    const uint2 bg = __ldg(a.bounds + a.n1 + a.n2);
+    const uint32_t lo_inv = max(max(b1.x, b2.x), bg.x), hi_bits = max(max(b1.y, b2.y), bg.y);
+    if (lo_inv == 0u) {  // no weighted block projects onto the tile
+        r.re = r.rc;
+        return;
+    }
+    const float lo = __uint_as_float(~lo_inv), hi = __uint_as_float(hi_bits);
+    const float cm = fmaxf(fmaxf(fabsf(r.R.ox), fabsf(r.R.oy)), fabsf(r.R.oz));
+    const float first = lo - (1e-4f + 1e-4f * lo + 1e-6f * (cm + lo));
+    const float last = hi + (1e-4f + 1e-4f * hi + 1e-6f * (cm + hi));
+    r.re = fminf(r.re, last);
+    if (first > r.rc && r.rc < r.re) {
+        const int before = r.steps;
+        r.rc = vsg_chain_advance(r.rc, a.s.voxel * 0.5f, fminf(first, r.re), kMaxMarch - r.steps, &r.steps);
+        r.n_skip += (uint32_t)(r.steps - before);
+        ++r.n_jump;
+    }
+}
+
 // One iteration of the march: a skip jump, a march sample or a
 // regula-falsi sample.  Returns true when the ray is done.
 static __device__ __forceinline__ bool ray_step(const RenderArgs& a, RayState& r, size_t pi) {
@@ -438,6 +470,7 @@ static __device__ __forceinline__ void render_pixel(const RenderArgs& a, int x, 
     RayState r;
     ray_setup(a, T, x, y, r);
     if (march_enabled(a)) {
+        if (a.bounds) apply_bounds(a, x, y, r);
 #pragma unroll 1
         while (!ray_step(a, r, pi)) {
         }
