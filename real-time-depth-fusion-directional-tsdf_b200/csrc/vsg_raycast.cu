@@ -38,9 +38,12 @@ __global__ void __launch_bounds__(128, 6) k_render(RenderArgs a) {
 
 // Ray-distance bounds per pixel tile for the march (apply_bounds).  One
 // thread per pool block.  A block that holds a weighted voxel (or has not
-// been integrated yet) is taken as its box grown by 3 voxels: a sample's taps
-// lie within 1.5 voxels of it per axis (RayCastRender.cu:17-25, 127-170), so
-// only samples inside the grown box can read the block.  The part of the box
+// been integrated yet: all of it) is taken as the bounding box of its
+// weighted 2x2x2 sub-cubes grown by 2 voxels: the taps of a sample at p are
+// voxels floor(p/v) - 1 .. floor(p/v) + 1 per axis (RayCastRender.cu:17-25,
+// 127-170, whose round-half-away-from-zero reaches one voxel lower for
+// negative coordinates), so a sample can only read voxel i from within one
+// voxel of it, and the second voxel of growth is slack.  The part of the box
 // in front of the plane at half the minimum depth (every sample is at least
 // the minimum depth ahead of the camera) is projected; its pixel rectangle,
 // grown by a 2-pixel margin, is entered into the 8x4 tiles it covers (up to
@@ -80,13 +83,26 @@ __global__ void __launch_bounds__(256) k_tile_bounds(RenderArgs a) {
     for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < hw; b += gridDim.x * blockDim.x) {
         const unsigned long long key = s.block_key[b];
         if (key == kKeyEmpty || key == kKeyTomb) continue;
-        if (!s.block_fresh[b] && s.block_wmask[b] == 0ull) continue;
+        const unsigned long long wm = s.block_fresh[b] ? ~0ull : s.block_wmask[b];
+        if (wm == 0ull) continue;
         int bx, by, bz;
         unpack_key(key, bx, by, bz);
-        const float lo[3] = {((float)(bx * kBlock) - 3.0f) * v, ((float)(by * kBlock) - 3.0f) * v,
-                             ((float)(bz * kBlock) - 3.0f) * v};
-        const float hi[3] = {((float)(bx * kBlock) + (kBlock + 3.0f)) * v, ((float)(by * kBlock) + (kBlock + 3.0f)) * v,
-                             ((float)(bz * kBlock) + (kBlock + 3.0f)) * v};
+        // occupied sub-cube rows per axis (bit (sz*4+sy)*4+sx of wm)
+        unsigned long long f = wm | (wm >> 32);
+        f |= f >> 16;
+        const unsigned yz = (unsigned)(f & 0xFFFFull);  // (sy, sx) over all sz
+        unsigned xm = yz | (yz >> 8);
+        xm = (xm | (xm >> 4)) & 0xFu;
+        const unsigned ym = ((yz & 0xFu) ? 1u : 0u) | ((yz & 0xF0u) ? 2u : 0u) | ((yz & 0xF00u) ? 4u : 0u) |
+                            ((yz & 0xF000u) ? 8u : 0u);
+        const unsigned zm = ((wm & 0xFFFFull) ? 1u : 0u) | ((wm & 0xFFFF0000ull) ? 2u : 0u) |
+                            ((wm & 0xFFFF00000000ull) ? 4u : 0u) | ((wm & 0xFFFF000000000000ull) ? 8u : 0u);
+        const int sx0 = __ffs(xm) - 1, sx1 = 31 - __clz(xm), sy0 = __ffs(ym) - 1, sy1 = 31 - __clz(ym);
+        const int sz0 = __ffs(zm) - 1, sz1 = 31 - __clz(zm);
+        const float lo[3] = {((float)(bx * kBlock + 2 * sx0) - 2.0f) * v, ((float)(by * kBlock + 2 * sy0) - 2.0f) * v,
+                             ((float)(bz * kBlock + 2 * sz0) - 2.0f) * v};
+        const float hi[3] = {((float)(bx * kBlock + 2 * sx1) + 4.0f) * v, ((float)(by * kBlock + 2 * sy1) + 4.0f) * v,
+                             ((float)(bz * kBlock + 2 * sz1) + 4.0f) * v};
         const float c[3] = {a.camx, a.camy, a.camz};
         float n2 = 0.0f, f2 = 0.0f;
 #pragma unroll
