@@ -1,0 +1,39 @@
+"""How far a ray-cast sample reaches for its trilinear taps (CPU).
+
+The ray caster's distance bounds grow each block's weighted sub-cubes by 2
+voxels on the premise that a sample at p reads voxel i only when p lies in
+[(i - 1) v, (i + 2) v], i.e. within one voxel of the voxel's cell.  This
+checks that premise on the tap arithmetic of trilinearInterpolationSimpleFastFast
+(RayCastRender.cu:127-170; worldToVirtualVoxelPos, :17-25: x0 = round half
+away from zero of (p - v/2) / v, x1 the same of (p + v/2) / v), evaluated in
+FP32 like the kernel, over positions of both signs and of several magnitudes.
+"""
+import numpy as np
+import pytest
+
+
+def _tap(q):
+    q = q.astype(np.float32)
+    sg = np.sign(q).astype(np.float32)
+    return np.floor((q + np.float32(0.5) * sg).astype(np.float32)).astype(np.int64)
+
+
+@pytest.mark.parametrize("voxel", [0.0005, 0.002, 0.004, 0.01])
+def test_taps_lie_within_one_voxel_of_the_sample(voxel):
+    rng = np.random.default_rng(int(voxel * 1e5))
+    v = np.float32(voxel)
+    n = 1_000_000
+    p = (rng.uniform(-50.0, 50.0, n) * rng.choice([1.0, 0.01, 0.001], n)).astype(np.float32)
+    dx = (p - v / np.float32(2)).astype(np.float32)
+    x0 = _tap((dx / v).astype(np.float32))
+    x1 = _tap(((dx + v).astype(np.float32) / v).astype(np.float32))
+    pv = p.astype(np.float64) / float(v)
+    for i in (x0, x1):
+        # p / v in [i - 1, i + 2] up to FP32 rounding of p / v
+        assert (pv - (i - 1)).min() > -0.01
+        assert ((i + 2) - pv).min() > -0.01
+    # the taps are floor(p / v) - 1 .. floor(p / v) + 1
+    fl = np.floor(pv).astype(np.int64)
+    ok = np.abs(pv - np.round(pv)) > 1e-4 + 1e-6 * np.abs(pv)  # away from the rounding boundaries
+    assert np.all((x0[ok] >= fl[ok] - 1) & (x1[ok] <= fl[ok] + 1))
+    assert np.all((x1 - x0 >= 0) & (x1 - x0 <= 2))
