@@ -87,6 +87,24 @@ __global__ void __launch_bounds__(256, 4) k_batch_integrate(const BatchHeader* h
     integrate_work(args[blockIdx.y]);
 }
 
+// The ray-distance bounds of every scene ray cast this step: cleared, then
+// filled by tile_bounds_range over each scene's pool blocks.
+__global__ void __launch_bounds__(256) k_batch_bounds_clear(const BatchHeader* h, const RenderArgs* args) {
+    if ((int)blockIdx.y >= h->n) return;
+    const RenderArgs& a = args[blockIdx.y];
+    if (a.W <= 0 || !a.bounds) return;
+    uint2* b = const_cast<uint2*>(a.bounds);
+    const int n = a.n1 + a.n2 + 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = make_uint2(0u, 0u);
+}
+
+__global__ void __launch_bounds__(256) k_batch_tile_bounds(const BatchHeader* h, const RenderArgs* args) {
+    if ((int)blockIdx.y >= h->n) return;
+    const RenderArgs& a = args[blockIdx.y];
+    if (a.W <= 0 || !a.bounds) return;
+    tile_bounds_range(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
 template <int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks) k_batch_render(const BatchHeader* h, const RenderArgs* args) {
     const int i = scene_of(h->render_prefix, h->n, blockIdx.x);
@@ -139,6 +157,16 @@ using vsg::Batch;
 
 namespace vsg {
 
+// Enqueue the ray-distance bounds of the scenes a step ray casts.
+static void enqueue_bounds(Batch& b, int n, cudaStream_t st) {
+    const BatchLayout L = layout_for(n);
+    const BatchHeader* h = reinterpret_cast<const BatchHeader*>(b.d_step);
+    const RenderArgs* ra = reinterpret_cast<const RenderArgs*>(b.d_step + L.render_off);
+    const int bnd_x = std::max(2, (b.sm_count * 4) / n);
+    k_batch_bounds_clear<<<dim3(bnd_x, n), 256, 0, st>>>(h, ra);
+    k_batch_tile_bounds<<<dim3(bnd_x, n), 256, 0, st>>>(h, ra);
+}
+
 // Enqueue the stages of one step (argument blocks already on the device).
 static void enqueue_stages(Batch& b, int n, uint32_t alloc_tiles, uint32_t render_tiles, int render_variant,
                            cudaStream_t st) {
@@ -153,7 +181,10 @@ static void enqueue_stages(Batch& b, int n, uint32_t alloc_tiles, uint32_t rende
     k_batch_select<<<dim3(sel_x, n), 256, 0, st>>>(h, ia);
     const int integ_x = std::max(2, (b.sm_count * 4) / n);
     k_batch_integrate<<<dim3(integ_x, n), 256, 0, st>>>(h, ia);
-    if (render_tiles) launch_render_variant(render_variant, dim3(render_tiles), st, h, ra);
+    if (render_tiles) {
+        enqueue_bounds(b, n, st);
+        launch_render_variant(render_variant, dim3(render_tiles), st, h, ra);
+    }
 }
 
 }  // namespace vsg
@@ -320,6 +351,12 @@ int vsg_batch_step(vsg_batch* b, const vsg_batch_frame* frames, int n_frames, vs
             R.pos = r->position;
             R.col = r->color;
             R.nrm = r->normal;
+            // the renderer's bounds buffer (sized for r->w x r->h == f.w x f.h)
+            R.bounds = r->bounds;
+            R.t1x = (f.w + 7) / 8;
+            R.t2x = (f.w + 63) / 64;
+            R.n1 = R.t1x * ((f.h + 3) / 4);
+            R.n2 = R.t2x * ((f.h + 31) / 32);
         }
         sc->integrated_frames++;
     }
@@ -335,6 +372,7 @@ int vsg_batch_step(vsg_batch* b, const vsg_batch_frame* frames, int n_frames, vs
         enqueue_stages(B, n_frames, at, 0, 0, st);
         int best = 0;
         if (rt) {
+            enqueue_bounds(B, n_frames, st);
             const BatchHeader* dh = reinterpret_cast<const BatchHeader*>(B.d_step);
             const RenderArgs* dr = reinterpret_cast<const RenderArgs*>(B.d_step + L.render_off);
             if (B.autotune) {

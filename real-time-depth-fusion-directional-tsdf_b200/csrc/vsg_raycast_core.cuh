@@ -309,6 +309,158 @@ static __device__ __forceinline__ void apply_bounds(const RenderArgs& a, int x, 
     }
 }
 
+// Ray-distance bounds per pixel tile for the march (apply_bounds).  One
+// thread per pool block.  A block that holds a weighted voxel (or has not
+// been integrated yet: all of it) is taken as the bounding box of its
+// weighted 2x2x2 sub-cubes grown by 2 voxels: the taps of a sample at p are
+// voxels floor(p/v) - 1 .. floor(p/v) + 1 per axis (RayCastRender.cu:17-25,
+// 127-170, whose round-half-away-from-zero reaches one voxel lower for
+// negative coordinates), so a sample can only read voxel i from within one
+// voxel of it, and the second voxel of growth is slack.  The part of the box
+// in front of the plane at half the minimum depth (every sample is at least
+// the minimum depth ahead of the camera) is projected; its pixel rectangle,
+// grown by a 2-pixel margin, is entered into the 8x4 tiles it covers (up to
+// 64 of them), else into the 64x32 tiles (up to 4096), else into the entry
+// for every pixel: nearest distance by atomicMax of ~bits, farthest by
+// atomicMax of bits (non-negative floats order like their bits).  A pose
+// whose rotation is not orthonormal, a zero focal length or a non-positive
+// minimum depth disables the bounds (nearest 0, farthest infinity).
+// Pool blocks first, first + stride, ... of one render's scene.
+static __device__ __forceinline__ void tile_bounds_range(const RenderArgs& a, uint32_t first, uint32_t stride) {
+    const SceneDev& s = a.s;
+    unsigned* bnd = reinterpret_cast<unsigned*>(const_cast<uint2*>(a.bounds));
+    unsigned* glob = bnd + 2 * (a.n1 + a.n2);
+    float T[12];
+    load_pose(a, T);
+    float e = 0.0f;  // largest entry of R^T R - I
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float d = T[i] * T[j] + T[4 + i] * T[4 + j] + T[8 + i] * T[8 + j] - (i == j ? 1.0f : 0.0f);
+            e = fmaxf(e, fabsf(d));
+        }
+    const bool ok = e < 1e-4f && isfinite(a.fx) && isfinite(a.fy) && a.fx != 0.0f && a.fy != 0.0f &&
+                    isfinite(a.cx) && isfinite(a.cy) && a.minD > 0.0f && isfinite(a.minD) && isfinite(a.camx) &&
+                    isfinite(a.camy) && isfinite(a.camz);
+    if (!ok) {
+        if (first == 0u) {
+            atomicMax(glob, 0xFFFFFFFFu);  // nearest 0
+            atomicMax(glob + 1, 0x7F800000u);  // farthest +inf
+        }
+        return;
+    }
+    const float zc = 0.5f * a.minD;
+    const float mpx = 2.0f + 10.0f * e * (fabsf(a.fx) + fabsf(a.fy) + (float)a.W + (float)a.H);
+    const float v = s.voxel;
+    const uint32_t hw = s.ctr->high_water;
+    for (uint32_t b = first; b < hw; b += stride) {
+        const unsigned long long key = s.block_key[b];
+        if (key == kKeyEmpty || key == kKeyTomb) continue;
+        const unsigned long long wm = s.block_fresh[b] ? ~0ull : s.block_wmask[b];
+        if (wm == 0ull) continue;
+        int bx, by, bz;
+        unpack_key(key, bx, by, bz);
+        // occupied sub-cube rows per axis (bit (sz*4+sy)*4+sx of wm)
+        unsigned long long f = wm | (wm >> 32);
+        f |= f >> 16;
+        const unsigned yz = (unsigned)(f & 0xFFFFull);  // (sy, sx) over all sz
+        unsigned xm = yz | (yz >> 8);
+        xm = (xm | (xm >> 4)) & 0xFu;
+        const unsigned ym = ((yz & 0xFu) ? 1u : 0u) | ((yz & 0xF0u) ? 2u : 0u) | ((yz & 0xF00u) ? 4u : 0u) |
+                            ((yz & 0xF000u) ? 8u : 0u);
+        const unsigned zm = ((wm & 0xFFFFull) ? 1u : 0u) | ((wm & 0xFFFF0000ull) ? 2u : 0u) |
+                            ((wm & 0xFFFF00000000ull) ? 4u : 0u) | ((wm & 0xFFFF000000000000ull) ? 8u : 0u);
+        const int sx0 = __ffs(xm) - 1, sx1 = 31 - __clz(xm), sy0 = __ffs(ym) - 1, sy1 = 31 - __clz(ym);
+        const int sz0 = __ffs(zm) - 1, sz1 = 31 - __clz(zm);
+        const float lo[3] = {((float)(bx * kBlock + 2 * sx0) - 2.0f) * v, ((float)(by * kBlock + 2 * sy0) - 2.0f) * v,
+                             ((float)(bz * kBlock + 2 * sz0) - 2.0f) * v};
+        const float hi[3] = {((float)(bx * kBlock + 2 * sx1) + 4.0f) * v, ((float)(by * kBlock + 2 * sy1) + 4.0f) * v,
+                             ((float)(bz * kBlock + 2 * sz1) + 4.0f) * v};
+        const float c[3] = {a.camx, a.camy, a.camz};
+        float n2 = 0.0f, f2 = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float dl = lo[i] - c[i], dh = hi[i] - c[i];
+            const float n = fmaxf(fmaxf(dl, -dh), 0.0f), f = fmaxf(fabsf(dl), fabsf(dh));
+            n2 += n * n;
+            f2 += f * f;
+        }
+        const float dmin = sqrtf(n2), dmax = sqrtf(f2);
+        // camera coordinates of the 8 corners
+        float px[8], py[8], pz[8];
+        bool any_front = false;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const float dx = ((k & 1) ? hi[0] : lo[0]) - c[0];
+            const float dy = ((k & 2) ? hi[1] : lo[1]) - c[1];
+            const float dz = ((k & 4) ? hi[2] : lo[2]) - c[2];
+            px[k] = T[0] * dx + T[4] * dy + T[8] * dz;
+            py[k] = T[1] * dx + T[5] * dy + T[9] * dz;
+            pz[k] = T[2] * dx + T[6] * dy + T[10] * dz;
+            any_front |= pz[k] >= zc;
+        }
+        if (!any_front) continue;  // wholly nearer than any sample
+        float u0 = 3.4e38f, u1 = -3.4e38f, w0 = 3.4e38f, w1 = -3.4e38f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (pz[k] >= zc) {
+                const float u = a.fx * (px[k] / pz[k]) + a.cx, w = a.fy * (py[k] / pz[k]) + a.cy;
+                u0 = fminf(u0, u);
+                u1 = fmaxf(u1, u);
+                w0 = fminf(w0, w);
+                w1 = fmaxf(w1, w);
+            }
+        }
+        // edges crossing the plane z = zc (corners k and k ^ axis bit)
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+#pragma unroll
+            for (int ax = 1; ax < 8; ax <<= 1) {
+                if (k & ax) continue;
+                const int j = k | ax;
+                if ((pz[k] >= zc) == (pz[j] >= zc)) continue;
+                const float t = (zc - pz[k]) / (pz[j] - pz[k]);
+                const float qx = px[k] + t * (px[j] - px[k]), qy = py[k] + t * (py[j] - py[k]);
+                const float u = a.fx * (qx / zc) + a.cx, w = a.fy * (qy / zc) + a.cy;
+                u0 = fminf(u0, u);
+                u1 = fmaxf(u1, u);
+                w0 = fminf(w0, w);
+                w1 = fmaxf(w1, w);
+            }
+        u0 -= mpx;
+        u1 += mpx;
+        w0 -= mpx;
+        w1 += mpx;
+        if (!(u1 >= 0.0f && w1 >= 0.0f && u0 <= (float)(a.W - 1) && w0 <= (float)(a.H - 1))) continue;
+        const int x0 = (int)fmaxf(u0, 0.0f), x1 = (int)fminf(u1, (float)(a.W - 1));
+        const int y0 = (int)fmaxf(w0, 0.0f), y1 = (int)fminf(w1, (float)(a.H - 1));
+        const unsigned lo_inv = ~__float_as_uint(dmin), hi_bits = __float_as_uint(dmax);
+        const int ax0 = x0 >> 3, ax1 = x1 >> 3, ay0 = y0 >> 2, ay1 = y1 >> 2;
+        if ((ax1 - ax0 + 1) * (ay1 - ay0 + 1) <= 64) {
+            for (int ty = ay0; ty <= ay1; ++ty)
+                for (int tx = ax0; tx <= ax1; ++tx) {
+                    unsigned* e1 = bnd + 2 * (ty * a.t1x + tx);
+                    atomicMax(e1, lo_inv);
+                    atomicMax(e1 + 1, hi_bits);
+                }
+            continue;
+        }
+        const int bx0 = x0 >> 6, bx1 = x1 >> 6, by0 = y0 >> 5, by1 = y1 >> 5;
+        if ((bx1 - bx0 + 1) * (by1 - by0 + 1) <= 4096) {
+            for (int ty = by0; ty <= by1; ++ty)
+                for (int tx = bx0; tx <= bx1; ++tx) {
+                    unsigned* e2 = bnd + 2 * (a.n1 + ty * a.t2x + tx);
+                    atomicMax(e2, lo_inv);
+                    atomicMax(e2 + 1, hi_bits);
+                }
+            continue;
+        }
+        atomicMax(glob, lo_inv);
+        atomicMax(glob + 1, hi_bits);
+    }
+}
+
 // One iteration of the march: a skip jump, a march sample or a
 // regula-falsi sample.  Returns true when the ray is done.
 static __device__ __forceinline__ bool ray_step(const RenderArgs& a, RayState& r, size_t pi) {
