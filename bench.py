@@ -237,8 +237,9 @@ def run_ours(args):
         import shard
 
         ms = shard.max_over_ranks(ms, dist)
-    # per step: reset (3 kernels) + per frame: frame_begin, alloc, select, integrate, render_begin, render
-    launches_per_step = 3 + len(dev) * 6
+    # per step: reset (3 kernels) + per frame: frame_begin, alloc, select, integrate, render_begin,
+    # tile_bounds, render
+    launches_per_step = 3 + len(dev) * 7
     # per-kernel times (separate pass with events around each launch)
     sc.timing(True)
     sc.timing_reset()
