@@ -229,7 +229,10 @@ VSG_API int vsg_renderer_destroy(vsg_renderer* r);
 /* Ray cast the scene.  pose_dev: DEVICE float[16] row-major camera->world
  * (the reference passes a caller-owned device matrix); only its rotation is
  * read, cam_pos (host float[3]) is the ray origin.  When the scene holds no
- * block the outputs are left untouched, as in the reference. */
+ * block the outputs are left untouched, as in the reference.  Two launches
+ * on the stream: per-tile march distance bounds (into the renderer's own
+ * buffer), then the ray cast; calls on one renderer must not overlap on the
+ * GPU (they share its outputs and that buffer). */
 VSG_API int vsg_render(vsg_renderer* r, const vsg_scene* s, const float cam_pos[3], const float* pose_dev,
                float fx, float fy, float cx, float cy, float min_depth, float max_depth,
                vsg_stream_t stream);

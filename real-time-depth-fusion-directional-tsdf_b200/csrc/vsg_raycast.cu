@@ -15,7 +15,10 @@
 // Skipped runs are replayed in O(1) by vsg_chain_advance, which lands on the
 // exact float the serial additions produce.  Surviving samples take the full
 // trilinear interpolation (8 taps, blocks resolved through the dense block
-// index, cached across samples).
+// index, cached across samples).  Before the march, k_tile_bounds records per
+// pixel tile the nearest and farthest distance at which any weighted block
+// can be read; each ray starts at the first and stops after the second
+// (tile_bounds_range, apply_bounds).
 #include <cuda_runtime.h>
 
 #include <cstring>
