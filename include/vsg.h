@@ -58,7 +58,7 @@ enum {
     VSG_ERR_INVALID_ARG = 1,   /* null pointer, non-positive size, bad knob */
     VSG_ERR_NOT_ALLOCATED = 2, /* handle not initialised */
     VSG_ERR_CUDA = 3,          /* a CUDA runtime call failed */
-    VSG_ERR_OUT_OF_MEMORY = 4, /* device allocation failed */
+    VSG_ERR_OUT_OF_MEMORY = 4, /* device or host allocation failed */
     VSG_ERR_TOO_LARGE = 5      /* a size exceeds a documented maximum */
 };
 

@@ -192,41 +192,43 @@ static void enqueue_stages(Batch& b, int n, uint32_t alloc_tiles, uint32_t rende
 extern "C" {
 
 int vsg_batch_create(vsg_scene* const* scenes, vsg_renderer* const* renderers, int n, vsg_batch** out) {
-    if (!out || !scenes || n <= 0) return VSG_ERR_INVALID_ARG;
-    if (n > vsg::kMaxBatch) return VSG_ERR_TOO_LARGE;
-    *out = nullptr;
-    vsg_batch* b = new (std::nothrow) vsg_batch();
-    if (!b) return VSG_ERR_OUT_OF_MEMORY;
-    Batch& B = b->impl;
-    cudaGetDevice(&B.device);
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B.device);
-    B.sm_count = sms > 0 ? sms : 148;
-    for (int i = 0; i < n; ++i) {
-        if (!scenes[i] || scenes[i]->impl.device != B.device) {
+    return vsg::host_guard([&]() -> int {
+        if (!out || !scenes || n <= 0) return VSG_ERR_INVALID_ARG;
+        if (n > vsg::kMaxBatch) return VSG_ERR_TOO_LARGE;
+        *out = nullptr;
+        vsg_batch* b = new (std::nothrow) vsg_batch();
+        if (!b) return VSG_ERR_OUT_OF_MEMORY;
+        Batch& B = b->impl;
+        cudaGetDevice(&B.device);
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B.device);
+        B.sm_count = sms > 0 ? sms : 148;
+        for (int i = 0; i < n; ++i) {
+            if (!scenes[i] || scenes[i]->impl.device != B.device) {
+                delete b;
+                return VSG_ERR_INVALID_ARG;
+            }
+            B.scenes.push_back(&scenes[i]->impl);
+            B.renderers.push_back(renderers ? (renderers[i] ? &renderers[i]->impl : nullptr) : nullptr);
+        }
+        B.step_bytes = vsg::layout_for(vsg::kMaxBatch).bytes;
+        bool ok = cudaMalloc(&B.d_step, B.step_bytes) == cudaSuccess;
+        for (int i = 0; i < 2 && ok; ++i)
+            ok = cudaMallocHost(&B.h_step[i], B.step_bytes) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&B.done[i], cudaEventDisableTiming) == cudaSuccess;
+        if (!ok) {
+            cudaFree(B.d_step);
+            for (int i = 0; i < 2; ++i) {
+                if (B.h_step[i]) cudaFreeHost(B.h_step[i]);
+                if (B.done[i]) cudaEventDestroy(B.done[i]);
+            }
             delete b;
-            return VSG_ERR_INVALID_ARG;
+            return VSG_ERR_OUT_OF_MEMORY;
         }
-        B.scenes.push_back(&scenes[i]->impl);
-        B.renderers.push_back(renderers ? (renderers[i] ? &renderers[i]->impl : nullptr) : nullptr);
-    }
-    B.step_bytes = vsg::layout_for(vsg::kMaxBatch).bytes;
-    bool ok = cudaMalloc(&B.d_step, B.step_bytes) == cudaSuccess;
-    for (int i = 0; i < 2 && ok; ++i)
-        ok = cudaMallocHost(&B.h_step[i], B.step_bytes) == cudaSuccess &&
-             cudaEventCreateWithFlags(&B.done[i], cudaEventDisableTiming) == cudaSuccess;
-    if (!ok) {
-        cudaFree(B.d_step);
-        for (int i = 0; i < 2; ++i) {
-            if (B.h_step[i]) cudaFreeHost(B.h_step[i]);
-            if (B.done[i]) cudaEventDestroy(B.done[i]);
-        }
-        delete b;
-        return VSG_ERR_OUT_OF_MEMORY;
-    }
-    for (int i = 0; i < 2; ++i) memset(B.h_step[i], 0, B.step_bytes);
-    *out = b;
-    return VSG_OK;
+        for (int i = 0; i < 2; ++i) memset(B.h_step[i], 0, B.step_bytes);
+        *out = b;
+        return VSG_OK;
+    });
 }
 
 int vsg_batch_destroy(vsg_batch* b) {
@@ -251,181 +253,183 @@ int vsg_batch_autotune(vsg_batch* b, int enable) {
 }
 
 int vsg_batch_step(vsg_batch* b, const vsg_batch_frame* frames, int n_frames, vsg_stream_t stream) {
-    using namespace vsg;
-    if (!b) return VSG_ERR_NOT_ALLOCATED;
-    if (!frames || n_frames <= 0) return VSG_ERR_INVALID_ARG;
-    Batch& B = b->impl;
-    if (n_frames > (int)B.scenes.size()) return VSG_ERR_INVALID_ARG;
-    cudaStream_t st = (cudaStream_t)stream;
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev != B.device) return VSG_ERR_INVALID_ARG;
-    // validate, make sure each scene's per-pixel buffers fit (allocates only
-    // on a scene's first frame of a larger resolution)
-    std::vector<char> seen(B.scenes.size(), 0);
-    for (int k = 0; k < n_frames; ++k) {
-        const vsg_batch_frame& f = frames[k];
-        if (f.scene < 0 || f.scene >= (int)B.scenes.size() || seen[f.scene]) return VSG_ERR_INVALID_ARG;
-        seen[f.scene] = 1;
-        if (!f.pointmap || !f.rgb || !f.normals || f.w <= 0 || f.h <= 0) return VSG_ERR_INVALID_ARG;
-        // normal-direction allocation needs its own parent pass: per-scene calls only
-        if (B.scenes[f.scene]->dev.alloc_method == 2) return VSG_ERR_INVALID_ARG;
-        if (f.render) {
-            Renderer* r = B.renderers[f.scene];
-            if (!r || r->w != f.w || r->h != f.h) return VSG_ERR_INVALID_ARG;
-        }
-        const int rc = ensure_pixel_buffers(B.scenes[f.scene], (size_t)f.w * f.h);
-        if (rc != VSG_OK) return rc;
-    }
-    // alternate staging buffers; the step that last read this one must be done
-    const int pb = B.parity;
-    B.parity ^= 1;
-    if (B.pending[pb]) {
-        cudaEventSynchronize(B.done[pb]);
-        B.pending[pb] = false;
-    }
-    unsigned char* hs = B.h_step[pb];
-    const BatchLayout L = layout_for(n_frames);
-    BatchHeader* h = reinterpret_cast<BatchHeader*>(hs);
-    AllocArgs* aa = reinterpret_cast<AllocArgs*>(hs + L.alloc_off);
-    IntegArgs* ia = reinterpret_cast<IntegArgs*>(hs + L.integ_off);
-    RenderArgs* ra = reinterpret_cast<RenderArgs*>(hs + L.render_off);
-    h->n = n_frames;
-    std::vector<int> key;
-    key.push_back(n_frames);
-    uint32_t at = 0, rt = 0;
-    for (int k = 0; k < n_frames; ++k) {
-        const vsg_batch_frame& f = frames[k];
-        Scene* sc = B.scenes[f.scene];
-        const int ax = (f.w + kTile - 1) / kTile, ay = (f.h + kTile - 1) / kTile;
-        h->alloc_prefix[k] = at;
-        h->alloc_tiles_x[k] = ax;
-        at += (uint32_t)(ax * ay);
-        const int rx = (f.w + kRenderTileW - 1) / kRenderTileW, ry = (f.h + kRenderTileH - 1) / kRenderTileH;
-        h->render_prefix[k] = rt;
-        h->render_tiles_x[k] = rx;
-        if (f.render) rt += (uint32_t)(rx * ry);
-        key.push_back(f.w);
-        key.push_back(f.h);
-        key.push_back(f.render ? 1 : 0);
-        Pose P;
-        memcpy(P.T, f.pose, sizeof(P.T));
-        AllocArgs& A = aa[k];
-        A.s = sc->dev;
-        A.pm = f.pointmap;
-        A.rgb = f.rgb;
-        A.nm = f.normals;
-        A.W = f.w;
-        A.H = f.h;
-        A.trunc = f.truncation;
-        A.pose = P;
-        IntegArgs& I = ia[k];
-        I.s = sc->dev;
-        I.W = f.w;
-        I.H = f.h;
-        I.trunc = f.truncation;
-        I.pose = P;
-        I.fx = f.fx;
-        I.fy = f.fy;
-        I.cx = f.cx;
-        I.cy = f.cy;
-        RenderArgs& R = ra[k];
-        memset(&R, 0, sizeof(R));
-        R.s = sc->dev;
-        if (f.render) {
-            Renderer* r = B.renderers[f.scene];
-            R.W = f.w;
-            R.H = f.h;
-            R.camx = f.pose[3];
-            R.camy = f.pose[7];
-            R.camz = f.pose[11];
-            R.pose = P;
-            R.pose_dev = nullptr;
-            R.touched = nullptr;
-            R.fx = f.fx;
-            R.fy = f.fy;
-            R.cx = f.cx;
-            R.cy = f.cy;
-            R.minD = f.min_depth;
-            R.maxD = f.max_depth;
-            R.depth = r->depth;
-            R.pos = r->position;
-            R.col = r->color;
-            R.nrm = r->normal;
-            // the renderer's bounds buffer (sized for r->w x r->h == f.w x f.h)
-            R.bounds = r->bounds;
-            R.t1x = (f.w + 7) / 8;
-            R.t2x = (f.w + 63) / 64;
-            R.n1 = R.t1x * ((f.h + 3) / 4);
-            R.n2 = R.t2x * ((f.h + 31) / 32);
-        }
-        sc->integrated_frames++;
-    }
-    h->alloc_prefix[n_frames] = at;
-    h->render_prefix[n_frames] = rt;
-    const size_t bytes = L.bytes;
-    Batch::Shape& shape = B.shapes[key];
-    if (shape.render_variant < 0) {
-        // first step of this shape: run it eagerly, tuning the ray-cast
-        // variant on the step's own data (ray casting leaves the scene as it
-        // is, so repeating it only rewrites the same outputs)
-        if (cudaMemcpyAsync(B.d_step, hs, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) return VSG_ERR_CUDA;
-        enqueue_stages(B, n_frames, at, 0, 0, st);
-        int best = 0;
-        if (rt) {
-            enqueue_bounds(B, n_frames, st);
-            const BatchHeader* dh = reinterpret_cast<const BatchHeader*>(B.d_step);
-            const RenderArgs* dr = reinterpret_cast<const RenderArgs*>(B.d_step + L.render_off);
-            if (B.autotune) {
-                float best_ms = 3.4e38f;
-                cudaEvent_t e0, e1;
-                cudaEventCreate(&e0);
-                cudaEventCreate(&e1);
-                for (int v = 0; v < 3; ++v) {
-                    cudaEventRecord(e0, st);
-                    launch_render_variant(v, dim3(rt), st, dh, dr);
-                    cudaEventRecord(e1, st);
-                    cudaEventSynchronize(e1);
-                    float ms = 0.0f;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                    if (ms < best_ms) {
-                        best_ms = ms;
-                        best = v;
-                    }
-                }
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-            } else {
-                launch_render_variant(0, dim3(rt), st, dh, dr);
+    return vsg::host_guard([&]() -> int {
+        using namespace vsg;
+        if (!b) return VSG_ERR_NOT_ALLOCATED;
+        if (!frames || n_frames <= 0) return VSG_ERR_INVALID_ARG;
+        Batch& B = b->impl;
+        if (n_frames > (int)B.scenes.size()) return VSG_ERR_INVALID_ARG;
+        cudaStream_t st = (cudaStream_t)stream;
+        int dev = -1;
+        if (cudaGetDevice(&dev) != cudaSuccess || dev != B.device) return VSG_ERR_INVALID_ARG;
+        // validate, make sure each scene's per-pixel buffers fit (allocates only
+        // on a scene's first frame of a larger resolution)
+        std::vector<char> seen(B.scenes.size(), 0);
+        for (int k = 0; k < n_frames; ++k) {
+            const vsg_batch_frame& f = frames[k];
+            if (f.scene < 0 || f.scene >= (int)B.scenes.size() || seen[f.scene]) return VSG_ERR_INVALID_ARG;
+            seen[f.scene] = 1;
+            if (!f.pointmap || !f.rgb || !f.normals || f.w <= 0 || f.h <= 0) return VSG_ERR_INVALID_ARG;
+            // normal-direction allocation needs its own parent pass: per-scene calls only
+            if (B.scenes[f.scene]->dev.alloc_method == 2) return VSG_ERR_INVALID_ARG;
+            if (f.render) {
+                Renderer* r = B.renderers[f.scene];
+                if (!r || r->w != f.w || r->h != f.h) return VSG_ERR_INVALID_ARG;
             }
+            const int rc = ensure_pixel_buffers(B.scenes[f.scene], (size_t)f.w * f.h);
+            if (rc != VSG_OK) return rc;
         }
-        shape.render_variant = best;
+        // alternate staging buffers; the step that last read this one must be done
+        const int pb = B.parity;
+        B.parity ^= 1;
+        if (B.pending[pb]) {
+            cudaEventSynchronize(B.done[pb]);
+            B.pending[pb] = false;
+        }
+        unsigned char* hs = B.h_step[pb];
+        const BatchLayout L = layout_for(n_frames);
+        BatchHeader* h = reinterpret_cast<BatchHeader*>(hs);
+        AllocArgs* aa = reinterpret_cast<AllocArgs*>(hs + L.alloc_off);
+        IntegArgs* ia = reinterpret_cast<IntegArgs*>(hs + L.integ_off);
+        RenderArgs* ra = reinterpret_cast<RenderArgs*>(hs + L.render_off);
+        h->n = n_frames;
+        std::vector<int> key;
+        key.push_back(n_frames);
+        uint32_t at = 0, rt = 0;
+        for (int k = 0; k < n_frames; ++k) {
+            const vsg_batch_frame& f = frames[k];
+            Scene* sc = B.scenes[f.scene];
+            const int ax = (f.w + kTile - 1) / kTile, ay = (f.h + kTile - 1) / kTile;
+            h->alloc_prefix[k] = at;
+            h->alloc_tiles_x[k] = ax;
+            at += (uint32_t)(ax * ay);
+            const int rx = (f.w + kRenderTileW - 1) / kRenderTileW, ry = (f.h + kRenderTileH - 1) / kRenderTileH;
+            h->render_prefix[k] = rt;
+            h->render_tiles_x[k] = rx;
+            if (f.render) rt += (uint32_t)(rx * ry);
+            key.push_back(f.w);
+            key.push_back(f.h);
+            key.push_back(f.render ? 1 : 0);
+            Pose P;
+            memcpy(P.T, f.pose, sizeof(P.T));
+            AllocArgs& A = aa[k];
+            A.s = sc->dev;
+            A.pm = f.pointmap;
+            A.rgb = f.rgb;
+            A.nm = f.normals;
+            A.W = f.w;
+            A.H = f.h;
+            A.trunc = f.truncation;
+            A.pose = P;
+            IntegArgs& I = ia[k];
+            I.s = sc->dev;
+            I.W = f.w;
+            I.H = f.h;
+            I.trunc = f.truncation;
+            I.pose = P;
+            I.fx = f.fx;
+            I.fy = f.fy;
+            I.cx = f.cx;
+            I.cy = f.cy;
+            RenderArgs& R = ra[k];
+            memset(&R, 0, sizeof(R));
+            R.s = sc->dev;
+            if (f.render) {
+                Renderer* r = B.renderers[f.scene];
+                R.W = f.w;
+                R.H = f.h;
+                R.camx = f.pose[3];
+                R.camy = f.pose[7];
+                R.camz = f.pose[11];
+                R.pose = P;
+                R.pose_dev = nullptr;
+                R.touched = nullptr;
+                R.fx = f.fx;
+                R.fy = f.fy;
+                R.cx = f.cx;
+                R.cy = f.cy;
+                R.minD = f.min_depth;
+                R.maxD = f.max_depth;
+                R.depth = r->depth;
+                R.pos = r->position;
+                R.col = r->color;
+                R.nrm = r->normal;
+                // the renderer's bounds buffer (sized for r->w x r->h == f.w x f.h)
+                R.bounds = r->bounds;
+                R.t1x = (f.w + 7) / 8;
+                R.t2x = (f.w + 63) / 64;
+                R.n1 = R.t1x * ((f.h + 3) / 4);
+                R.n2 = R.t2x * ((f.h + 31) / 32);
+            }
+            sc->integrated_frames++;
+        }
+        h->alloc_prefix[n_frames] = at;
+        h->render_prefix[n_frames] = rt;
+        const size_t bytes = L.bytes;
+        Batch::Shape& shape = B.shapes[key];
+        if (shape.render_variant < 0) {
+            // first step of this shape: run it eagerly, tuning the ray-cast
+            // variant on the step's own data (ray casting leaves the scene as it
+            // is, so repeating it only rewrites the same outputs)
+            if (cudaMemcpyAsync(B.d_step, hs, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) return VSG_ERR_CUDA;
+            enqueue_stages(B, n_frames, at, 0, 0, st);
+            int best = 0;
+            if (rt) {
+                enqueue_bounds(B, n_frames, st);
+                const BatchHeader* dh = reinterpret_cast<const BatchHeader*>(B.d_step);
+                const RenderArgs* dr = reinterpret_cast<const RenderArgs*>(B.d_step + L.render_off);
+                if (B.autotune) {
+                    float best_ms = 3.4e38f;
+                    cudaEvent_t e0, e1;
+                    cudaEventCreate(&e0);
+                    cudaEventCreate(&e1);
+                    for (int v = 0; v < 3; ++v) {
+                        cudaEventRecord(e0, st);
+                        launch_render_variant(v, dim3(rt), st, dh, dr);
+                        cudaEventRecord(e1, st);
+                        cudaEventSynchronize(e1);
+                        float ms = 0.0f;
+                        cudaEventElapsedTime(&ms, e0, e1);
+                        if (ms < best_ms) {
+                            best_ms = ms;
+                            best = v;
+                        }
+                    }
+                    cudaEventDestroy(e0);
+                    cudaEventDestroy(e1);
+                } else {
+                    launch_render_variant(0, dim3(rt), st, dh, dr);
+                }
+            }
+            shape.render_variant = best;
+            cudaEventRecord(B.done[pb], st);
+            B.pending[pb] = true;
+            // capture the step for replay: copy of the argument blocks from
+            // staging buffer i, then the stages; one graph per staging buffer
+            for (int i = 0; i < 2; ++i) {
+                cudaStream_t cs;
+                if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return VSG_ERR_CUDA;
+                cudaGraph_t g = nullptr;
+                cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+                cudaMemcpyAsync(B.d_step, B.h_step[i], bytes, cudaMemcpyHostToDevice, cs);
+                enqueue_stages(B, n_frames, at, rt, best, cs);
+                const cudaError_t ce = cudaStreamEndCapture(cs, &g);
+                cudaStreamDestroy(cs);
+                if (ce != cudaSuccess || !g) return VSG_ERR_CUDA;
+                const cudaError_t ie = cudaGraphInstantiate(&shape.exec[i], g, 0);
+                cudaGraphDestroy(g);
+                if (ie != cudaSuccess) {
+                    shape.exec[i] = nullptr;
+                    return VSG_ERR_CUDA;
+                }
+            }
+            return cudaGetLastError() == cudaSuccess ? VSG_OK : VSG_ERR_CUDA;
+        }
+        if (cudaGraphLaunch(shape.exec[pb], st) != cudaSuccess) return VSG_ERR_CUDA;
         cudaEventRecord(B.done[pb], st);
         B.pending[pb] = true;
-        // capture the step for replay: copy of the argument blocks from
-        // staging buffer i, then the stages; one graph per staging buffer
-        for (int i = 0; i < 2; ++i) {
-            cudaStream_t cs;
-            if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return VSG_ERR_CUDA;
-            cudaGraph_t g = nullptr;
-            cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-            cudaMemcpyAsync(B.d_step, B.h_step[i], bytes, cudaMemcpyHostToDevice, cs);
-            enqueue_stages(B, n_frames, at, rt, best, cs);
-            const cudaError_t ce = cudaStreamEndCapture(cs, &g);
-            cudaStreamDestroy(cs);
-            if (ce != cudaSuccess || !g) return VSG_ERR_CUDA;
-            const cudaError_t ie = cudaGraphInstantiate(&shape.exec[i], g, 0);
-            cudaGraphDestroy(g);
-            if (ie != cudaSuccess) {
-                shape.exec[i] = nullptr;
-                return VSG_ERR_CUDA;
-            }
-        }
         return cudaGetLastError() == cudaSuccess ? VSG_OK : VSG_ERR_CUDA;
-    }
-    if (cudaGraphLaunch(shape.exec[pb], st) != cudaSuccess) return VSG_ERR_CUDA;
-    cudaEventRecord(B.done[pb], st);
-    B.pending[pb] = true;
-    return cudaGetLastError() == cudaSuccess ? VSG_OK : VSG_ERR_CUDA;
+    });
 }
 
 }  // extern "C"

@@ -211,42 +211,44 @@ int vsg_scene_stats(vsg_scene* s, vsg_stats* out) {
 }
 
 int vsg_scene_export(vsg_scene* s, int32_t* coords, uint8_t* voxels, uint32_t max_blocks, uint32_t* n_out) {
-    if (!s || !coords || !n_out) return VSG_ERR_INVALID_ARG;
-    if (cudaDeviceSynchronize() != cudaSuccess) return VSG_ERR_CUDA;
-    vsg::SceneCounters c;
-    if (cudaMemcpy(&c, s->impl.dev.ctr, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return VSG_ERR_CUDA;
-    const uint32_t hw = c.high_water;
-    std::vector<unsigned long long> keys(hw);
-    if (hw && cudaMemcpy(keys.data(), s->impl.dev.block_key, hw * sizeof(unsigned long long),
-                         cudaMemcpyDeviceToHost) != cudaSuccess)
-        return VSG_ERR_CUDA;
-    std::vector<std::pair<std::array<int, 3>, uint32_t>> live;
-    live.reserve(hw);
-    for (uint32_t i = 0; i < hw; ++i) {
-        if (keys[i] == vsg::kKeyEmpty || keys[i] == vsg::kKeyTomb) continue;
-        int x, y, z;
-        vsg::unpack_key(keys[i], x, y, z);
-        live.push_back({{x, y, z}, i});
-    }
-    *n_out = (uint32_t)live.size();
-    if (live.size() > max_blocks) return VSG_ERR_TOO_LARGE;
-    std::sort(live.begin(), live.end());
-    std::vector<vsg::Voxel> vox;
-    if (voxels && hw) {
-        vox.resize((size_t)hw * vsg::kVoxPerBlock);
-        if (cudaMemcpy(vox.data(), s->impl.dev.voxels, vox.size() * sizeof(vsg::Voxel), cudaMemcpyDeviceToHost) !=
-            cudaSuccess)
+    return vsg::host_guard([&]() -> int {
+        if (!s || !coords || !n_out) return VSG_ERR_INVALID_ARG;
+        if (cudaDeviceSynchronize() != cudaSuccess) return VSG_ERR_CUDA;
+        vsg::SceneCounters c;
+        if (cudaMemcpy(&c, s->impl.dev.ctr, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return VSG_ERR_CUDA;
+        const uint32_t hw = c.high_water;
+        std::vector<unsigned long long> keys(hw);
+        if (hw && cudaMemcpy(keys.data(), s->impl.dev.block_key, hw * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost) != cudaSuccess)
             return VSG_ERR_CUDA;
-    }
-    for (size_t i = 0; i < live.size(); ++i) {
-        coords[3 * i + 0] = live[i].first[0];
-        coords[3 * i + 1] = live[i].first[1];
-        coords[3 * i + 2] = live[i].first[2];
-        if (voxels)
-            memcpy(voxels + i * vsg::kVoxPerBlock * 8, vox.data() + (size_t)live[i].second * vsg::kVoxPerBlock,
-                   vsg::kVoxPerBlock * 8);
-    }
-    return VSG_OK;
+        std::vector<std::pair<std::array<int, 3>, uint32_t>> live;
+        live.reserve(hw);
+        for (uint32_t i = 0; i < hw; ++i) {
+            if (keys[i] == vsg::kKeyEmpty || keys[i] == vsg::kKeyTomb) continue;
+            int x, y, z;
+            vsg::unpack_key(keys[i], x, y, z);
+            live.push_back({{x, y, z}, i});
+        }
+        *n_out = (uint32_t)live.size();
+        if (live.size() > max_blocks) return VSG_ERR_TOO_LARGE;
+        std::sort(live.begin(), live.end());
+        std::vector<vsg::Voxel> vox;
+        if (voxels && hw) {
+            vox.resize((size_t)hw * vsg::kVoxPerBlock);
+            if (cudaMemcpy(vox.data(), s->impl.dev.voxels, vox.size() * sizeof(vsg::Voxel), cudaMemcpyDeviceToHost) !=
+                cudaSuccess)
+                return VSG_ERR_CUDA;
+        }
+        for (size_t i = 0; i < live.size(); ++i) {
+            coords[3 * i + 0] = live[i].first[0];
+            coords[3 * i + 1] = live[i].first[1];
+            coords[3 * i + 2] = live[i].first[2];
+            if (voxels)
+                memcpy(voxels + i * vsg::kVoxPerBlock * 8, vox.data() + (size_t)live[i].second * vsg::kVoxPerBlock,
+                       vsg::kVoxPerBlock * 8);
+        }
+        return VSG_OK;
+    });
 }
 
 int vsg_renderer_create(int w, int h, vsg_renderer** out) {
@@ -331,44 +333,46 @@ int vsg_renderer_download(const vsg_renderer* r, float* depth, float* position, 
 }
 
 int vsg_renderer_save_ply(const vsg_renderer* r, const char* path, int64_t* n_points) {
-    if (!r || !path) return VSG_ERR_INVALID_ARG;
-    if (n_points) *n_points = 0;
-    const size_t n = (size_t)r->impl.w * r->impl.h;
-    std::vector<float> D(n);
-    std::vector<float4> P(n), C(n);
-    int rc = vsg_renderer_download(r, D.data(), reinterpret_cast<float*>(P.data()),
-                                   reinterpret_cast<float*>(C.data()), nullptr);
-    if (rc != VSG_OK) return rc;
-    auto valid = [&](size_t i) {
-        return std::isfinite(D[i]) && D[i] > 0.0f && std::fabs(D[i]) < 1e9f && std::isfinite(P[i].x) &&
-               std::isfinite(P[i].y) && std::isfinite(P[i].z);
-    };
-    int64_t count = 0;
-    for (size_t i = 0; i < n; ++i) count += valid(i) ? 1 : 0;
-    if (count == 0) return VSG_ERR_INVALID_ARG;
-    std::error_code ec;
-    const std::filesystem::path out(path);
-    if (out.has_parent_path()) std::filesystem::create_directories(out.parent_path(), ec);
-    FILE* f = std::fopen(path, "w");
-    if (!f) return VSG_ERR_INVALID_ARG;
-    std::fprintf(f,
-                 "ply\nformat ascii 1.0\ncomment Generated by RayCastRender\nelement vertex %lld\n"
-                 "property float x\nproperty float y\nproperty float z\n"
-                 "property uchar red\nproperty uchar green\nproperty uchar blue\nend_header\n",
-                 (long long)count);
-    auto channel = [](float c) -> int {
-        if (!std::isfinite(c)) return 255;
-        c = c < 0.0f ? 0.0f : (c > 1.0f ? 1.0f : c);
-        return static_cast<int>(c * 255.0f + 0.5f);
-    };
-    for (size_t i = 0; i < n; ++i) {
-        if (!valid(i)) continue;
-        std::fprintf(f, "%g %g %g %d %d %d\n", P[i].x, P[i].y, P[i].z, channel(C[i].x), channel(C[i].y),
-                     channel(C[i].z));
-    }
-    if (std::fclose(f) != 0) return VSG_ERR_INVALID_ARG;
-    if (n_points) *n_points = count;
-    return VSG_OK;
+    return vsg::host_guard([&]() -> int {
+        if (!r || !path) return VSG_ERR_INVALID_ARG;
+        if (n_points) *n_points = 0;
+        const size_t n = (size_t)r->impl.w * r->impl.h;
+        std::vector<float> D(n);
+        std::vector<float4> P(n), C(n);
+        int rc = vsg_renderer_download(r, D.data(), reinterpret_cast<float*>(P.data()),
+                                       reinterpret_cast<float*>(C.data()), nullptr);
+        if (rc != VSG_OK) return rc;
+        auto valid = [&](size_t i) {
+            return std::isfinite(D[i]) && D[i] > 0.0f && std::fabs(D[i]) < 1e9f && std::isfinite(P[i].x) &&
+                   std::isfinite(P[i].y) && std::isfinite(P[i].z);
+        };
+        int64_t count = 0;
+        for (size_t i = 0; i < n; ++i) count += valid(i) ? 1 : 0;
+        if (count == 0) return VSG_ERR_INVALID_ARG;
+        std::error_code ec;
+        const std::filesystem::path out(path);
+        if (out.has_parent_path()) std::filesystem::create_directories(out.parent_path(), ec);
+        FILE* f = std::fopen(path, "w");
+        if (!f) return VSG_ERR_INVALID_ARG;
+        std::fprintf(f,
+                     "ply\nformat ascii 1.0\ncomment Generated by RayCastRender\nelement vertex %lld\n"
+                     "property float x\nproperty float y\nproperty float z\n"
+                     "property uchar red\nproperty uchar green\nproperty uchar blue\nend_header\n",
+                     (long long)count);
+        auto channel = [](float c) -> int {
+            if (!std::isfinite(c)) return 255;
+            c = c < 0.0f ? 0.0f : (c > 1.0f ? 1.0f : c);
+            return static_cast<int>(c * 255.0f + 0.5f);
+        };
+        for (size_t i = 0; i < n; ++i) {
+            if (!valid(i)) continue;
+            std::fprintf(f, "%g %g %g %d %d %d\n", P[i].x, P[i].y, P[i].z, channel(C[i].x), channel(C[i].y),
+                         channel(C[i].z));
+        }
+        if (std::fclose(f) != 0) return VSG_ERR_INVALID_ARG;
+        if (n_points) *n_points = count;
+        return VSG_OK;
+    });
 }
 
 int vsg_timing_enable(vsg_scene* s, int enable) {

@@ -6,7 +6,25 @@
 #include "../../include/vsg.h"
 #include "vsg_device.cuh"
 
+#include <new>
+#include <stdexcept>
+
 namespace vsg {
+
+// Host-side entry points run their body through this: an exception (host
+// memory exhausted) becomes an error code instead of crossing the C ABI.
+template <class F>
+int host_guard(F&& f) noexcept {
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        return VSG_ERR_OUT_OF_MEMORY;
+    } catch (const std::length_error&) {
+        return VSG_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        return VSG_ERR_INVALID_ARG;
+    }
+}
 
 enum TimingSlot {
     kSlotAlloc = 0,

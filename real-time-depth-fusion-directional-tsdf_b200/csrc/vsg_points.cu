@@ -292,37 +292,39 @@ int vsg_points_download(const vsg_points* m, float* positions, float* colors, fl
 // written points with finite positions; colour channels clamped to [0, 1]
 // and rounded to 0..255 (non-finite -> 255).
 int vsg_points_save_ply(const vsg_points* m, const char* path) {
-    if (!m || !path) return VSG_ERR_INVALID_ARG;
-    int64_t n = 0;
-    int rc = vsg_points_count(m, &n);
-    if (rc != VSG_OK) return rc;
-    const size_t k = (size_t)(n < m->impl.max_pts ? n : m->impl.max_pts);
-    std::vector<float4> P(k), C(k), N(k);
-    rc = vsg_points_download(m, reinterpret_cast<float*>(P.data()), reinterpret_cast<float*>(C.data()),
-                             reinterpret_cast<float*>(N.data()), nullptr);
-    if (rc != VSG_OK) return rc;
-    size_t valid = 0;
-    for (size_t i = 0; i < k; ++i)
-        if (std::isfinite(P[i].x) && std::isfinite(P[i].y) && std::isfinite(P[i].z)) ++valid;
-    FILE* f = std::fopen(path, "w");
-    if (!f) return VSG_ERR_INVALID_ARG;
-    std::fprintf(f,
-                 "ply\nformat ascii 1.0\ncomment Generated by RayCastRender::extractSurfacePoints\n"
-                 "element vertex %zu\nproperty float x\nproperty float y\nproperty float z\n"
-                 "property float nx\nproperty float ny\nproperty float nz\n"
-                 "property uchar red\nproperty uchar green\nproperty uchar blue\nend_header\n",
-                 valid);
-    auto channel = [](float c) -> int {
-        if (!std::isfinite(c)) return 255;
-        c = c < 0.0f ? 0.0f : (c > 1.0f ? 1.0f : c);
-        return static_cast<int>(c * 255.0f + 0.5f);
-    };
-    for (size_t i = 0; i < k; ++i) {
-        if (!(std::isfinite(P[i].x) && std::isfinite(P[i].y) && std::isfinite(P[i].z))) continue;
-        std::fprintf(f, "%g %g %g %g %g %g %d %d %d\n", P[i].x, P[i].y, P[i].z, N[i].x, N[i].y, N[i].z,
-                     channel(C[i].x), channel(C[i].y), channel(C[i].z));
-    }
-    return std::fclose(f) == 0 ? VSG_OK : VSG_ERR_INVALID_ARG;
+    return vsg::host_guard([&]() -> int {
+        if (!m || !path) return VSG_ERR_INVALID_ARG;
+        int64_t n = 0;
+        int rc = vsg_points_count(m, &n);
+        if (rc != VSG_OK) return rc;
+        const size_t k = (size_t)(n < m->impl.max_pts ? n : m->impl.max_pts);
+        std::vector<float4> P(k), C(k), N(k);
+        rc = vsg_points_download(m, reinterpret_cast<float*>(P.data()), reinterpret_cast<float*>(C.data()),
+                                 reinterpret_cast<float*>(N.data()), nullptr);
+        if (rc != VSG_OK) return rc;
+        size_t valid = 0;
+        for (size_t i = 0; i < k; ++i)
+            if (std::isfinite(P[i].x) && std::isfinite(P[i].y) && std::isfinite(P[i].z)) ++valid;
+        FILE* f = std::fopen(path, "w");
+        if (!f) return VSG_ERR_INVALID_ARG;
+        std::fprintf(f,
+                     "ply\nformat ascii 1.0\ncomment Generated by RayCastRender::extractSurfacePoints\n"
+                     "element vertex %zu\nproperty float x\nproperty float y\nproperty float z\n"
+                     "property float nx\nproperty float ny\nproperty float nz\n"
+                     "property uchar red\nproperty uchar green\nproperty uchar blue\nend_header\n",
+                     valid);
+        auto channel = [](float c) -> int {
+            if (!std::isfinite(c)) return 255;
+            c = c < 0.0f ? 0.0f : (c > 1.0f ? 1.0f : c);
+            return static_cast<int>(c * 255.0f + 0.5f);
+        };
+        for (size_t i = 0; i < k; ++i) {
+            if (!(std::isfinite(P[i].x) && std::isfinite(P[i].y) && std::isfinite(P[i].z))) continue;
+            std::fprintf(f, "%g %g %g %g %g %g %d %d %d\n", P[i].x, P[i].y, P[i].z, N[i].x, N[i].y, N[i].z,
+                         channel(C[i].x), channel(C[i].y), channel(C[i].z));
+        }
+        return std::fclose(f) == 0 ? VSG_OK : VSG_ERR_INVALID_ARG;
+    });
 }
 
 }  // extern "C"

@@ -278,13 +278,15 @@ struct BlockStore {
             free_slabs.pop_back();
             return s;
         }
-        slab_mem.emplace_back(new Voxel[kSlabBlocks * kVoxPerBlock]);
+        std::unique_ptr<Voxel[]> m(new Voxel[kSlabBlocks * kVoxPerBlock]);
+        slab_mem.push_back(std::move(m));
         return slab_mem.back().get();
     }
     // drop a chunk, keeping its slabs for reuse
     void erase_chunk(const std::array<int, 3>& ck) {
         auto it = chunks.find(ck);
         if (it == chunks.end()) return;
+        free_slabs.reserve(free_slabs.size() + it->second.slabs.size());
         n_blocks -= it->second.coords.size();
         for (Voxel* s : it->second.slabs) free_slabs.push_back(s);
         chunks.erase(it);
@@ -320,7 +322,9 @@ struct BlockStore {
     }
 
     // File one block into its chunk; returns 1 when the block is new.  With
-    // a lock, slabs are taken under it (chunk-parallel filing).
+    // a lock, slabs are taken under it (chunk-parallel filing).  Every
+    // allocation comes before the block is entered, so std::bad_alloc leaves
+    // the chunk's blocks as they were (at most a spare slab is kept).
     int add_to(Chunk& ch, int x, int y, int z, const Voxel* v, std::mutex* lock) {
         const std::array<int, 3> key{x, y, z};
         auto it = ch.index.find(key);
@@ -330,13 +334,17 @@ struct BlockStore {
             return 0;
         }
         const size_t i = ch.coords.size();
-        if (i % kSlabBlocks == 0) {
+        if (ch.coords.size() == ch.coords.capacity()) ch.coords.reserve(std::max<size_t>(16, 2 * i));
+        if (i / kSlabBlocks >= ch.slabs.size()) {
+            if (ch.slabs.size() == ch.slabs.capacity()) ch.slabs.reserve(std::max<size_t>(4, 2 * ch.slabs.size()));
+            Voxel* slab;
             if (lock) {
                 std::lock_guard<std::mutex> g(*lock);
-                ch.slabs.push_back(new_slab());
+                slab = new_slab();
             } else {
-                ch.slabs.push_back(new_slab());
+                slab = new_slab();
             }
+            ch.slabs.push_back(slab);
         }
         ch.index.emplace(key, (uint32_t)i);
         ch.coords.push_back(key);
@@ -373,23 +381,34 @@ struct BlockStore {
         std::mutex lock;
         std::atomic<uint32_t> next{0};
         std::atomic<uint64_t> added{0};
+        std::atomic<bool> out_of_memory{false};
         auto work = [&]() {
             uint64_t mine = 0;
-            for (uint32_t g; (g = next.fetch_add(1)) < groups.size();)
-                for (uint32_t k = groups[g].begin; k < groups[g].end; ++k) {
-                    const uint32_t i = keyed[k].second;
-                    mine += (uint64_t)add_to(*groups[g].ch, info[i].x, info[i].y, info[i].z,
-                                             vox + (size_t)i * kVoxPerBlock, &lock);
-                }
+            try {
+                for (uint32_t g; (g = next.fetch_add(1)) < groups.size();)
+                    for (uint32_t k = groups[g].begin; k < groups[g].end; ++k) {
+                        const uint32_t i = keyed[k].second;
+                        mine += (uint64_t)add_to(*groups[g].ch, info[i].x, info[i].y, info[i].z,
+                                                 vox + (size_t)i * kVoxPerBlock, &lock);
+                    }
+            } catch (...) {  // host memory exhausted: stop every thread, report after the join
+                out_of_memory = true;
+                next = (uint32_t)groups.size();
+            }
             added += mine;
         };
         const unsigned hw = std::thread::hardware_concurrency();
         const unsigned nt = std::min<unsigned>(std::min<unsigned>(hw ? hw : 1u, 8u), (unsigned)groups.size());
         std::vector<std::thread> pool;
-        for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
+        try {
+            pool.reserve(nt);
+            for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
+        } catch (...) {  // fewer threads: the ones started and this one take every group
+        }
         work();
         for (auto& th : pool) th.join();
         n_blocks += added.load();
+        if (out_of_memory) throw std::bad_alloc();
     }
 
     // streamInFindChunk, :993-1140: the chunks a stream-in takes (sorted,
@@ -479,9 +498,15 @@ int insert_blocks(Scene* sc, const std::vector<std::array<int, 3>>& coords, cons
         const unsigned hw = std::thread::hardware_concurrency();
         const unsigned nt = n < 512 ? 1u : std::min<unsigned>(hw ? hw : 1u, 8u);
         std::vector<std::thread> pool;
-        for (unsigned t = 1; t < nt; ++t) pool.emplace_back(gather, (uint32_t)((uint64_t)n * t / nt),
-                                                            (uint32_t)((uint64_t)n * (t + 1) / nt));
+        unsigned started = 1;  // ranges 1 .. started-1 run on their own threads
+        try {
+            pool.reserve(nt);
+            for (unsigned t = 1; t < nt; ++t, ++started)
+                pool.emplace_back(gather, (uint32_t)((uint64_t)n * t / nt), (uint32_t)((uint64_t)n * (t + 1) / nt));
+        } catch (...) {  // a thread could not start: this thread gathers the rest
+        }
         gather(0, (uint32_t)((uint64_t)n / nt));
+        if (started < nt) gather((uint32_t)((uint64_t)n * started / nt), n);
         for (auto& th : pool) th.join();
         if (cudaMemsetAsync(sg->d_ctr, 0, sizeof(StreamCounters), st) != cudaSuccess ||
             cudaMemcpyAsync(sg->d_info, sg->h_info, n * sizeof(int4), cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -657,194 +682,223 @@ int vsg_store_info(const vsg_block_store* st, uint64_t* n_blocks, uint64_t* n_ch
 
 int vsg_store_count(const vsg_block_store* st, const float center[3], float radius, uint64_t* n_blocks,
                     uint64_t* n_chunks) {
-    if (!st || (!center && radius >= 0.0f)) return VSG_ERR_INVALID_ARG;
-    const float zero[3] = {0.0f, 0.0f, 0.0f};
-    const std::vector<std::array<int, 3>> take = st->impl.chunks_for(center ? center : zero, radius);
-    uint64_t nb = 0;
-    for (const auto& ck : take) nb += st->impl.chunks.at(ck).coords.size();
-    if (n_blocks) *n_blocks = nb;
-    if (n_chunks) *n_chunks = take.size();
-    return VSG_OK;
+    return vsg::host_guard([&]() -> int {
+        if (!st || (!center && radius >= 0.0f)) return VSG_ERR_INVALID_ARG;
+        const float zero[3] = {0.0f, 0.0f, 0.0f};
+        const std::vector<std::array<int, 3>> take = st->impl.chunks_for(center ? center : zero, radius);
+        uint64_t nb = 0;
+        for (const auto& ck : take) nb += st->impl.chunks.at(ck).coords.size();
+        if (n_blocks) *n_blocks = nb;
+        if (n_chunks) *n_chunks = take.size();
+        return VSG_OK;
+    });
 }
 
 int vsg_store_add_records(vsg_block_store* st, float voxel_size, const int32_t* infos, const uint8_t* voxels,
                           uint64_t n) {
-    if (!st || !(voxel_size > 0.0f) || (n && (!infos || !voxels))) return VSG_ERR_INVALID_ARG;
-    if (n == 0) return VSG_OK;
-    if (st->impl.n_blocks && st->impl.voxel != voxel_size) return VSG_ERR_INVALID_ARG;
-    st->impl.voxel = voxel_size;
-    std::vector<vsg::Voxel> blk(vsg::kVoxPerBlock);
-    for (uint64_t i = 0; i < n; ++i) {
-        const uint8_t* src = voxels + i * (uint64_t)vsg::kVoxPerBlock * 12u;
-        for (int v = 0; v < vsg::kVoxPerBlock; ++v) blk[v] = from_ref_voxel(src + 12 * v);
-        st->impl.add(infos[4 * i], infos[4 * i + 1], infos[4 * i + 2], blk.data(), voxel_size);
-    }
-    return VSG_OK;
+    return vsg::host_guard([&]() -> int {
+        if (!st || !(voxel_size > 0.0f) || (n && (!infos || !voxels))) return VSG_ERR_INVALID_ARG;
+        if (n == 0) return VSG_OK;
+        if (st->impl.n_blocks && st->impl.voxel != voxel_size) return VSG_ERR_INVALID_ARG;
+        st->impl.voxel = voxel_size;
+        // converted and filed in passes of up to 8192 blocks (add_many: chunk-parallel,
+        // repeats merged in input order)
+        const uint64_t pass = std::min<uint64_t>(n, 8192);
+        std::vector<int4> info((size_t)pass);
+        std::vector<vsg::Voxel> blk((size_t)pass * vsg::kVoxPerBlock);
+        for (uint64_t done = 0; done < n;) {
+            const uint32_t m = (uint32_t)std::min<uint64_t>(pass, n - done);
+            for (uint32_t j = 0; j < m; ++j) {
+                const uint64_t i = done + j;
+                info[j] = make_int4(infos[4 * i], infos[4 * i + 1], infos[4 * i + 2], -1);
+                const uint8_t* src = voxels + i * (uint64_t)vsg::kVoxPerBlock * 12u;
+                for (int v = 0; v < vsg::kVoxPerBlock; ++v)
+                    blk[(size_t)j * vsg::kVoxPerBlock + v] = from_ref_voxel(src + 12 * v);
+            }
+            st->impl.add_many(info.data(), blk.data(), m, voxel_size);
+            done += m;
+        }
+        return VSG_OK;
+    });
 }
 
 int vsg_store_export(const vsg_block_store* st, int32_t* coords, uint8_t* voxels, uint64_t max_blocks,
                      uint64_t* n_out) {
-    if (!st || !n_out) return VSG_ERR_INVALID_ARG;
-    *n_out = st->impl.n_blocks;
-    if (st->impl.n_blocks > max_blocks) return VSG_ERR_TOO_LARGE;
-    if (!coords) return VSG_ERR_INVALID_ARG;
-    std::vector<std::pair<std::array<int, 3>, const vsg::Voxel*>> all;
-    all.reserve(st->impl.n_blocks);
-    for (const auto& kv : st->impl.chunks)
-        for (size_t i = 0; i < kv.second.coords.size(); ++i)
-            all.push_back({kv.second.coords[i], kv.second.block(i)});
-    std::sort(all.begin(), all.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-    for (size_t i = 0; i < all.size(); ++i) {
-        coords[3 * i + 0] = all[i].first[0];
-        coords[3 * i + 1] = all[i].first[1];
-        coords[3 * i + 2] = all[i].first[2];
-        if (voxels) std::memcpy(voxels + i * vsg::kVoxPerBlock * 8, all[i].second, vsg::kVoxPerBlock * 8);
-    }
-    return VSG_OK;
+    return vsg::host_guard([&]() -> int {
+        if (!st || !n_out) return VSG_ERR_INVALID_ARG;
+        *n_out = st->impl.n_blocks;
+        if (st->impl.n_blocks > max_blocks) return VSG_ERR_TOO_LARGE;
+        if (!coords) return VSG_ERR_INVALID_ARG;
+        std::vector<std::pair<std::array<int, 3>, const vsg::Voxel*>> all;
+        all.reserve(st->impl.n_blocks);
+        for (const auto& kv : st->impl.chunks)
+            for (size_t i = 0; i < kv.second.coords.size(); ++i)
+                all.push_back({kv.second.coords[i], kv.second.block(i)});
+        std::sort(all.begin(), all.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        for (size_t i = 0; i < all.size(); ++i) {
+            coords[3 * i + 0] = all[i].first[0];
+            coords[3 * i + 1] = all[i].first[1];
+            coords[3 * i + 2] = all[i].first[2];
+            if (voxels) std::memcpy(voxels + i * vsg::kVoxPerBlock * 8, all[i].second, vsg::kVoxPerBlock * 8);
+        }
+        return VSG_OK;
+    });
 }
 
 int vsg_store_save(const vsg_block_store* st, const char* path) {
-    if (!st || !path) return VSG_ERR_INVALID_ARG;
-    std::vector<std::array<int, 3>> coords;
-    std::vector<const vsg::Voxel*> vox;
-    for (const auto& kv : st->impl.chunks)
-        for (size_t i = 0; i < kv.second.coords.size(); ++i) {
-            coords.push_back(kv.second.coords[i]);
-            vox.push_back(kv.second.block(i));
-        }
-    return write_blocks(path, st->impl.voxel, coords, vox);
+    return vsg::host_guard([&]() -> int {
+        if (!st || !path) return VSG_ERR_INVALID_ARG;
+        std::vector<std::array<int, 3>> coords;
+        std::vector<const vsg::Voxel*> vox;
+        for (const auto& kv : st->impl.chunks)
+            for (size_t i = 0; i < kv.second.coords.size(); ++i) {
+                coords.push_back(kv.second.coords[i]);
+                vox.push_back(kv.second.block(i));
+            }
+        return write_blocks(path, st->impl.voxel, coords, vox);
+    });
 }
 
 int vsg_store_load(vsg_block_store* st, const char* path) {
-    if (!st || !path) return VSG_ERR_INVALID_ARG;
-    float voxel = 0.0f;
-    std::vector<std::array<int, 3>> coords;
-    std::vector<vsg::Voxel> vox;
-    const int rc = read_blocks(path, &voxel, &coords, &vox);
-    if (rc != VSG_OK) return rc;
-    if (coords.empty()) return VSG_OK;
-    if (st->impl.n_blocks && st->impl.voxel != voxel) return VSG_ERR_INVALID_ARG;
-    st->impl.voxel = voxel;
-    for (size_t i = 0; i < coords.size(); ++i)
-        st->impl.add(coords[i][0], coords[i][1], coords[i][2], vox.data() + i * vsg::kVoxPerBlock, voxel);
-    return VSG_OK;
+    return vsg::host_guard([&]() -> int {
+        if (!st || !path) return VSG_ERR_INVALID_ARG;
+        float voxel = 0.0f;
+        std::vector<std::array<int, 3>> coords;
+        std::vector<vsg::Voxel> vox;
+        const int rc = read_blocks(path, &voxel, &coords, &vox);
+        if (rc != VSG_OK) return rc;
+        if (coords.empty()) return VSG_OK;
+        if (st->impl.n_blocks && st->impl.voxel != voxel) return VSG_ERR_INVALID_ARG;
+        st->impl.voxel = voxel;
+        for (size_t i = 0; i < coords.size(); ++i)
+            st->impl.add(coords[i][0], coords[i][1], coords[i][2], vox.data() + i * vsg::kVoxPerBlock, voxel);
+        return VSG_OK;
+    });
 }
 
 int vsg_stream_out(vsg_scene* s, vsg_block_store* store, const float center[3], float radius, uint32_t* n_out,
                    vsg_stream_t stream) {
-    if (!s || !store || !center || !scene_on_current_device(s)) return VSG_ERR_INVALID_ARG;
-    vsg::Scene* sc = &s->impl;
-    const float voxel = sc->params.voxel_size;
-    if (store->impl.n_blocks && store->impl.voxel != voxel) return VSG_ERR_INVALID_ARG;
-    vsg::StreamStage* sg = nullptr;
-    int rc = vsg::stage_for(sc, &sg);
-    if (rc != VSG_OK) return rc;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    uint32_t total = 0;
-    for (;;) {
-        if (cudaMemsetAsync(sg->d_ctr, 0, sizeof(vsg::StreamCounters), st) != cudaSuccess) return VSG_ERR_CUDA;
-        vsg::k_stream_select<<<sc->sm_count * 4, 256, 0, st>>>(sc->dev, center[0], center[1], center[2], radius,
-                                                               sg->d_list, vsg::kStageBlocks, sg->d_ctr);
-        if (cudaGetLastError() != cudaSuccess) return VSG_ERR_CUDA;
-        vsg::StreamCounters c{};
-        rc = vsg::read_counters(sg, &c, st);
+    return vsg::host_guard([&]() -> int {
+        if (!s || !store || !center || !scene_on_current_device(s)) return VSG_ERR_INVALID_ARG;
+        vsg::Scene* sc = &s->impl;
+        const float voxel = sc->params.voxel_size;
+        if (store->impl.n_blocks && store->impl.voxel != voxel) return VSG_ERR_INVALID_ARG;
+        vsg::StreamStage* sg = nullptr;
+        int rc = vsg::stage_for(sc, &sg);
         if (rc != VSG_OK) return rc;
-        const uint32_t n = std::min(c.found, vsg::kStageBlocks);
-        if (n == 0) break;
-        vsg::k_stream_extract<<<vsg::grid_for(sc, n), 256, 0, st>>>(sc->dev, sg->d_list, n, sg->d_info, sg->d_vox);
-        if (cudaGetLastError() != cudaSuccess ||
-            cudaMemcpyAsync(sg->h_info, sg->d_info, n * sizeof(int4), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-            cudaMemcpyAsync(sg->h_vox, sg->d_vox, (size_t)n * vsg::kVoxPerBlock * sizeof(vsg::Voxel),
-                            cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-            cudaStreamSynchronize(st) != cudaSuccess)
-            return VSG_ERR_CUDA;
-        store->impl.voxel = voxel;
-        store->impl.add_many(sg->h_info, sg->h_vox, n, voxel);
-        total += n;
-        if (c.found <= vsg::kStageBlocks) break;
-    }
-    if (n_out) *n_out = total;
-    return VSG_OK;
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        uint32_t total = 0;
+        for (;;) {
+            if (cudaMemsetAsync(sg->d_ctr, 0, sizeof(vsg::StreamCounters), st) != cudaSuccess) return VSG_ERR_CUDA;
+            vsg::k_stream_select<<<sc->sm_count * 4, 256, 0, st>>>(sc->dev, center[0], center[1], center[2], radius,
+                                                                   sg->d_list, vsg::kStageBlocks, sg->d_ctr);
+            if (cudaGetLastError() != cudaSuccess) return VSG_ERR_CUDA;
+            vsg::StreamCounters c{};
+            rc = vsg::read_counters(sg, &c, st);
+            if (rc != VSG_OK) return rc;
+            const uint32_t n = std::min(c.found, vsg::kStageBlocks);
+            if (n == 0) break;
+            vsg::k_stream_extract<<<vsg::grid_for(sc, n), 256, 0, st>>>(sc->dev, sg->d_list, n, sg->d_info, sg->d_vox);
+            if (cudaGetLastError() != cudaSuccess ||
+                cudaMemcpyAsync(sg->h_info, sg->d_info, n * sizeof(int4), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaMemcpyAsync(sg->h_vox, sg->d_vox, (size_t)n * vsg::kVoxPerBlock * sizeof(vsg::Voxel),
+                                cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return VSG_ERR_CUDA;
+            store->impl.voxel = voxel;
+            store->impl.add_many(sg->h_info, sg->h_vox, n, voxel);
+            total += n;
+            if (c.found <= vsg::kStageBlocks) break;
+        }
+        if (n_out) *n_out = total;
+        return VSG_OK;
+    });
 }
 
 int vsg_stream_in(vsg_scene* s, vsg_block_store* store, const float center[3], float radius, uint32_t* n_in,
                   uint32_t* n_merged, vsg_stream_t stream) {
-    if (!s || !store || (!center && radius >= 0.0f) || !scene_on_current_device(s)) return VSG_ERR_INVALID_ARG;
-    vsg::Scene* sc = &s->impl;
-    vsg::BlockStore& bs = store->impl;
-    if (n_in) *n_in = 0;
-    if (n_merged) *n_merged = 0;
-    if (bs.n_blocks == 0) return VSG_OK;
-    if (bs.voxel != sc->params.voxel_size) return VSG_ERR_INVALID_ARG;
-    const float zero[3] = {0.0f, 0.0f, 0.0f};
-    const std::vector<std::array<int, 3>> take = bs.chunks_for(center ? center : zero, radius);
-    std::vector<std::array<int, 3>> coords;
-    std::vector<const vsg::Voxel*> vox;
-    for (const auto& ck : take) {
-        const vsg::Chunk& ch = bs.chunks.at(ck);
-        for (size_t i = 0; i < ch.coords.size(); ++i) {
-            coords.push_back(ch.coords[i]);
-            vox.push_back(ch.block(i));
+    return vsg::host_guard([&]() -> int {
+        if (!s || !store || (!center && radius >= 0.0f) || !scene_on_current_device(s)) return VSG_ERR_INVALID_ARG;
+        vsg::Scene* sc = &s->impl;
+        vsg::BlockStore& bs = store->impl;
+        if (n_in) *n_in = 0;
+        if (n_merged) *n_merged = 0;
+        if (bs.n_blocks == 0) return VSG_OK;
+        if (bs.voxel != sc->params.voxel_size) return VSG_ERR_INVALID_ARG;
+        const float zero[3] = {0.0f, 0.0f, 0.0f};
+        const std::vector<std::array<int, 3>> take = bs.chunks_for(center ? center : zero, radius);
+        std::vector<std::array<int, 3>> coords;
+        std::vector<const vsg::Voxel*> vox;
+        for (const auto& ck : take) {
+            const vsg::Chunk& ch = bs.chunks.at(ck);
+            for (size_t i = 0; i < ch.coords.size(); ++i) {
+                coords.push_back(ch.coords[i]);
+                vox.push_back(ch.block(i));
+            }
         }
-    }
-    if (coords.empty()) return VSG_OK;
-    // the pool must hold every incoming block (a merge needs none, so the
-    // test is conservative); otherwise nothing moves
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    uint64_t free_blocks = 0;
-    int rc = free_pool_blocks(sc, st, &free_blocks);
-    if (rc != VSG_OK) return rc;
-    if (free_blocks < coords.size()) return VSG_ERR_TOO_LARGE;
-    uint32_t merged = 0, failed = 0;
-    rc = vsg::insert_blocks(sc, coords, vox, st, &merged, &failed);
-    if (rc != VSG_OK) return rc;
-    for (const auto& ck : take) {
-        bs.erase_chunk(ck);
-    }
-    if (n_in) *n_in = (uint32_t)coords.size() - failed;
-    if (n_merged) *n_merged = merged;
-    return failed ? VSG_ERR_OUT_OF_MEMORY : VSG_OK;
+        if (coords.empty()) return VSG_OK;
+        // the pool must hold every incoming block (a merge needs none, so the
+        // test is conservative); otherwise nothing moves
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        uint64_t free_blocks = 0;
+        int rc = free_pool_blocks(sc, st, &free_blocks);
+        if (rc != VSG_OK) return rc;
+        if (free_blocks < coords.size()) return VSG_ERR_TOO_LARGE;
+        uint32_t merged = 0, failed = 0;
+        rc = vsg::insert_blocks(sc, coords, vox, st, &merged, &failed);
+        if (rc != VSG_OK) return rc;
+        for (const auto& ck : take) {
+            bs.erase_chunk(ck);
+        }
+        if (n_in) *n_in = (uint32_t)coords.size() - failed;
+        if (n_merged) *n_merged = merged;
+        return failed ? VSG_ERR_OUT_OF_MEMORY : VSG_OK;
+    });
 }
 
 int vsg_scene_save(vsg_scene* s, const char* path) {
-    if (!s || !path) return VSG_ERR_INVALID_ARG;
-    uint32_t n = 0;
-    int32_t dummy[3];
-    int rc = vsg_scene_export(s, dummy, nullptr, 0, &n);
-    if (rc != VSG_OK && rc != VSG_ERR_TOO_LARGE) return rc;
-    std::vector<int32_t> c((size_t)n * 3 + 3);
-    std::vector<vsg::Voxel> v((size_t)n * vsg::kVoxPerBlock + 1);
-    rc = vsg_scene_export(s, c.data(), reinterpret_cast<uint8_t*>(v.data()), n, &n);
-    if (rc != VSG_OK) return rc;
-    std::vector<std::array<int, 3>> coords(n);
-    std::vector<const vsg::Voxel*> vox(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        coords[i] = {c[3 * i], c[3 * i + 1], c[3 * i + 2]};
-        vox[i] = v.data() + (size_t)i * vsg::kVoxPerBlock;
-    }
-    return write_blocks(path, s->impl.params.voxel_size, coords, vox);
+    return vsg::host_guard([&]() -> int {
+        if (!s || !path) return VSG_ERR_INVALID_ARG;
+        uint32_t n = 0;
+        int32_t dummy[3];
+        int rc = vsg_scene_export(s, dummy, nullptr, 0, &n);
+        if (rc != VSG_OK && rc != VSG_ERR_TOO_LARGE) return rc;
+        std::vector<int32_t> c((size_t)n * 3 + 3);
+        std::vector<vsg::Voxel> v((size_t)n * vsg::kVoxPerBlock + 1);
+        rc = vsg_scene_export(s, c.data(), reinterpret_cast<uint8_t*>(v.data()), n, &n);
+        if (rc != VSG_OK) return rc;
+        std::vector<std::array<int, 3>> coords(n);
+        std::vector<const vsg::Voxel*> vox(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            coords[i] = {c[3 * i], c[3 * i + 1], c[3 * i + 2]};
+            vox[i] = v.data() + (size_t)i * vsg::kVoxPerBlock;
+        }
+        return write_blocks(path, s->impl.params.voxel_size, coords, vox);
+    });
 }
 
 int vsg_scene_load(vsg_scene* s, const char* path, vsg_stream_t stream) {
-    if (!s || !path || !scene_on_current_device(s)) return VSG_ERR_INVALID_ARG;
-    float voxel = 0.0f;
-    std::vector<std::array<int, 3>> coords;
-    std::vector<vsg::Voxel> vox;
-    int rc = read_blocks(path, &voxel, &coords, &vox);
-    if (rc != VSG_OK) return rc;
-    if (coords.empty()) return VSG_OK;
-    if (voxel != s->impl.params.voxel_size) return VSG_ERR_INVALID_ARG;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    uint64_t free_blocks = 0;
-    rc = free_pool_blocks(&s->impl, st, &free_blocks);
-    if (rc != VSG_OK) return rc;
-    if (free_blocks < coords.size()) return VSG_ERR_TOO_LARGE;
-    std::vector<const vsg::Voxel*> ptrs(coords.size());
-    for (size_t i = 0; i < coords.size(); ++i) ptrs[i] = vox.data() + i * vsg::kVoxPerBlock;
-    uint32_t failed = 0;
-    rc = vsg::insert_blocks(&s->impl, coords, ptrs, st, nullptr, &failed);
-    if (rc != VSG_OK) return rc;
-    return failed ? VSG_ERR_OUT_OF_MEMORY : VSG_OK;
+    return vsg::host_guard([&]() -> int {
+        if (!s || !path || !scene_on_current_device(s)) return VSG_ERR_INVALID_ARG;
+        float voxel = 0.0f;
+        std::vector<std::array<int, 3>> coords;
+        std::vector<vsg::Voxel> vox;
+        int rc = read_blocks(path, &voxel, &coords, &vox);
+        if (rc != VSG_OK) return rc;
+        if (coords.empty()) return VSG_OK;
+        if (voxel != s->impl.params.voxel_size) return VSG_ERR_INVALID_ARG;
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        uint64_t free_blocks = 0;
+        rc = free_pool_blocks(&s->impl, st, &free_blocks);
+        if (rc != VSG_OK) return rc;
+        if (free_blocks < coords.size()) return VSG_ERR_TOO_LARGE;
+        std::vector<const vsg::Voxel*> ptrs(coords.size());
+        for (size_t i = 0; i < coords.size(); ++i) ptrs[i] = vox.data() + i * vsg::kVoxPerBlock;
+        uint32_t failed = 0;
+        rc = vsg::insert_blocks(&s->impl, coords, ptrs, st, nullptr, &failed);
+        if (rc != VSG_OK) return rc;
+        return failed ? VSG_ERR_OUT_OF_MEMORY : VSG_OK;
+    });
 }
 
 }  // extern "C"

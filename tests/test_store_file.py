@@ -148,3 +148,35 @@ def test_store_records_and_counts(oracle_mod):
     assert st.count(None, -1.0)[0] == len(coords)
     with pytest.raises(vsg.VsgError):
         st.add_records(0.008, infos[:1], rec[:1].reshape(1, -1))
+
+
+def test_store_records_parallel_filing_merges_repeats_in_order(oracle_mod):
+    """More than 512 records in one call take the chunk-parallel filing
+    (groups by chunk, one host thread per chunk); repeats of a block within the
+    call merge in input order, exactly as the oracle's sequential filing."""
+    import vsg
+
+    rng = np.random.default_rng(11)
+    coords, vox = _blocks(rng, 1500)
+    rep = rng.choice(len(coords), 600)  # repeated blocks, new voxel contents
+    _, vox2 = _blocks(np.random.default_rng(12), 1500)
+    all_c = np.concatenate([coords, coords[rep]])
+    all_v = np.concatenate([vox, vox2[: len(rep)]])
+    perm = rng.permutation(len(all_c))
+    all_c, all_v = all_c[perm], all_v[perm]
+    v = all_v.reshape(len(all_c), 512, 8)
+    rec = np.zeros((len(all_c), 512, 12), np.uint8)
+    rec[:, :, 0:3] = v[:, :, 4:7]
+    rec[:, :, 3] = v[:, :, 7]
+    rec[:, :, 4:8] = v[:, :, 0:4]
+    infos = np.concatenate([all_c, -np.ones((len(all_c), 1), np.int32)], 1)
+    ext = (0.25, 0.25, 0.25)
+    st = vsg.Store(ext)
+    st.add_records(0.004, infos, rec.reshape(len(all_c), -1))
+    oc = oracle_mod.ChunkStore(0.004, ext)
+    oc.add(all_c, all_v)
+    gc, gv = st.export()
+    ocs, ov = oc.export()
+    assert len(gc) == len(coords)
+    assert np.array_equal(gc, ocs) and np.array_equal(gv, ov)
+    assert st.count(None, -1.0)[0] == len(coords)
