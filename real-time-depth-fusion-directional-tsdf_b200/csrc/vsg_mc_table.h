@@ -49,14 +49,6 @@ static int vsg_mc_edge_of(int a, int b) {
     return -1;
 }
 
-/* Bit e set when edge e joins an inside and an outside corner. */
-static int vsg_mc_edge_mask(int c) {
-    int e, m = 0;
-    for (e = 0; e < 12; ++e)
-        if (((c >> kMcEdge[e][0]) & 1) != ((c >> kMcEdge[e][1]) & 1)) m |= 1 << e;
-    return m;
-}
-
 static void vsg_mc_build_table(unsigned char tab[256][16]) {
     int c, f, i, e;
     for (c = 0; c < 256; ++c) {
