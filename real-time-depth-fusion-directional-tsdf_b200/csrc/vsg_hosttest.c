@@ -20,5 +20,8 @@ float vsg_test_chain_serial(float r, float h, float target, int max_steps, int* 
 
 #include "vsg_mc_table.h"
 
-/* the generated marching-cubes table, 256 x 16 bytes */
+/* the marching-cubes table the kernel uses, 256 x 16 bytes */
 void vsg_test_mc_table(unsigned char* out) { vsg_mc_build_table((unsigned char(*)[16])out); }
+
+/* every case generated by the table's geometric rule, 256 x 16 bytes */
+void vsg_test_mc_generated(unsigned char* out) { vsg_mc_generate_table((unsigned char(*)[16])out); }

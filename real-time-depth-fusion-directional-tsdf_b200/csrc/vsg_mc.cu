@@ -6,9 +6,10 @@
 // voxel, case bit k set when corner k's SDF is below the iso value (weights
 // are not read), edge vertices by vertexInterp (:313-327), one face normal per
 // triangle by computeNormal (:329-350), triangles appended through one
-// counter.  The case table is generated (vsg_mc_table.h) instead of the
-// reference's, whose triangle rows are malformed past row 183 and missing
-// past row 208.
+// counter.  The case table (vsg_mc_table.h) holds the reference's triangle
+// rows for its 186 well-formed cases, entry for entry, and generated rows for
+// the 70 cases its table leaves undefined (rows missing past 208, rows 140,
+// 184-186, 189 and 191-208 naming edges their case does not cross).
 //
 // Layout of the work: one CTA of 352 threads walks the pool blocks; per
 // block it stages the 512 SDF values in shared memory, gives each of the 343

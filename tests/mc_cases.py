@@ -87,7 +87,7 @@ def triangles(c: int):
     return tris
 
 
-def table() -> np.ndarray:
+def generated_table() -> np.ndarray:
     """(256, 16) uint8: triangle edge indices, count in column 15, 0xFF unused."""
     t = np.full((256, 16), 0xFF, np.uint8)
     for c in range(256):

@@ -1,15 +1,24 @@
 """Marching cubes (vsg_mc_*) against the oracle's restatement of
 MarchingCubes.cu:352-467 on the same volume, bit for bit: the GPU volume is
-read back and loaded into the oracle, which extracts with the independently
-generated case table of mc_cases.py.  Triangle order is unspecified on both
+read back and loaded into the oracle, which extracts with the case table of
+the library's header built on the host (its reference rows and generated rows
+are pinned on the CPU by test_mc_table.py).  Triangle order is unspecified on both
 sides (the reference appends through an atomic counter), so triangles are
 compared as sorted multisets of their 18 floats (needs a GPU)."""
+import ctypes
+
 import numpy as np
 import pytest
 
-import mc_cases
 
 pytestmark = pytest.mark.gpu
+
+
+def _table(hosttest_lib):
+    t = np.zeros((256, 16), np.uint8)
+    hosttest_lib.vsg_test_mc_table.argtypes = [ctypes.c_void_p]
+    hosttest_lib.vsg_test_mc_table(t.ctypes.data)
+    return t
 
 
 def _rows(v, n):
@@ -35,7 +44,7 @@ def _oracle_of(oracle_mod, sc, voxel):
 
 
 @pytest.mark.parametrize("iso,voxel_override", [(0.0, 0.0), (0.004, 0.0), (-0.003, 0.005)])
-def test_mc_matches_oracle(cuda, synth_mod, oracle_mod, iso, voxel_override):
+def test_mc_matches_oracle(cuda, synth_mod, oracle_mod, hosttest_lib, iso, voxel_override):
     import vsg
 
     sc = _scene(vsg, cuda, synth_mod, 21, 160, 120, 4)
@@ -47,7 +56,7 @@ def test_mc_matches_oracle(cuda, synth_mod, oracle_mod, iso, voxel_override):
     mc.run(sc, iso=iso, voxel_size=voxel_override)
     n, v, nrm = mc.download()
     o = _oracle_of(oracle_mod, sc, 0.004)
-    on, ov, onrm = o.marching_cubes(mc_cases.table(), iso, voxel_override if voxel_override > 0 else 0.004, need)
+    on, ov, onrm = o.marching_cubes(_table(hosttest_lib), iso, voxel_override if voxel_override > 0 else 0.004, need)
     assert n == on == need == v.shape[0] > 1000
     assert np.array_equal(_rows(v, nrm), _rows(ov, onrm))
     # every normal is unit length or zero
@@ -57,7 +66,7 @@ def test_mc_matches_oracle(cuda, synth_mod, oracle_mod, iso, voxel_override):
     sc.close()
 
 
-def test_mc_capacity_and_empty(cuda, synth_mod, oracle_mod):
+def test_mc_capacity_and_empty(cuda, synth_mod, oracle_mod, hosttest_lib):
     import vsg
 
     sc = vsg.Scene(voxel_size=0.004, hash_num_slots=5003, num_sdf_blocks=8000)
@@ -70,7 +79,7 @@ def test_mc_capacity_and_empty(cuda, synth_mod, oracle_mod):
     mc.run(sc)
     n, v, nrm = mc.download()
     o = _oracle_of(oracle_mod, sc, 0.004)
-    on, ov, onrm = o.marching_cubes(mc_cases.table(), 0.0, 0.004, n)
+    on, ov, onrm = o.marching_cubes(_table(hosttest_lib), 0.0, 0.004, n)
     assert n == on > 64 and v.shape[0] == 64
     full = {r.tobytes() for r in _rows(ov, onrm)}
     assert all(r.tobytes() in full for r in _rows(v, nrm))  # the written ones are genuine

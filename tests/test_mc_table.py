@@ -1,19 +1,25 @@
 """Marching-cubes case table (no GPU).
 
 - The library's generator (csrc/vsg_mc_table.h, host build) and the
-  independent numpy restatement (mc_cases.py) give the same table.
+  independent numpy restatement (mc_cases.py) give the same generated table.
+- The table the kernel uses holds the reference's rows for its 186
+  well-formed cases and generated rows for the other 70; it is pinned by a
+  SHA-256 digest, so the pin holds without the reference tree.
 - Every case crosses exactly the edges whose corners differ (the edge table
   the reference indexes, MarchingCubes.cu:13-45), uses at most 5 triangles,
   and its triangles' face normals point towards the inside corners.
 - The surface is closed: on random sign grids every directed segment between
   edge vertices is matched by as many reversed ones, except on the border.
 - Against the reference's own table (read as text when the reference source
-  tree is present; skipped otherwise): its edge table equals the computed
-  one; its triangle table is malformed (209 of 256 rows; rows whose edges are
-  not the crossed edges of their case); every well-formed row has the same
-  face segments, with the same orientation, as the generated table.
+  tree is present, at $VSG_REFERENCE_ROOT or the default location; skipped
+  otherwise): its edge table equals the computed one; its triangle table is
+  malformed (209 of 256 rows; rows whose edges are not the crossed edges of
+  their case); every well-formed row equals the table's row entry for entry,
+  and the generated rows make the same face segments as every well-formed
+  reference row.
 """
 import ctypes
+import hashlib
 import os
 import re
 
@@ -22,7 +28,14 @@ import pytest
 
 import mc_cases
 
-REF_MC = "/root/reference/VoxelSG/src/MarchingCubes.cu"
+REF_ROOT = os.environ.get("VSG_REFERENCE_ROOT", "/root/reference")
+REF_MC = os.path.join(REF_ROOT, "VoxelSG", "src", "MarchingCubes.cu")
+
+# cases with no usable reference row (rows 209-255 missing; 140, 184-186,
+# 189, 191-208 cross other edges): their rows are generated
+GENERATED_CASES = [140, 184, 185, 186, 189] + list(range(191, 256))
+# SHA-256 of the 256 x 16-byte table the kernel uses
+TABLE_SHA256 = "74cda788d96d6c9e699235e89ed43e21056639d184c50c7fee91e5ff8b8ffce7"
 
 
 @pytest.fixture(scope="module")
@@ -33,8 +46,33 @@ def c_table(hosttest_lib):
     return out
 
 
-def test_c_generator_matches_independent_restatement(c_table):
-    assert np.array_equal(c_table, mc_cases.table())
+@pytest.fixture(scope="module")
+def c_generated(hosttest_lib):
+    out = np.zeros((256, 16), np.uint8)
+    hosttest_lib.vsg_test_mc_generated.argtypes = [ctypes.c_void_p]
+    hosttest_lib.vsg_test_mc_generated(out.ctypes.data)
+    return out
+
+
+def test_c_generator_matches_independent_restatement(c_generated):
+    assert np.array_equal(c_generated, mc_cases.generated_table())
+
+
+def test_table_takes_generated_rows_only_where_reference_has_none(c_table, c_generated):
+    gen = set(GENERATED_CASES)
+    assert len(gen) == 70
+    for c in range(256):
+        if c in gen:
+            assert np.array_equal(c_table[c], c_generated[c]), c
+    # the reference rows make the generated rows' face segments
+    for c in range(256):
+        mine = [tuple(int(e) for e in c_table[c, 3 * t:3 * t + 3]) for t in range(int(c_table[c, 15]))]
+        gen_t = [tuple(int(e) for e in c_generated[c, 3 * t:3 * t + 3]) for t in range(int(c_generated[c, 15]))]
+        assert mc_cases.boundary(mine) == mc_cases.boundary(gen_t), c
+
+
+def test_table_digest(c_table):
+    assert hashlib.sha256(c_table.tobytes()).hexdigest() == TABLE_SHA256
 
 
 def test_cases_cross_exactly_the_sign_change_edges(c_table):
@@ -154,7 +192,7 @@ def test_reference_edge_table_equals_computed():
     assert edge == [mc_cases.edge_mask(c) for c in range(256)]
 
 
-def test_reference_triangle_table_well_formed_rows_agree(c_table):
+def test_reference_triangle_table_well_formed_rows_equal(c_table):
     _, rows = _reference_tables()
     assert len(rows) == 209  # MC_TRI_TABLE_HOST[256][16]: rows 209..255 are zero-filled
     good, bad = [], []
@@ -165,13 +203,23 @@ def test_reference_triangle_table_well_formed_rows_agree(c_table):
             good.append(c)
         else:
             bad.append(c)
-    assert len(good) == 186 and bad[0] == 140, bad
-    same_tris = 0
+    bad += list(range(len(rows), 256))
+    assert len(good) == 186 and bad == GENERATED_CASES, bad
+    same_rows = 0
     for c in good:
         r = rows[c]
+        k = r.index(-1)
+        n = int(c_table[c, 15])
+        assert n == k // 3, c
+        same_rows += [int(e) for e in c_table[c, :k]] == r[:k] and all(v == 0xFF for v in c_table[c, k:15])
+    assert same_rows == 186
+
+
+def test_reference_rows_share_face_segments_with_generated(c_generated):
+    _, rows = _reference_tables()
+    for c, r in enumerate(rows):
+        if c in GENERATED_CASES:
+            continue
         ref = [tuple(r[i:i + 3]) for i in range(0, r.index(-1), 3)]
-        mine = [tuple(int(e) for e in c_table[c, 3 * t:3 * t + 3]) for t in range(int(c_table[c, 15]))]
-        assert mc_cases.boundary(mine) == mc_cases.boundary(ref), c
-        canon = lambda t: min(t[i:] + t[:i] for i in range(3))
-        same_tris += sorted(map(canon, mine)) == sorted(map(canon, ref))
-    assert same_tris == 85
+        gen = [tuple(int(e) for e in c_generated[c, 3 * t:3 * t + 3]) for t in range(int(c_generated[c, 15]))]
+        assert mc_cases.boundary(gen) == mc_cases.boundary(ref), c
