@@ -783,6 +783,27 @@ def run_batched(args, dist=None) -> dict:
     return res
 
 
+def _cudart():
+    """The CUDA runtime the library is linked against, for the e2e leg's
+    asynchronous copies: $VSG_CUDART if set, else the already loaded
+    libcudart.so.12 (libvsg.so depends on it), else the toolkit's copy.
+    Raises when none loads: the e2e number must not be silently absent."""
+    import ctypes
+    import ctypes.util
+
+    names = [os.environ.get("VSG_CUDART"), "libcudart.so.12", ctypes.util.find_library("cudart"),
+             os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "lib64", "libcudart.so.12")]
+    errors = []
+    for n in names:
+        if not n:
+            continue
+        try:
+            return ctypes.CDLL(n)
+        except OSError as e:
+            errors.append(f"{n}: {e}")
+    raise RuntimeError("e2e leg: no CUDA runtime library could be loaded (" + "; ".join(errors) + ")")
+
+
 def e2e(args, frames, K, sc, rr) -> dict:
     """Same stream through the C ABI with pinned host inputs: per frame H2D of
     the point/colour/normal maps, integrate, ray cast, D2H of depth,
@@ -801,11 +822,7 @@ def e2e(args, frames, K, sc, rr) -> dict:
     W, H = K.width, K.height
     host = [(torch.from_numpy(f.pointmap).pin_memory(), torch.from_numpy(f.rgb).pin_memory(),
              torch.from_numpy(f.normals).pin_memory(), f.pose) for f in frames]
-    lib = "/usr/local/cuda/lib64/libcudart.so.12"
-    cudart = ctypes.CDLL(lib) if os.path.exists(lib) else None
-    if cudart is None:
-        return {"value": None, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
-                "note": "libcudart not found"}
+    cudart = _cudart()
     dev_in = [(torch.empty((H, W, 3), dtype=torch.float32, device="cuda"),
                torch.empty((H, W, 3), dtype=torch.uint8, device="cuda"),
                torch.empty((H, W, 3), dtype=torch.float32, device="cuda")) for _ in range(2)]

@@ -111,6 +111,9 @@ typedef struct vsg_stats {
     uint32_t fast_division;      /* 1: the ray caster divides by the voxel size with a
                                     product + correction verified exhaustively against
                                     IEEE division at scene creation */
+    uint32_t pixel_buffer_capacity; /* pixels the scene's own per-pixel work buffers hold
+                                       (grown by vsg_integrate; 0 if only
+                                       vsg_integrate_noalloc has run) */
 } vsg_stats;
 
 /* Reference defaults of the knobs used by the tests (README.md:79-83). */
@@ -144,7 +147,13 @@ VSG_API int vsg_integrate(vsg_scene* s, const float* pointmap, const uint8_t* rg
  *   - at most 1,048,576 pixels (w*h) per frame; larger frames return
  *     VSG_ERR_TOO_LARGE without doing anything;
  *   - the first call on each device looks the array's address up
- *     (cudaGetSymbolAddress) and should come before any stream capture;
+ *     (cudaGetSymbolAddress) and should come before any stream capture; the
+ *     address is cached with the id of the device's current context and
+ *     looked up again, by the next call, when that context has changed
+ *     (after cudaDeviceReset, or with another driver context made current),
+ *     so that call too should come before any stream capture;
+ *   - its launches are not timed: the vsg_timing_* slots see only
+ *     vsg_integrate's frames;
  *   - every call on a device shares the one array, so calls whose work
  *     overlaps on the GPU (other streams, other scenes) race; serialise them;
  *   - the scene must live on the current device (else VSG_ERR_INVALID_ARG);

@@ -13,7 +13,8 @@ MarchingCubes.cu with oracle/ref_shim.cu and a two-line OpenCV stand-in
 
 Nothing is copied out of the reference tree; the reference build system is
 not used.  Skipped when the reference checkout is absent (a machine without
-it uses the files built here).
+it uses the files built here).  The checkout is found at $VSG_REFERENCE_ROOT,
+else at its default location.
 """
 from __future__ import annotations
 
@@ -23,8 +24,10 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF_SRC = "/root/reference/VoxelSG/src"
-REF_INC = "/root/reference/VoxelSG/include"
+# the reference checkout: $VSG_REFERENCE_ROOT, else its default location here
+REF_ROOT = os.environ.get("VSG_REFERENCE_ROOT", "/root/reference")
+REF_SRC = os.path.join(REF_ROOT, "VoxelSG", "src")
+REF_INC = os.path.join(REF_ROOT, "VoxelSG", "include")
 SOURCES = ["VoxelScene.cu", "RayCastRender.cu", "CUDAHashRef.cu", "MarchingCubes.cu"]
 VARIANTS = {"libvsgref.so": [], "libvsgref_nofma.so": ["-fmad=false"]}
 

@@ -149,8 +149,18 @@ int vsg_scene_destroy(vsg_scene* s) {
     return VSG_OK;
 }
 
+// True when the calling thread's current device is `device`: a scene's hash,
+// pool and counters, and a renderer's outputs, live on the device current at
+// their creation, and kernels launched on another device would dereference
+// that device's pointers.
+static bool on_device(int device) {
+    int dev = -1;
+    return cudaGetDevice(&dev) == cudaSuccess && dev == device;
+}
+
 int vsg_scene_reset(vsg_scene* s, vsg_stream_t stream) {
     if (!s) return VSG_ERR_INVALID_ARG;
+    if (!on_device(s->impl.device)) return VSG_ERR_INVALID_ARG;
     return vsg::scene_reset_device(&s->impl, (cudaStream_t)stream);
 }
 
@@ -166,6 +176,7 @@ int vsg_integrate(vsg_scene* s, const float* pointmap, const uint8_t* rgb, const
     if (!s) return VSG_ERR_NOT_ALLOCATED;
     if (!pointmap || !rgb || !normals || !pose) return VSG_ERR_INVALID_ARG;
     if (w <= 0 || h <= 0 || (long long)w * h > (1ll << 30)) return VSG_ERR_INVALID_ARG;
+    if (!on_device(s->impl.device)) return VSG_ERR_INVALID_ARG;
     return vsg::scene_integrate(&s->impl, pointmap, rgb, normals, w, h, truncation, pose, fx, fy, cx, cy,
                                 (cudaStream_t)stream);
 }
@@ -207,6 +218,7 @@ int vsg_scene_stats(vsg_scene* s, vsg_stats* out) {
     out->render_warp_iters = f.warp_iters;
     out->flags = c.flags;
     out->fast_division = s->impl.dev.div_fast ? 1u : 0u;
+    out->pixel_buffer_capacity = (uint32_t)std::min<size_t>(s->impl.pix_capacity, UINT32_MAX);
     return VSG_OK;
 }
 
@@ -298,6 +310,7 @@ int vsg_render(vsg_renderer* r, const vsg_scene* s, const float cam_pos[3], cons
                float fy, float cx, float cy, float min_depth, float max_depth, vsg_stream_t stream) {
     if (!r) return VSG_ERR_NOT_ALLOCATED;
     if (!s || !cam_pos || !pose_dev) return VSG_ERR_INVALID_ARG;
+    if (!on_device(s->impl.device) || !on_device(r->impl.device)) return VSG_ERR_INVALID_ARG;
     return vsg::render_launch(&r->impl, const_cast<Scene*>(&s->impl), cam_pos, pose_dev, nullptr, fx, fy, cx, cy,
                               min_depth, max_depth, (cudaStream_t)stream);
 }
@@ -306,6 +319,7 @@ int vsg_render_hostpose(vsg_renderer* r, const vsg_scene* s, const float cam_pos
                         float fy, float cx, float cy, float min_depth, float max_depth, vsg_stream_t stream) {
     if (!r) return VSG_ERR_NOT_ALLOCATED;
     if (!s || !cam_pos || !pose) return VSG_ERR_INVALID_ARG;
+    if (!on_device(s->impl.device) || !on_device(r->impl.device)) return VSG_ERR_INVALID_ARG;
     return vsg::render_launch(&r->impl, const_cast<Scene*>(&s->impl), cam_pos, nullptr, pose, fx, fy, cx, cy,
                               min_depth, max_depth, (cudaStream_t)stream);
 }

@@ -13,6 +13,7 @@
 // vsg_integrate_noalloc runs the same integration with those work buffers
 // taken from one fixed array of device memory compiled into this file, so
 // the caller passes only its inputs (and the scene, created beforehand).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -33,23 +34,56 @@ constexpr size_t kScratchBytes = kWorldBytes + kMaxPixels * sizeof(uint32_t);
 
 static __device__ __align__(256) unsigned char g_pixel_scratch[kScratchBytes];
 
-// The array's device address, looked up once per device.  In host code the
-// name g_pixel_scratch is only a host-side stand-in for the symbol, never a
-// device address, so kernels must be given the looked-up pointer.
+// The array's device address.  In host code the name g_pixel_scratch is only
+// a host-side stand-in for the symbol, never a device address, so kernels
+// must be given the address that cudaGetSymbolAddress returns with the
+// device current.  That address belongs to the device's current context: it
+// is looked up on the first call on each device and cached together with the
+// context's unique id (cuCtxGetId), and looked up again whenever the id
+// differs -- after cudaDeviceReset, or when the caller made another driver
+// context current -- because the module, and with it the array, may then sit
+// at another address.  Where the driver offers no context id, nothing is
+// cached and every call looks the address up.
 constexpr int kMaxDevices = 64;
+struct ScratchSlot {
+    unsigned long long ctx_id = 0;
+    void* addr = nullptr;
+};
 std::mutex g_mutex;
-void* g_scratch_addr[kMaxDevices] = {};
+ScratchSlot g_slot[kMaxDevices];
+
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// The current context's unique id; false without a current context or
+// without cuCtxGetId in the driver.
+bool current_context_id(unsigned long long* id) {
+    static CtxGetIdFn fn = []() -> CtxGetIdFn {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<CtxGetIdFn>(f);
+    }();
+    return fn && fn(nullptr, id) == CUDA_SUCCESS;
+}
 
 int scratch_for_device(int dev, unsigned char** out) {
     if (dev < 0 || dev >= kMaxDevices) return VSG_ERR_TOO_LARGE;
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        // runs with `dev` current: the caller's current device
-        if (cudaGetSymbolAddress(&p, g_pixel_scratch) != cudaSuccess || p == nullptr) return VSG_ERR_CUDA;
-        g_scratch_addr[dev] = p;
+    unsigned long long id = 0;
+    bool have_id = current_context_id(&id);
+    if (have_id && g_slot[dev].addr && g_slot[dev].ctx_id == id) {
+        *out = static_cast<unsigned char*>(g_slot[dev].addr);
+        return VSG_OK;
     }
-    *out = static_cast<unsigned char*>(g_scratch_addr[dev]);
+    void* p = nullptr;
+    // runs with `dev` current: the caller's current device
+    if (cudaGetSymbolAddress(&p, g_pixel_scratch) != cudaSuccess || p == nullptr) return VSG_ERR_CUDA;
+    if (!have_id) have_id = current_context_id(&id);  // the lookup made the primary context current
+    g_slot[dev].ctx_id = have_id ? id : 0;
+    g_slot[dev].addr = have_id ? p : nullptr;
+    *out = static_cast<unsigned char*>(p);
     return VSG_OK;
 }
 

@@ -68,7 +68,7 @@ class Stats(ctypes.Structure):
         "frame_updated_voxels", "render_hits", "render_misses", "render_samples_full",
         "render_samples_skipped", "render_jumps", "render_singles", "render_blocks_read",
         "render_lane_iters", "render_warp_iters", "flags",
-        "fast_division")]
+        "fast_division", "pixel_buffer_capacity")]
 
     def as_dict(self) -> dict:
         return {n: int(getattr(self, n)) for n, _ in self._fields_}

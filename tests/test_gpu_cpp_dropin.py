@@ -112,3 +112,14 @@ def test_cpp_depth_map_generator_matches_binding(cuda, synth_mod, tmp_path):
     for k, g in got.items():
         assert np.array_equal(g.view(np.uint8), want[k].cpu().numpy().view(np.uint8)), k
     assert want["n_valid"] > 0.5 * W * H and not got["colormap"].any()
+
+
+def test_wrong_device_is_refused_before_any_launch(cuda, tmp_path):
+    """vsg_integrate / vsg_scene_reset / vsg_render / vsg_render_hostpose with a
+    handle recorded on another device return VSG_ERR_INVALID_ARG and touch
+    nothing (tests/cpp/device_guard.cu)."""
+    from test_cpp_dropin_build import build_device_guard
+
+    exe = build_device_guard(tmp_path)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "device_guard ok" in r.stdout, r.stdout + r.stderr
