@@ -69,9 +69,11 @@ enum {
     VSG_FLAG_COORD_RANGE = 4u,      /* a block coordinate outside +-2^20 was skipped */
     VSG_FLAG_INSERT_RETRY = 8u,     /* a bounded insert retry loop gave up */
     VSG_FLAG_MARCH_LIMIT = 16u,     /* a ray hit the iteration guard */
-    VSG_FLAG_PARENT_OVERFLOW = 32u  /* normal-direction allocation: a frame's parent records
+    VSG_FLAG_PARENT_OVERFLOW = 32u, /* normal-direction allocation: a frame's parent records
                                        overflowed (a DDA ran to its 1024-block guard); some
                                        blocks kept an older parent pixel */
+    VSG_FLAG_BATCH_WAIT = 64u       /* batched step: a stage of this scene gave up waiting for
+                                       its previous stage (bounded wait) and ran anyway */
 };
 
 /* GlobalParamsConfig knobs (globalPramasConfig.h:101-109) and the sizes
@@ -111,6 +113,9 @@ typedef struct vsg_stats {
     uint32_t fast_division;      /* 1: the ray caster divides by the voxel size with a
                                     product + correction verified exhaustively against
                                     IEEE division at scene creation */
+    uint32_t fast_avg_divisors;  /* of the running average's 256 divisors (new weight
+                                    1..256), those whose one-correction product was
+                                    verified equal to IEEE division for every dividend */
     uint32_t pixel_buffer_capacity; /* pixels the scene's own per-pixel work buffers hold
                                        (grown by vsg_integrate; 0 if only
                                        vsg_integrate_noalloc has run) */

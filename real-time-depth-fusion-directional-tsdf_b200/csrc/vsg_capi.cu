@@ -218,6 +218,12 @@ int vsg_scene_stats(vsg_scene* s, vsg_stats* out) {
     out->render_warp_iters = f.warp_iters;
     out->flags = c.flags;
     out->fast_division = s->impl.dev.div_fast ? 1u : 0u;
+    {
+        float tab[257];
+        if (cudaMemcpy(tab, s->impl.dev.avg_recip, sizeof(tab), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return VSG_ERR_CUDA;
+        for (int d = 1; d <= 256; ++d) out->fast_avg_divisors += tab[d] != 0.0f ? 1u : 0u;
+    }
     out->pixel_buffer_capacity = (uint32_t)std::min<size_t>(s->impl.pix_capacity, UINT32_MAX);
     return VSG_OK;
 }

@@ -13,16 +13,20 @@
 //   block_fresh u8[B]             1 until the block's first integration pass
 //   block_wmask u64[B]            bit (sz*4+sy)*4+sx: sub-cube (2x2x2 voxels)
 //                                 holds a voxel with weight > 0
+//   block_pmask u64[B]            same bits: sub-cube has held a weighted
+//                                 voxel with SDF > 0 (kept by OR)
 //   heap        u32[B]            free-list stack of pool indices
 //   bindex      u64[2^(3k)]       dense toroidal block index: cell (x,y,z) mod 2^k
 //                                 holds ptr (22 bits) | high coordinate bits
 //                                 (tag) << 22 of the one block mapped there;
 //                                 ~0 = none, ~0-1 = several (use the hash)
-//   dwm         u64[2^(3k)]       per toroidal block position: sub-cubes that
-//                                 have a weighted sub-cube within one sub-cube
-//                                 (3x3x3, across block faces); ray-march skip
+//   dmask       u64x2[2^(3k)]     per toroidal block position, .x: sub-cubes
+//                                 that have a weighted sub-cube within one
+//                                 sub-cube (3x3x3, across block faces); .y:
+//                                 the same dilation of the positive sub-cubes
+//                                 (block_pmask); ray-march skip grid
 //   sup         u32[2^(3(k-3))/32] per toroidal super-cell (8^3 block
-//                                 positions): some dwm word in it is non-zero
+//                                 positions): some dmask word in it is non-zero
 //   visible     u32[B]            pool indices the current frame integrates
 //   pix_world   float4[W*H]       per pixel of the current frame: world point
 //                                 T*p and its camera distance (-1: invalid)
@@ -38,6 +42,17 @@
 
 #include <cstdint>
 #include <cuda_runtime.h>
+
+// Loads of data that no CTA writes while the reading kernel runs go through
+// the read-only (non-coherent) cache.  A translation unit whose kernel reads,
+// in the same launch, data that other CTAs of that launch wrote (after
+// waiting for them) defines VSG_COHERENT_LOADS before including the device
+// headers; those loads then take the coherent path.
+#ifdef VSG_COHERENT_LOADS
+#define VSG_LDG(p) (*(p))
+#else
+#define VSG_LDG(p) __ldg(p)
+#endif
 
 namespace vsg {
 
@@ -110,10 +125,11 @@ struct SceneDev {
     int* block_slot;
     uint8_t* block_fresh;
     unsigned long long* block_wmask;  // per block: 2x2x2-voxel sub-cubes holding a weighted voxel
+    unsigned long long* block_pmask;  // per block: sub-cubes that have held a weighted voxel with SDF > 0
     uint8_t* block_touched;           // instrumented renders: block read by a ray
     uint32_t* heap;
     unsigned long long* bindex;
-    unsigned long long* dwm;
+    ulonglong2* dmask;  // .x dilated weight mask, .y dilated positive mask
     uint32_t* sup;
     uint32_t* visible;
     float4* pix_world;   // per pixel of the current frame: T*p and |T*p - c| (-1 = invalid)
@@ -138,6 +154,10 @@ struct SceneDev {
     float voxel;
     float inv_voxel;  // RN(1 / voxel)
     bool div_fast;    // fixed-divisor division verified for this voxel size
+    // [257]: entry d (1..256) = RN(1/d) when the one-correction quotient
+    // (avg_div) equals IEEE division by d for every dividend, else 0 (IEEE
+    // division); the running average divides by the new weight d
+    const float* avg_recip;
 };
 
 struct Pose {
@@ -195,6 +215,62 @@ __host__ __device__ __forceinline__ float ord2f(uint32_t u) {
 #endif
 }
 
+// ------------------------------------------------ exact division shortcuts
+
+// x / d for a running-average divisor d (the new weight, 1..256), given
+// y = avg_recip[d]: one Markstein correction of the product x*y (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990): r = x - q d is exact and
+// RN(q + r y) is the quotient.  For a fixed d the three operations commute
+// with scaling x by a power of two while |x| stays in [2^-100, 2^100) (q, r
+// and the result stay representable), and with negation, so the verification
+// at scene creation over every x in [1, 2) covers that whole range; +0 gives
+// +0 as IEEE division does.  Other x (and divisors that failed verification,
+// y = 0) use IEEE division; -0 among them, which IEEE division keeps negative.
+__device__ __forceinline__ float avg_div(float x, float d, float y) {
+    const float ax = fabsf(x);
+    if (y != 0.0f && ax < 0x1p100f && (ax >= 0x1p-100f || __float_as_uint(x) == 0u)) {
+        const float q = __fmul_rn(x, y);
+        const float r = __fmaf_rn(-q, d, x);
+        return __fmaf_rn(r, y, q);
+    }
+    return x / d;
+}
+
+// For a camera distance w = RN(sqrt(.)) of a pixel's point: the smallest
+// float D >= 0 with RN(sqrt(D)) >= w.  RN(sqrt(.)) is non-decreasing over
+// the floats, so for every float D >= 0, RN(sqrt(D)) < w exactly when
+// D < sqrt_threshold(w): integration decides the sign of a voxel's SDF
+// (cameraDist < depthPos distance, VoxelScene.cu:1055-1066) on the squared
+// distance without a square root per voxel.  w = +0, +inf and NaN are their
+// own thresholds (the comparison is then false as with w itself).  The
+// threshold is within a few ulps of RN(w*w); it is stepped there and checked
+// against its definition, else found by bisection over the float order.
+__device__ __forceinline__ float sqrt_threshold(float w) {
+    if (!(w > 0.0f) || w == __int_as_float(0x7F800000)) return w;
+    float c = w * w;
+    bool ok = false;
+    if (w >= 0x1p-60f && w <= 0x1p60f) {
+        for (int i = 0; i < 8 && sqrtf(c) < w; ++i) c = __uint_as_float(__float_as_uint(c) + 1u);
+        for (int i = 0; i < 8 && c > 0.0f && sqrtf(__uint_as_float(__float_as_uint(c) - 1u)) >= w; ++i)
+            c = __uint_as_float(__float_as_uint(c) - 1u);
+        ok = sqrtf(c) >= w && (c == 0.0f || sqrtf(__uint_as_float(__float_as_uint(c) - 1u)) < w);
+    }
+    if (!ok) {
+        // min u in [0, +inf bits] with RN(sqrt(float(u))) >= w
+        uint32_t lo = 0u, hi = 0x7F800000u;
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2u;
+            if (sqrtf(__uint_as_float(mid)) >= w)
+                hi = mid;
+            else
+                lo = mid + 1u;
+        }
+        c = __uint_as_float(lo);
+    }
+    return c;
+}
+
 // ------------------------------------------- sub-cube masks and skip grid
 
 // 4x4x4 sub-cubes (2x2x2 voxels each) of a block: bit (cz*4 + cy)*4 + cx
@@ -247,14 +323,14 @@ __device__ __forceinline__ int lookup_block(const SceneDev& s, unsigned long lon
     const Entry* bk = s.buckets + (size_t)b * kBucketSlots;
 #pragma unroll
     for (int j = 0; j < kBucketSlots; ++j) {
-        const uint4 e = __ldg(reinterpret_cast<const uint4*>(bk + j));
+        const uint4 e = VSG_LDG(reinterpret_cast<const uint4*>(bk + j));
         const unsigned long long k = ((unsigned long long)e.y << 32) | e.x;
         if (k == key) return (int)e.z;
         if (k == kKeyEmpty) return -1;
     }
-    int n = __ldg(s.bucket_next + b);
+    int n = VSG_LDG(s.bucket_next + b);
     for (int it = 0; n >= 0 && it < s.max_nodes; ++it) {
-        const uint4 e = __ldg(reinterpret_cast<const uint4*>(s.nodes + n));
+        const uint4 e = VSG_LDG(reinterpret_cast<const uint4*>(s.nodes + n));
         const unsigned long long k = ((unsigned long long)e.y << 32) | e.x;
         if (k == key) return (int)e.z;
         n = (int)e.w;
@@ -266,7 +342,7 @@ __device__ __forceinline__ int lookup_block(const SceneDev& s, unsigned long lon
 // cells shared by several blocks.  -1 = not allocated.
 __device__ __forceinline__ int block_ptr(const SceneDev& s, int x, int y, int z) {
     if (!coord_ok(x, y, z)) return -1;
-    const unsigned long long e = __ldg(s.bindex + bidx_cell(x, y, z, s.bidx_log2));
+    const unsigned long long e = VSG_LDG(s.bindex + bidx_cell(x, y, z, s.bidx_log2));
     if (e == kIdxEmpty) return -1;
     if (e == kIdxShared) return lookup_block(s, pack_key(x, y, z), x, y, z);
     return ((e >> 22) == bidx_tag(x, y, z, s.bidx_log2)) ? (int)(e & kIdxPtrMask) : -1;

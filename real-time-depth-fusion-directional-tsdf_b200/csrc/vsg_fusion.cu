@@ -75,11 +75,55 @@ __global__ void k_init_counters(SceneCounters* c, int num_blocks) {
 
 __global__ void k_frame_begin(FrameCounters* f) { frame_begin(f); }
 
+// avg_div against IEEE division for every divisor d = 1..256 and every
+// dividend x in [1, 2) (2^31 pairs; by the scaling argument at avg_div that
+// covers 2^-100 <= |x| < 2^100): fail[d] = 1 where any quotient differs.
+__global__ void k_verify_avg_div(unsigned int* fail) {
+    const uint32_t n = 256u << 23;
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+        const uint32_t d = (u >> 23) + 1u;
+        const float x = __uint_as_float(0x3F800000u | (u & 0x7FFFFFu));
+        const float df = (float)d;
+        const float y = 1.0f / df;
+        if (__float_as_uint(avg_div(x, df, y)) != __float_as_uint(x / df)) fail[d] = 1u;
+    }
+}
+
 // ====================================================================
 // host side
 // ====================================================================
 
 static size_t sup_words(int k) { return ((1ull << (3 * (k - 3))) + 31ull) / 32ull; }
+
+// The running average's reciprocal table (SceneDev::avg_recip): RN(1/d) for
+// the divisors that passed k_verify_avg_div, 0 for the others.  Which
+// divisors pass is a property of IEEE binary32 arithmetic, not of a scene or
+// a device, so it is verified once per process, on the GPU current at the
+// first scene creation.
+static int avg_recip_table(float out[257]) {
+    static std::mutex mu;
+    static bool done = false;
+    static float table[257];
+    std::lock_guard<std::mutex> lock(mu);
+    if (!done) {
+        unsigned int* fail = nullptr;
+        if (cudaMalloc(&fail, 257 * sizeof(unsigned int)) != cudaSuccess) return VSG_ERR_OUT_OF_MEMORY;
+        cudaMemset(fail, 0, 257 * sizeof(unsigned int));
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        k_verify_avg_div<<<sms * 8, 256>>>(fail);
+        unsigned int h[257];
+        const cudaError_t e = cudaMemcpy(h, fail, sizeof(h), cudaMemcpyDeviceToHost);
+        cudaFree(fail);
+        if (e != cudaSuccess) return VSG_ERR_CUDA;
+        table[0] = 0.0f;
+        for (int d = 1; d <= 256; ++d) table[d] = h[d] ? 0.0f : 1.0f / (float)d;
+        done = true;
+    }
+    memcpy(out, table, sizeof(table));
+    return VSG_OK;
+}
 
 int scene_alloc_device(Scene* sc) {
     SceneDev& d = sc->dev;
@@ -99,11 +143,12 @@ int scene_alloc_device(Scene* sc) {
     VSG_MALLOC(d.block_slot, B * sizeof(int));
     VSG_MALLOC(d.block_fresh, B);
     VSG_MALLOC(d.block_wmask, B * sizeof(unsigned long long));
+    VSG_MALLOC(d.block_pmask, B * sizeof(unsigned long long));
     VSG_MALLOC(d.block_touched, B);
     VSG_MALLOC(d.block_parent, B * sizeof(unsigned long long));
     VSG_MALLOC(d.heap, B * sizeof(uint32_t));
     VSG_MALLOC(d.bindex, sizeof(unsigned long long) << (3 * sc->bidx_log2));
-    VSG_MALLOC(d.dwm, sizeof(unsigned long long) << (3 * sc->bidx_log2));
+    VSG_MALLOC(d.dmask, sizeof(ulonglong2) << (3 * sc->bidx_log2));
     VSG_MALLOC(d.sup, sup_words(sc->bidx_log2) * 4);
     VSG_MALLOC(d.visible, B * sizeof(uint32_t));
     d.pix_world = nullptr;
@@ -113,6 +158,7 @@ int scene_alloc_device(Scene* sc) {
     d.parent_tag = nullptr;
     d.parent_cap = 0;
     d.alloc_method = 1;
+    VSG_MALLOC(d.avg_recip, 257 * sizeof(float));
     VSG_MALLOC(d.ctr, sizeof(SceneCounters));
     VSG_MALLOC(d.frame, sizeof(FrameCounters));
 #undef VSG_MALLOC
@@ -125,6 +171,13 @@ int scene_alloc_device(Scene* sc) {
     bool fast = false;
     if (verify_fixed_division(d.voxel, &fast) != VSG_OK) fast = false;
     d.div_fast = fast;
+    {
+        float tab[257];
+        const int rc = avg_recip_table(tab);
+        if (rc != VSG_OK) return rc;
+        if (cudaMemcpy(const_cast<float*>(d.avg_recip), tab, sizeof(tab), cudaMemcpyHostToDevice) != cudaSuccess)
+            return VSG_ERR_CUDA;
+    }
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_integrate, 256, 0);
     sc->integ_ctas_per_sm = per_sm > 0 ? per_sm : 2;
@@ -133,9 +186,9 @@ int scene_alloc_device(Scene* sc) {
 
 void scene_free_device(Scene* sc) {
     SceneDev& d = sc->dev;
-    void* ptrs[] = {d.block_parent, d.parent_key, d.parent_tag, d.block_touched, d.sup, d.dwm,     d.bindex,    d.block_wmask, d.buckets,   d.bucket_next,
+    void* ptrs[] = {d.block_parent, d.parent_key, d.parent_tag, d.block_touched, d.sup, d.dmask,   d.bindex,    d.block_wmask, d.block_pmask, d.buckets,   d.bucket_next,
                     d.nodes,     d.voxels,  d.block_key, d.block_slot,  d.block_fresh, d.heap,
-                    d.visible,   d.pix_world, d.pix_rgb, d.ctr,         d.frame};
+                    d.visible,   d.pix_world, d.pix_rgb, d.ctr,         d.frame, const_cast<float*>(d.avg_recip)};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     memset(&d, 0, sizeof(d));
@@ -152,7 +205,7 @@ int scene_reset_device(Scene* sc, cudaStream_t st) {
     cudaMemsetAsync(d.block_fresh, 0, B, st);
     cudaMemsetAsync(d.block_parent, 0, B * sizeof(unsigned long long), st);
     cudaMemsetAsync(d.bindex, 0xFF, sizeof(unsigned long long) << (3 * sc->bidx_log2), st);
-    cudaMemsetAsync(d.dwm, 0, sizeof(unsigned long long) << (3 * sc->bidx_log2), st);
+    cudaMemsetAsync(d.dmask, 0, sizeof(ulonglong2) << (3 * sc->bidx_log2), st);
     cudaMemsetAsync(d.sup, 0, sup_words(sc->bidx_log2) * 4, st);
     k_init_heap<<<(unsigned)((B + 255) / 256), 256, 0, st>>>(d.heap, (int)B);
     k_init_counters<<<1, 1, 0, st>>>(d.ctr, (int)B);

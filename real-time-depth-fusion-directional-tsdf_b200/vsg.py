@@ -68,7 +68,7 @@ class Stats(ctypes.Structure):
         "frame_updated_voxels", "render_hits", "render_misses", "render_samples_full",
         "render_samples_skipped", "render_jumps", "render_singles", "render_blocks_read",
         "render_lane_iters", "render_warp_iters", "flags",
-        "fast_division", "pixel_buffer_capacity")]
+        "fast_division", "fast_avg_divisors", "pixel_buffer_capacity")]
 
     def as_dict(self) -> dict:
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
@@ -357,6 +357,130 @@ def refine_pose(scene, renderer, target_depth, pose, fx, fy, cx, cy, min_depth, 
     return T, rms
 
 
+def _normal_matrix(v: np.ndarray):
+    Hm = np.zeros((6, 6))
+    iu = np.triu_indices(6)
+    Hm[iu] = v[:21]
+    return Hm + np.triu(Hm, 1).T, v[21:]
+
+
+def refine_poses(scenes, renderers, targets, poses, intrinsics, min_depth, max_depth, steps: int = 8,
+                 huber: float = 0.01, damping: float = 1e-6, min_weight_sum: float = 0.5,
+                 max_residual=(0.2, 0.05), min_incidence: float = 0.0, min_pixels: int = 500,
+                 max_step=(0.1, 0.1), streams=None):
+    """refine_pose for several independent (scene, renderer, target depth,
+    pose) problems at once, with the same steps, weights, stopping rules and
+    results: in every Gauss-Newton step all problems' GPU work (render,
+    normals, residuals, normal equations) is issued -- on one CUDA stream per
+    problem when `streams` (torch streams) is given, else on the current
+    stream -- before ONE host synchronisation collects every system; the
+    6x6 solves and pose updates then run on the host.  intrinsics: one
+    (fx, fy, cx, cy) for all or one per problem.  Returns (list of 4x4
+    float64 poses, list of per-step weighted RMS residual lists)."""
+    import torch
+
+    n = len(scenes)
+    K = [tuple(intrinsics)] * n if np.isscalar(intrinsics[0]) else [tuple(k) for k in intrinsics]
+    T = [np.asarray(p, np.float64).reshape(4, 4).copy() for p in poses]
+    cur = torch.cuda.current_stream()
+    if streams is None:
+        streams = [cur] * n
+    for st in {id(x): x for x in streams}.values():
+        st.wait_stream(cur)
+    for r in renderers:
+        r.record(True)
+    rays = [_unit_rays(renderers[i].width, renderers[i].height, *K[i]) if min_incidence > 0 else None
+            for i in range(n)]
+    r0, r1 = (float(max_residual[0]), float(max_residual[1])) if max_residual is not None else (np.inf, np.inf)
+    rms = [[] for _ in range(n)]
+    active = [True] * n
+    ne = torch.zeros((n, 27), dtype=torch.float64, device="cuda")
+    cnt = torch.zeros(n, dtype=torch.int64, device="cuda")
+    res = torch.zeros(n, dtype=torch.float32, device="cuda")
+    for k in range(steps):
+        todo = [i for i in range(n) if active[i]]
+        if not todo:
+            break
+        tau = r0 * (r1 / r0) ** (k / max(steps - 1, 1)) if np.isfinite(r0) else np.inf
+        for i in todo:
+            fx, fy, cx, cy = K[i]
+            T32 = T[i].astype(np.float32)
+            sh = streams[i].cuda_stream
+            with torch.cuda.stream(streams[i]):
+                renderers[i].render(scenes[i], T32, fx, fy, cx, cy, min_depth, max_depth, stream=sh)
+                d = renderers[i].depth_tensor()
+                tg = targets[i]
+                m = (d < 1e9) & (tg < 1e9)
+                if rays[i] is not None:
+                    nrm, _ = renderers[i].normals(scenes[i], T32, fx, fy, cx, cy, stream=sh, sync=False)
+                    R = torch.as_tensor(T32[:3, :3], device="cuda")
+                    cos = (nrm[..., :3] * (rays[i] @ R.T)).sum(-1).abs()
+                    m = m & (cos >= min_incidence)
+                r = torch.where(m, d - tg, torch.zeros_like(d))
+                a = r.abs()
+                m = m & (a <= tau)
+                w = torch.where(m, torch.where(a <= huber, torch.ones_like(a), huber / a.clamp_min(huber)),
+                                torch.zeros_like(a))
+                cnt[i] = m.sum()
+                res[i] = torch.sqrt((w * r * r).sum() / w.sum().clamp_min(1e-30))
+                renderers[i].pose_normal_equations_into(scenes[i], T32, fx, fy, cx, cy, r, w, ne[i],
+                                                        min_weight_sum, stream=sh)
+        torch.cuda.synchronize()
+        ne_h, cnt_h, res_h = ne.cpu().numpy(), cnt.cpu().numpy(), res.cpu().numpy()
+        for i in todo:
+            if int(cnt_h[i]) < min_pixels:
+                active[i] = False
+                continue
+            Hm, b = _normal_matrix(ne_h[i])
+            rms[i].append(float(res_h[i]))
+            A = Hm + damping * np.diag(np.diag(Hm))
+            if not np.all(np.isfinite(A)) or np.linalg.matrix_rank(A) < 6:
+                active[i] = False
+                continue
+            xi = -np.linalg.solve(A, b)
+            sc = max(np.linalg.norm(xi[:3]) / max_step[0], np.linalg.norm(xi[3:]) / max_step[1], 1.0)
+            T[i] = T[i] @ se3_exp(xi / sc)
+    return T, rms
+
+
+def stream_scenes(scenes, stores, centers, r_out: float, r_in: float, streams=None, max_threads: int = 8):
+    """One streaming pass for several scenes at once, in the reference main
+    loop's order (voxelSG.cpp:503-551): per scene, stream out every block
+    farther than r_out from its centre into its store, then stream in the
+    stored chunks within r_in.  The scenes go through host threads (the C
+    calls release the interpreter lock), each on its own CUDA stream
+    (`streams`: torch streams, one per scene; created here when None), so
+    their transfers and host filing overlap.  Work queued on the current
+    stream before the call is waited for.  Returns per scene (blocks out,
+    blocks in, 1 if the stream-in was refused for lack of pool blocks)."""
+    import concurrent.futures as cf
+
+    import torch
+
+    n = len(scenes)
+    if streams is None:
+        streams = [torch.cuda.Stream() for _ in range(n)]
+    torch.cuda.current_stream().synchronize()
+    dev = torch.cuda.current_device()
+
+    def one(i):
+        torch.cuda.set_device(dev)
+        sh = streams[i].cuda_stream
+        c = np.asarray(centers[i], np.float32)
+        n_out = scenes[i].stream_out(stores[i], c, r_out, stream=sh)
+        refused = 0
+        try:
+            n_in = scenes[i].stream_in(stores[i], c, r_in, stream=sh)[0]
+        except VsgError as exc:
+            if exc.code != 5:  # VSG_ERR_TOO_LARGE: nothing moved
+                raise
+            n_in, refused = 0, 1
+        return n_out, n_in, refused
+
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(max_threads, n))) as ex:
+        return list(ex.map(one, range(n)))
+
+
 class Scene:
     """VoxelScene over the C ABI (vsg_scene_*, vsg_integrate)."""
 
@@ -555,8 +679,10 @@ class Renderer:
         Hm = Hm + np.triu(Hm, 1).T
         return Hm, v[21:], int(skipped.value)
 
-    def normals(self, scene: "Scene", pose, fx, fy, cx, cy, out=None, stream=None):
-        """Normals of the last recorded render: (H,W,4) float32 device tensor."""
+    def normals(self, scene: "Scene", pose, fx, fy, cx, cy, out=None, stream=None, sync: bool = True):
+        """Normals of the last recorded render: (H,W,4) float32 device tensor,
+        and the skipped-pixel count (None with sync=False: the call then
+        returns without waiting for the device)."""
         import torch
 
         T = np.ascontiguousarray(np.asarray(pose, np.float32).reshape(16))
@@ -564,9 +690,19 @@ class Renderer:
             out = torch.empty((self.height, self.width, 4), dtype=torch.float32, device="cuda")
         skipped = ctypes.c_uint32()
         check("vsg_render_normals", self.L.vsg_render_normals(
-            self.h, scene.h, _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _dptr(out), ctypes.byref(skipped),
+            self.h, scene.h, _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _dptr(out),
+            ctypes.byref(skipped) if sync else None, _stream(stream)))
+        return out, (int(skipped.value) if sync else None)
+
+    def pose_normal_equations_into(self, scene: "Scene", pose, fx, fy, cx, cy, residual, weights, out,
+                                   min_weight_sum: float = 0.5, stream=None):
+        """pose_normal_equations without waiting for the device: the 27
+        doubles (H's upper triangle, then b) go to the device tensor `out`."""
+        T = np.ascontiguousarray(np.asarray(pose, np.float32).reshape(16))
+        check("vsg_render_pose_normal_equations", self.L.vsg_render_pose_normal_equations(
+            self.h, scene.h, _hptr(T), _F(fx), _F(fy), _F(cx), _F(cy), _dptr(residual.contiguous()),
+            _dptr(weights.contiguous() if weights is not None else None), _F(min_weight_sum), _dptr(out), None,
             _stream(stream)))
-        return out, int(skipped.value)
 
     def depth_tensor(self):
         """The depth output buffer as a (H,W) float32 torch tensor view."""

@@ -38,8 +38,8 @@ def hosttest_lib(tmp_path_factory):
     import subprocess
 
     out = str(tmp_path_factory.mktemp("hosttest") / "libvsg_hosttest.so")
-    subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", out,
-                    os.path.join(PKG, "csrc", "vsg_hosttest.c"), "-lm"], check=True)
+    subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-I", os.path.join(PKG, "csrc"), "-o", out,
+                    os.path.join(ROOT, "tests", "hosttest.c"), "-lm"], check=True)
     return ctypes.CDLL(out)
 
 

@@ -1,8 +1,9 @@
 """Batched form (vsg_batch_*): independent scans of uneven resolution and
 frame count advanced together must give, scene by scene and step by step,
-exactly the results of vsg_integrate + vsg_render run one scene at a time.
-Covers the eager first step of each shape, graph replays, and shapes that
-change as scans finish (needs a GPU)."""
+exactly the results of vsg_integrate + vsg_render run one scene at a time,
+and of the CPU oracle restating the reference.  Covers the eager first step
+of each shape, graph replays, and shapes that change as scans finish (needs
+a GPU)."""
 import numpy as np
 import pytest
 
@@ -106,3 +107,46 @@ def test_batch_rejects_bad_frames(cuda, synth_mod):
     cuda.cuda.synchronize()
     assert sc.stats()["integrated_frames"] == 1
     b.close()
+
+
+def test_batch_matches_oracle(cuda, synth_mod, oracle_mod):
+    """Every batched scene against the CPU oracle restating the reference,
+    step by step: block sets and voxels bit for bit after each step, the
+    full ray cast bit for bit (depth, position, colour, normal), and the
+    per-frame counters."""
+    import vsg
+
+    streams = _streams(synth_mod)
+    kw = dict(voxel_size=0.004, truncation=0.02, hash_num_slots=30011, num_sdf_blocks=40000)
+    scenes = [vsg.Scene(**kw) for _ in streams]
+    rends = [vsg.Renderer(K.width, K.height) for _, K in streams]
+    oracles = [oracle_mod.OracleScene(0.004) for _ in streams]
+    batch = vsg.Batch(scenes, rends)
+    maps = [[_dev(cuda, f) for f in fr] for fr, _ in streams]
+    steps = max(len(fr) for fr, _ in streams)
+    for t in range(steps):
+        frames, ost = [], {}
+        for i, (fr, K) in enumerate(streams):
+            if t < len(fr):
+                pm, rgb, nm = maps[i][t]
+                frames.append(batch.frame(i, pm, rgb, nm, K.width, K.height, 0.02, fr[t].pose, K.fx, K.fy,
+                                          K.cx, K.cy, 0.2, 3.0, render=True))
+                ost[i] = oracles[i].integrate(fr[t].pointmap, fr[t].rgb, 0.02, fr[t].pose, K.fx, K.fy, K.cx, K.cy)
+        batch.step(frames)
+        cuda.cuda.synchronize()
+        for i, (fr, K) in enumerate(streams):
+            if t >= len(fr):
+                continue
+            gc, gv = scenes[i].export()
+            oc, ov = oracles[i].export()
+            v = compare_volumes(gc, gv, oc, ov["raw"])
+            assert v["same_blocks"] and v["bit_exact"], (t, i, v)
+            o = oracles[i].render(K.width, K.height, fr[t].pose, K.fx, K.fy, K.cx, K.cy, 0.2, 3.0)
+            r = compare_renders(rends[i].download(), o)
+            assert r["bit_exact_all"] and r["hits_gpu"] > 0, (t, i, r)
+            st = scenes[i].stats()
+            assert st["flags"] == 0
+            assert st["frame_new_blocks"] == ost[i]["new_blocks"], (t, i)
+            assert st["frame_updated_blocks"] == ost[i]["updated_blocks"], (t, i)
+            assert st["frame_updated_voxels"] == ost[i]["updated_voxels"], (t, i)
+    batch.close()

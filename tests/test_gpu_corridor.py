@@ -90,3 +90,96 @@ def test_corridor_frame_to_model_tracking(cuda, synth_mod):
     rot = [np.degrees(np.arccos(np.clip((np.trace(e[:3, :3].T @ np.asarray(f.pose, np.float64)[:3, :3]) - 1) / 2,
                                         -1, 1))) for e, f in zip(est, fr)]
     assert max(err) < 0.015 and max(rot) < 0.5, (err, rot)
+
+
+def test_batched_corridors_match_oracle(cuda, synth_mod, oracle_mod):
+    """Three corridors of uneven length advanced together: each step streams
+    every live corridor out and in (vsg.stream_scenes: host threads, one CUDA
+    stream per corridor), then integrates and ray casts all of them in one
+    vsg_batch_step.  Each corridor against its own oracle (OracleScene +
+    ChunkStore, the per-scene loop above): stream counts every frame; volume,
+    host store and render bit-exact at checkpoints."""
+    import vsg
+
+    specs = [(3, 30, 4.0, 60), (7, 18, 3.0, 40), (11, 24, 3.5, 50)]  # seed, frames, length, primitives
+    streams = [synth_mod.corridor_stream(sd, n, 160, 120, length=ln, n_prims=npr) for sd, n, ln, npr in specs]
+    K = streams[0][1]
+    scenes = [vsg.Scene(voxel_size=VOXEL, truncation=TRUNC, hash_num_slots=50021, num_sdf_blocks=120000)
+              for _ in specs]
+    rends = [vsg.Renderer(K.width, K.height) for _ in specs]
+    stores = [vsg.Store((0.5, 0.5, 0.5)) for _ in specs]
+    orcs = [oracle_mod.OracleScene(VOXEL) for _ in specs]
+    ostores = [oracle_mod.ChunkStore(VOXEL, (0.5, 0.5, 0.5)) for _ in specs]
+    batch = vsg.Batch(scenes, rends)
+    cstreams = [cuda.cuda.Stream() for _ in specs]
+    r_out, r_in = 2.5, 1.5
+    maps = [[tuple(cuda.from_numpy(x).cuda() for x in (f.pointmap, f.rgb, f.normals)) for f in fr]
+            for fr, _ in streams]
+    total_out = total_in = 0
+    for t in range(max(len(fr) for fr, _ in streams)):
+        live = [i for i, (fr, _) in enumerate(streams) if t < len(fr)]
+        centers = []
+        for i in live:
+            T = np.asarray(streams[i][0][t].pose, np.float32)
+            centers.append((T[:3, 3] + 0.75 * T[:3, 2]).astype(np.float32))
+        got = vsg.stream_scenes([scenes[i] for i in live], [stores[i] for i in live], centers, r_out, r_in,
+                                streams=[cstreams[i] for i in live])
+        frames = []
+        for k, i in enumerate(live):
+            c = centers[k]
+            oc, ov = orcs[i].stream_out(c, r_out)
+            ostores[i].add(oc, ov)
+            ic, iv = ostores[i].take(c, r_in)
+            orcs[i].stream_in(ic, iv)
+            assert got[k] == (len(oc), len(ic), 0), (t, i, got[k])
+            total_out += got[k][0]
+            total_in += got[k][1]
+            f = streams[i][0][t]
+            pm, rgb, nm = maps[i][t]
+            frames.append(batch.frame(i, pm, rgb, nm, K.width, K.height, TRUNC, f.pose, K.fx, K.fy, K.cx, K.cy,
+                                      0.2, 4.0, render=True))
+            orcs[i].integrate(f.pointmap, f.rgb, TRUNC, f.pose, K.fx, K.fy, K.cx, K.cy)
+        batch.step(frames)
+        cuda.cuda.synchronize()
+        for i in live:
+            n = len(streams[i][0])
+            if t % 6 == 5 or t == n - 1:
+                gc, gv = scenes[i].export()
+                occ, ovv = orcs[i].export()
+                v = compare_volumes(gc, gv, occ, ovv["raw"])
+                assert v["same_blocks"] and v["bit_exact"], (t, i, v)
+                sc_c, sc_v = stores[i].export()
+                os_c, os_v = ostores[i].export()
+                assert np.array_equal(sc_c, os_c) and np.array_equal(sc_v, os_v), (t, i)
+                f = streams[i][0][t]
+                want = orcs[i].render(K.width, K.height, f.pose, K.fx, K.fy, K.cx, K.cy, 0.2, 4.0)
+                assert compare_renders(rends[i].download(), want)["bit_exact_all"], (t, i)
+    assert total_out > 10000 and total_in > 2000, (total_out, total_in)
+    assert all(s.stats()["flags"] == 0 for s in scenes)
+    batch.close()
+
+
+def test_batched_tracking_equals_per_scene_tracking(cuda, synth_mod):
+    """vsg.refine_poses (lockstep Gauss-Newton over several scenes, one host
+    synchronisation per step, one CUDA stream per problem) returns exactly
+    the poses and residual histories of vsg.refine_pose run problem by
+    problem."""
+    import vsg
+
+    probs = []
+    for seed in (5, 6, 9):
+        fr, K = synth_mod.corridor_stream(seed, 120, 320, 240, length=4.0, n_prims=70, frame_ids=range(4))
+        sc = vsg.Scene(voxel_size=VOXEL, truncation=TRUNC, hash_num_slots=100003, num_sdf_blocks=150000)
+        for f in fr[:3]:
+            pm, rgb, nm = (cuda.from_numpy(x).cuda() for x in (f.pointmap, f.rgb, f.normals))
+            sc.integrate(pm, rgb, nm, K.width, K.height, TRUNC, f.pose, K.fx, K.fy, K.cx, K.cy)
+        z = cuda.from_numpy(np.ascontiguousarray(fr[3].pointmap[..., 2])).cuda()
+        target = cuda.where(z > 0, z, cuda.full_like(z, 1e10))
+        probs.append((sc, vsg.Renderer(K.width, K.height), target, np.asarray(fr[2].pose, np.float64)))
+    kw = dict(steps=10, min_incidence=0.5)
+    seq = [vsg.refine_pose(sc, rr, tg, T0, K.fx, K.fy, K.cx, K.cy, 0.2, 2.0, **kw) for sc, rr, tg, T0 in probs]
+    Ts, rms = vsg.refine_poses([p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs],
+                               [p[3] for p in probs], (K.fx, K.fy, K.cx, K.cy), 0.2, 2.0,
+                               streams=[cuda.cuda.Stream() for _ in probs], **kw)
+    for (T1, r1), T2, r2 in zip(seq, Ts, rms):
+        assert np.array_equal(T1, T2) and r1 == r2 and len(r1) > 3

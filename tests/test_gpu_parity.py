@@ -55,6 +55,19 @@ def _run_stream(torch, oracle_mod, frames, K, trunc=0.02, voxel=0.004, slots=200
     return reports
 
 
+def _triangle_digests(verts, norms):
+    """Sorted 64-bit digest per triangle of its 18 floats' bit patterns."""
+    m = verts.shape[0]
+    words = np.concatenate([verts.reshape(m, 9).view(np.uint32), norms.reshape(m, 9).view(np.uint32)], 1)
+    h = np.full(m, 0x9E3779B97F4A7C15, np.uint64)
+    with np.errstate(over="ignore"):
+        for k in range(18):
+            h ^= words[:, k].astype(np.uint64) + np.uint64(0x632BE59BD9B4E019) + (h << np.uint64(6)) + (h >> np.uint64(2))
+            h *= np.uint64(0xBF58476D1CE4E5B9)
+    h.sort()
+    return h
+
+
 def _assert_reports(reports):
     for rep in reports:
         if "volume" in rep:
@@ -82,8 +95,10 @@ def test_tabletop_small(cuda, oracle_mod, synth_mod, wh, frames):
     # the kernels restate the reference bit for bit
     assert all(r["volume"]["bit_exact"] for r in reports if "volume" in r)
     assert all(r["render"]["bit_exact_all"] for r in reports if "render" in r)
-    # the fixed-divisor division passed its exhaustive check for 4 mm
+    # the fixed-divisor division passed its exhaustive check for 4 mm, and
+    # every running-average divisor its check
     assert reports[-1]["stats"]["fast_division"] == 1
+    assert reports[-1]["stats"]["fast_avg_divisors"] == 256
 
 
 def test_tabletop_full_size(cuda, oracle_mod, synth_mod):
@@ -93,6 +108,25 @@ def test_tabletop_full_size(cuda, oracle_mod, synth_mod):
     for r in reports:
         print(r)
     _assert_reports(reports)
+
+
+def test_tabletop_full_stream_30_frames(cuda, oracle_mod, synth_mod):
+    """The whole timed workload: 30 frames 640x480, 4 mm, trunc 0.02, 200000
+    slots and blocks, min/max depth 0.2/3.0 m.  The volume is compared with
+    the oracle after every frame (the later frames grow the volume, the
+    overflow chains and the skip grids) and the full-frame ray cast every
+    5th frame and at the last, all bit for bit."""
+    fr, K = synth_mod.tabletop_stream(0, 30)
+    reports = _run_stream(cuda, oracle_mod, fr, K, render_every=5)
+    _assert_reports(reports)
+    assert all(r["volume"]["bit_exact"] for r in reports)
+    renders = [r["render"] for r in reports if "render" in r]
+    assert len(renders) == 7
+    for r in renders:
+        assert r["bit_exact_all"] and r["hits_gpu"] > 0.5 * r["pixels"], r
+    print({"blocks": reports[-1]["volume"]["gpu_blocks"],
+           "depth_max_err": max(r["depth_max_err"] for r in renders),
+           "depth_rms_err": max(r["depth_rms_err"] for r in renders)})
 
 
 def test_other_seed_and_truncation(cuda, oracle_mod, synth_mod):
@@ -131,15 +165,18 @@ def test_render_empty_scene_leaves_outputs(cuda, synth_mod):
         assert np.array_equal(first[k].view(np.uint32), second[k].view(np.uint32)), k
 
 
-def test_room_1280x720_2mm(cuda, oracle_mod, synth_mod):
+def test_room_1280x720_2mm(cuda, oracle_mod, synth_mod, hosttest_lib):
     """The room workload: 1280x720 frames of a seeded 4x3x2.5 m room with 40
     boxes and 20 spheres on a random walk, 2 mm voxels, truncation 0.01 m,
     2^20 buckets and pool blocks.  Volumes bit-exact after every frame; the
-    ray cast compared on a band of rows at full width (the oracle's full
-    frame would take minutes)."""
+    last frame's full ray cast (depth, position, colour, normal) bit-exact;
+    marching cubes over the room volume equal to the oracle's extraction
+    from its own volume, triangle for triangle."""
+    import ctypes
+
     import vsg
 
-    fr, K = synth_mod.room_stream(1, 3, 1280, 720)
+    fr, K = synth_mod.room_stream(1, 8, 1280, 720)
     voxel, trunc = 0.002, 0.01
     sc = vsg.Scene(voxel_size=voxel, truncation=trunc, hash_num_slots=1 << 20, num_sdf_blocks=1 << 20)
     rr = vsg.Renderer(K.width, K.height)
@@ -154,15 +191,33 @@ def test_room_1280x720_2mm(cuda, oracle_mod, synth_mod):
         assert v["same_blocks"] and v["bit_exact"], (i, v)
         st = sc.stats()
         assert st["flags"] == 0 and st["frame_new_blocks"] == ost["new_blocks"]
+        assert st["frame_updated_voxels"] == ost["updated_voxels"]
     f = fr[-1]
     rr.render(sc, f.pose, K.fx, K.fy, K.cx, K.cy, 0.2, 4.0)
     g = rr.download()
-    rows = (340, 372)
-    o = orc.render(K.width, K.height, f.pose, K.fx, K.fy, K.cx, K.cy, 0.2, 4.0, rows=rows)
-    band = {k: g[k][rows[0]:rows[1]] for k in ("depth", "position", "color", "normal")}
-    want = {k: o[k][rows[0]:rows[1]] for k in ("depth", "position", "color", "normal")}
-    r = compare_renders(band, want, DEPTH_TOL)
+    o = orc.render(K.width, K.height, f.pose, K.fx, K.fy, K.cx, K.cy, 0.2, 4.0)
+    r = compare_renders(g, o, DEPTH_TOL)
+    print(r)
     assert r["bit_exact_all"] and r["hits_gpu"] > 0.5 * r["pixels"], r
+    # marching cubes (MarchingCubes.cu:352-571) over the room volume
+    tab = np.zeros((256, 16), np.uint8)
+    hosttest_lib.vsg_test_mc_table.argtypes = [ctypes.c_void_p]
+    hosttest_lib.vsg_test_mc_table(tab.ctypes.data)
+    probe = vsg.MarchingCubes(1)
+    probe.run(sc)
+    need = probe.count()
+    probe.close()
+    mc = vsg.MarchingCubes(need)
+    mc.run(sc)
+    n, verts, norms = mc.download()
+    on, ov_, onrm = orc.marching_cubes(tab, 0.0, voxel, need)
+    assert n == on == need > 100000
+    # ~10^7 triangles: compared as sorted multisets of 64-bit digests of
+    # their 18 floats' bit patterns (both sides append in an unspecified order)
+    assert np.array_equal(_triangle_digests(verts, norms), _triangle_digests(ov_, onrm))
+    mc.close()
+    sc.close()
+    rr.close()
 
 
 @pytest.mark.parametrize("wh,frames,slots", [((160, 120), 6, 200000), ((320, 240), 3, 200000),
