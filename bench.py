@@ -62,6 +62,11 @@ def parse():
     ap.add_argument("--no-room", action="store_true")
     ap.add_argument("--corridor-frames", type=int, default=400)
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--room-frames", type=int, default=300)
+    ap.add_argument("--room-only", action="store_true",
+                    help="run only the room leg and print its object (profiling runs)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="time the headline step and skip every side measurement (profiling runs)")
     ap.add_argument("--corridor-scale", type=float, default=0.1,
                     help="batched corridors: fraction of the U[500,2000] frame counts to run")
     return ap.parse_args()
@@ -281,6 +286,11 @@ def run_ours(args):
 
     import vsg
 
+    if args.room_only:
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps({"room": room_measure(measured_peak_hbm()[0], args.room_frames)}), flush=True)
+        return
+
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -394,6 +404,14 @@ def run_ours(args):
         except Exception as exc:  # noqa: BLE001
             line[name] = {"error": f"{type(exc).__name__}: {exc}"}
 
+    if args.headline_only:
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        sc.close()
+        rr.close()
+        if dist:
+            dist.destroy_process_group()
+        return
     side("marching_cubes", mc_measure, sc, peak)
     side("surface_points", points_measure, sc, peak)
     side("streaming", stream_measure, sc)
@@ -402,7 +420,7 @@ def run_ours(args):
     if not args.no_ref_gpu and rank == 0:
         side("ref_gpu", ref_gpu_measure, frames, K)
     if not args.no_room:
-        side("room", room_measure, peak)
+        side("room", room_measure, peak, args.room_frames)
     if not args.no_e2e:
         line["e2e"] = e2e(args, frames, K, sc, rr)
     if not args.no_corridor:
