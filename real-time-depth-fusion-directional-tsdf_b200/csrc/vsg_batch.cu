@@ -11,7 +11,9 @@
 //   stage 3  integration workers, each taking visible blocks from the
 //            scene's work counter (integrate_work)
 //   stage 4  ray-distance bounds, strided over the pool (tile_bounds_range)
-//   stage 5  ray-cast tiles, 16x16 pixels (render_pixel)
+//   stage 5  ray-cast workers: each warp takes 8x4 pixel tiles from the
+//            scene's tile counter until none is left (render_pixel), so a
+//            CTA waits for its slowest warp once per item, not per tile
 // An item of stage k of scene i first waits until every item of the scene's
 // previous non-empty stage has finished: per scene and stage a counter that
 // finished items raise (release: CTA barrier, fence, atomic add) and that a
@@ -21,7 +23,9 @@
 // claimed in order, so an item only ever waits for items claimed earlier by
 // CTAs that are running; the earliest unfinished item never waits, and the
 // launch always completes.  Each wait is bounded all the same: after
-// kWaitLimit polls the item records VSG_FLAG_BATCH_WAIT in the scene's flags
+// kWaitLimit polls the item records VSG_FLAG_BATCH_WAIT in the scene's flags,
+// raises the launch's abort word -- every later wait of the launch then
+// returns at once, so a launch stalls for at most about one wait limit --
 // and goes on.  Data written earlier in the same launch (pixel buffers,
 // hash, voxels, skip grids, bounds) is read through the coherent load path
 // (VSG_COHERENT_LOADS).  Each stage runs exactly the per-scene device code
@@ -59,9 +63,10 @@ namespace vsg {
 constexpr int kMaxBatch = 256;
 constexpr int kStages = 6;
 constexpr int kStepThreads = 256;
-constexpr int kRenderTile = 16;   // 16x16 pixels: 8 warps of 8x4
+constexpr int kTilesPerWarp = 6;  // ray-cast workers per scene: 8x4 tiles / (8 warps x this)
 constexpr int kWaitLimit = 1 << 22;  // polls of 64-128 ns: about a second
-constexpr int kSyncWords = 32 + kMaxBatch * kStages;  // claim counter (own line), stage counters
+// claim counter and abort word (own line), stage counters, ray-cast tile counters
+constexpr int kSyncWords = 32 + kMaxBatch * kStages + kMaxBatch;
 
 struct BatchHeader {
     int n;
@@ -71,7 +76,6 @@ struct BatchHeader {
     uint32_t stage_end[kStages];               // items of stages 0..s, all scenes
     uint32_t prefix[kStages][kMaxBatch + 1];   // items of stage s of the scenes before i
     int alloc_tiles_x[kMaxBatch];
-    int render_tiles_x[kMaxBatch];
 };
 
 // device layout of one step: the header of the whole step, the header of its
@@ -106,14 +110,18 @@ __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
     return v;
 }
 
-// Whole CTA: wait until *ctr reaches `target` (bounded; on giving up, flag
-// the scene and go on).
-__device__ __forceinline__ void wait_stage(const uint32_t* ctr, uint32_t target, uint32_t* scene_flags) {
+// Whole CTA: wait until *ctr reaches `target`.  Bounded: after kWaitLimit
+// polls flag the scene, raise the launch's abort word and go on; once the
+// abort word is up no wait of the launch polls any more.
+__device__ __forceinline__ void wait_stage(const uint32_t* ctr, uint32_t target, uint32_t* scene_flags,
+                                           uint32_t* abort_word) {
     if (threadIdx.x == 0 && target) {
         int polls = 0;
         while (ld_acquire_u32(ctr) < target) {
+            if (*(volatile uint32_t*)abort_word) break;
             if (++polls > kWaitLimit) {
                 atomicOr(scene_flags, (uint32_t)VSG_FLAG_BATCH_WAIT);
+                atomicExch(abort_word, 1u);
                 break;
             }
             __nanosleep(64);
@@ -128,10 +136,12 @@ __global__ void __launch_bounds__(kStepThreads, 3) k_batch_step(const BatchHeade
                                                                 const RenderArgs* __restrict__ ra, uint32_t* sync) {
     __shared__ uint32_t s_item;
     uint32_t* claim = sync;
+    uint32_t* abort_word = sync + 1;
     uint32_t* done = sync + 32;
+    uint32_t* tiles = done + kMaxBatch * kStages;
     const int n = h->n;
     const uint32_t total = h->n_items;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     for (;;) {
         __syncthreads();  // every thread has read the previous s_item
         if (threadIdx.x == 0) s_item = atomicAdd(claim, 1u);
@@ -148,7 +158,7 @@ __global__ void __launch_bounds__(kStepThreads, 3) k_batch_step(const BatchHeade
             int prev = st - 1;
             while (prev > 0 && h->prefix[prev][i + 1] == h->prefix[prev][i]) --prev;
             wait_stage(done + i * kStages + prev, h->prefix[prev][i + 1] - h->prefix[prev][i],
-                       &ia[i].s.ctr->flags);
+                       &ia[i].s.ctr->flags, abort_word);
         }
         if (st == 0) {
             if (h->full && threadIdx.x == 0) frame_begin(ia[i].s.frame);
@@ -169,10 +179,16 @@ __global__ void __launch_bounds__(kStepThreads, 3) k_batch_step(const BatchHeade
             tile_bounds_range(ra[i], k * kStepThreads + threadIdx.x, cnt * kStepThreads);
         } else {
             const RenderArgs& R = ra[i];
-            const int tx = h->render_tiles_x[i];
-            const int x = (int)(k % (uint32_t)tx) * kRenderTile + (warp & 1) * 8 + (lane & 7);
-            const int y = (int)(k / (uint32_t)tx) * kRenderTile + (warp >> 1) * 4 + (lane >> 3);
-            if (x < R.W && y < R.H) render_pixel(R, x, y);
+            const int tx = (R.W + 7) / 8;
+            const uint32_t ntiles = (uint32_t)tx * (uint32_t)((R.H + 3) / 4);
+            for (;;) {
+                uint32_t tt = 0;
+                if (lane == 0) tt = atomicAdd(tiles + i, 1u);
+                tt = __shfl_sync(0xFFFFFFFFu, tt, 0);
+                if (tt >= ntiles) break;
+                const int x = (int)(tt % (uint32_t)tx) * 8 + (lane & 7), y = (int)(tt / (uint32_t)tx) * 4 + (lane >> 3);
+                if (x < R.W && y < R.H) render_pixel(R, x, y);
+            }
         }
         __syncthreads();  // the item's writes are done
         if (threadIdx.x == 0) {
@@ -355,15 +371,16 @@ int vsg_batch_step(vsg_batch* b, const vsg_batch_frame* frames, int n_frames, vs
             const vsg_batch_frame& f = frames[k];
             Scene* sc = B.scenes[f.scene];
             const int ax = (f.w + kTile - 1) / kTile, ay = (f.h + kTile - 1) / kTile;
-            const int rx = (f.w + kRenderTile - 1) / kRenderTile, ry = (f.h + kRenderTile - 1) / kRenderTile;
+            const int rtiles = ((f.w + 7) / 8) * ((f.h + 3) / 4);
+            const int rworkers = std::max(1, (rtiles + kStepThreads / 32 * kTilesPerWarp - 1) /
+                                                 (kStepThreads / 32 * kTilesPerWarp));
             h->alloc_tiles_x[k] = hr->alloc_tiles_x[k] = ax;
-            h->render_tiles_x[k] = hr->render_tiles_x[k] = rx;
             cnt[0][k] = 1;
             cnt[1][k] = (uint32_t)(ax * ay);
             cnt[2][k] = (uint32_t)sel_items;
             cnt[3][k] = (uint32_t)integ_items;
             cnt[4][k] = f.render ? (uint32_t)bnd_items : 0u;
-            cnt[5][k] = f.render ? (uint32_t)(rx * ry) : 0u;
+            cnt[5][k] = f.render ? (uint32_t)rworkers : 0u;
             cnt_r[0][k] = f.render ? 1u : 0u;
             cnt_r[1][k] = cnt_r[2][k] = cnt_r[3][k] = 0u;
             cnt_r[4][k] = cnt[4][k];

@@ -11,6 +11,9 @@
 namespace vsg {
 
 constexpr int kMaxMarch = 1 << 22;  // iteration guard of one ray
+// Shortest run (in march steps across the cell's remaining length) over which
+// a ray jumps to the run's last sample in a cell without positive voxels.
+constexpr float kMinPosRun = 4.0f;
 
 struct RenderArgs {
     SceneDev s;
@@ -521,13 +524,14 @@ static __device__ __forceinline__ bool ray_step(const RenderArgs& a, RayState& r
             // (lastSdf < 0 && dist > 0, RayCastRender.cu:321), and after a
             // run of them the march state (lastValid, lastSdf, lastAlpha) is
             // that of the run's last sample alone.  Replay the chain to the
-            // last sample before the cell's far end and evaluate only that one.
+            // last sample before the cell's far end and evaluate only that
+            // one -- when the run is long enough for the replay to cost less
+            // than the samples it saves (short runs are sampled in turn).
+            const float end = fminf(thi - m, r.re);
             if (r.rc > tlo + m && r.rc < thi - m) {
-                int to_end = 0;  // additions to the first sample at or past the far end
-                (void)vsg_chain_advance(r.rc, v * 0.5f, fminf(thi - m, r.re), kMaxMarch - r.steps, &to_end);
-                if (to_end > 1) {
+                if (end - r.rc > kMinPosRun * (v * 0.5f)) {
                     const int before = r.steps;
-                    r.rc = vsg_chain_advance(r.rc, v * 0.5f, 3.0e38f, to_end - 1, &r.steps);
+                    r.rc = vsg_chain_advance_ex(r.rc, v * 0.5f, end, kMaxMarch - r.steps, &r.steps, 1);
                     r.n_skip += (uint32_t)(r.steps - before);
                     ++r.n_jump;
                 }

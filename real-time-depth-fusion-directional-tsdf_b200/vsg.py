@@ -385,10 +385,10 @@ def refine_poses(scenes, renderers, targets, poses, intrinsics, min_depth, max_d
     cur = torch.cuda.current_stream()
     if streams is None:
         streams = [cur] * n
-    for st in {id(x): x for x in streams}.values():
-        st.wait_stream(cur)
     for r in renderers:
         r.record(True)
+    # everything the problems' streams read is made on the current stream
+    # first; then those streams wait for it
     rays = [_unit_rays(renderers[i].width, renderers[i].height, *K[i]) if min_incidence > 0 else None
             for i in range(n)]
     r0, r1 = (float(max_residual[0]), float(max_residual[1])) if max_residual is not None else (np.inf, np.inf)
@@ -397,6 +397,8 @@ def refine_poses(scenes, renderers, targets, poses, intrinsics, min_depth, max_d
     ne = torch.zeros((n, 27), dtype=torch.float64, device="cuda")
     cnt = torch.zeros(n, dtype=torch.int64, device="cuda")
     res = torch.zeros(n, dtype=torch.float32, device="cuda")
+    for st in {id(x): x for x in streams}.values():
+        st.wait_stream(cur)
     for k in range(steps):
         todo = [i for i in range(n) if active[i]]
         if not todo:
