@@ -69,11 +69,9 @@ enum {
     VSG_FLAG_COORD_RANGE = 4u,      /* a block coordinate outside +-2^20 was skipped */
     VSG_FLAG_INSERT_RETRY = 8u,     /* a bounded insert retry loop gave up */
     VSG_FLAG_MARCH_LIMIT = 16u,     /* a ray hit the iteration guard */
-    VSG_FLAG_PARENT_OVERFLOW = 32u, /* normal-direction allocation: a frame's parent records
+    VSG_FLAG_PARENT_OVERFLOW = 32u  /* normal-direction allocation: a frame's parent records
                                        overflowed (a DDA ran to its 1024-block guard); some
                                        blocks kept an older parent pixel */
-    VSG_FLAG_BATCH_WAIT = 64u       /* batched step: a stage of this scene gave up waiting for
-                                       its previous stage (bounded wait) and ran anyway */
 };
 
 /* GlobalParamsConfig knobs (globalPramasConfig.h:101-109) and the sizes
@@ -282,6 +280,16 @@ VSG_API int vsg_renderer_save_ply(const vsg_renderer* r, const char* path, int64
  * The render must have used the same scene, unchanged since, and the pose's
  * translation as ray origin (vsg_render_hostpose does). */
 VSG_API int vsg_renderer_record(vsg_renderer* r, int enable);
+/* March step of this renderer's ray casts, in metres (no reference
+ * counterpart; the reference always steps half a voxel, RayCastRender.cu:
+ * 389-392).  0 (the default) keeps the reference's step and its depths bit
+ * for bit.  Any positive value is an opt-in approximation for callers that
+ * trade depth accuracy for speed: samples are taken every `step` metres and
+ * the crossing is refined as before, so depths move by up to a few
+ * millimetres and thin structures can be missed.  Applies to vsg_render,
+ * vsg_render_hostpose and the batched step.  Negative or non-finite values:
+ * VSG_ERR_INVALID_ARG. */
+VSG_API int vsg_renderer_set_step(vsg_renderer* r, float step);
 /* grad_depth: device float[w*h] dL/d depth (NULL = 0); grad_position: device
  * float4[w*h] dL/d position (NULL = 0).  grad_pose: DEVICE double[12]
  * receiving dL/dT for the row-major 3x4 camera->world matrix (written;

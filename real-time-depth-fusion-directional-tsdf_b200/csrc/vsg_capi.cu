@@ -330,6 +330,13 @@ int vsg_render_hostpose(vsg_renderer* r, const vsg_scene* s, const float cam_pos
                               min_depth, max_depth, (cudaStream_t)stream);
 }
 
+int vsg_renderer_set_step(vsg_renderer* r, float step) {
+    if (!r) return VSG_ERR_NOT_ALLOCATED;
+    if (!(step >= 0.0f) || !std::isfinite(step)) return VSG_ERR_INVALID_ARG;
+    r->impl.step = step;
+    return VSG_OK;
+}
+
 int vsg_renderer_outputs(const vsg_renderer* r, float** depth, float** position, float** color, float** normal) {
     if (!r) return VSG_ERR_INVALID_ARG;
     if (depth) *depth = r->impl.depth;

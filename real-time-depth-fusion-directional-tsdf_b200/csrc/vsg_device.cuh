@@ -13,20 +13,16 @@
 //   block_fresh u8[B]             1 until the block's first integration pass
 //   block_wmask u64[B]            bit (sz*4+sy)*4+sx: sub-cube (2x2x2 voxels)
 //                                 holds a voxel with weight > 0
-//   block_pmask u64[B]            same bits: sub-cube has held a weighted
-//                                 voxel with SDF > 0 (kept by OR)
 //   heap        u32[B]            free-list stack of pool indices
 //   bindex      u64[2^(3k)]       dense toroidal block index: cell (x,y,z) mod 2^k
 //                                 holds ptr (22 bits) | high coordinate bits
 //                                 (tag) << 22 of the one block mapped there;
 //                                 ~0 = none, ~0-1 = several (use the hash)
-//   dmask       u64x2[2^(3k)]     per toroidal block position, .x: sub-cubes
-//                                 that have a weighted sub-cube within one
-//                                 sub-cube (3x3x3, across block faces); .y:
-//                                 the same dilation of the positive sub-cubes
-//                                 (block_pmask); ray-march skip grid
+//   dwm         u64[2^(3k)]       per toroidal block position: sub-cubes that
+//                                 have a weighted sub-cube within one sub-cube
+//                                 (3x3x3, across block faces); ray-march skip
 //   sup         u32[2^(3(k-3))/32] per toroidal super-cell (8^3 block
-//                                 positions): some dmask word in it is non-zero
+//                                 positions): some dwm word in it is non-zero
 //   visible     u32[B]            pool indices the current frame integrates
 //   pix_world   float4[W*H]       per pixel of the current frame: world point
 //                                 T*p and its camera distance (-1: invalid)
@@ -42,17 +38,6 @@
 
 #include <cstdint>
 #include <cuda_runtime.h>
-
-// Loads of data that no CTA writes while the reading kernel runs go through
-// the read-only (non-coherent) cache.  A translation unit whose kernel reads,
-// in the same launch, data that other CTAs of that launch wrote (after
-// waiting for them) defines VSG_COHERENT_LOADS before including the device
-// headers; those loads then take the coherent path.
-#ifdef VSG_COHERENT_LOADS
-#define VSG_LDG(p) (*(p))
-#else
-#define VSG_LDG(p) __ldg(p)
-#endif
 
 namespace vsg {
 
@@ -125,11 +110,10 @@ struct SceneDev {
     int* block_slot;
     uint8_t* block_fresh;
     unsigned long long* block_wmask;  // per block: 2x2x2-voxel sub-cubes holding a weighted voxel
-    unsigned long long* block_pmask;  // per block: sub-cubes that have held a weighted voxel with SDF > 0
     uint8_t* block_touched;           // instrumented renders: block read by a ray
     uint32_t* heap;
     unsigned long long* bindex;
-    ulonglong2* dmask;  // .x dilated weight mask, .y dilated positive mask
+    unsigned long long* dwm;
     uint32_t* sup;
     uint32_t* visible;
     float4* pix_world;   // per pixel of the current frame: T*p and |T*p - c| (-1 = invalid)
@@ -323,14 +307,14 @@ __device__ __forceinline__ int lookup_block(const SceneDev& s, unsigned long lon
     const Entry* bk = s.buckets + (size_t)b * kBucketSlots;
 #pragma unroll
     for (int j = 0; j < kBucketSlots; ++j) {
-        const uint4 e = VSG_LDG(reinterpret_cast<const uint4*>(bk + j));
+        const uint4 e = __ldg(reinterpret_cast<const uint4*>(bk + j));
         const unsigned long long k = ((unsigned long long)e.y << 32) | e.x;
         if (k == key) return (int)e.z;
         if (k == kKeyEmpty) return -1;
     }
-    int n = VSG_LDG(s.bucket_next + b);
+    int n = __ldg(s.bucket_next + b);
     for (int it = 0; n >= 0 && it < s.max_nodes; ++it) {
-        const uint4 e = VSG_LDG(reinterpret_cast<const uint4*>(s.nodes + n));
+        const uint4 e = __ldg(reinterpret_cast<const uint4*>(s.nodes + n));
         const unsigned long long k = ((unsigned long long)e.y << 32) | e.x;
         if (k == key) return (int)e.z;
         n = (int)e.w;
@@ -342,7 +326,7 @@ __device__ __forceinline__ int lookup_block(const SceneDev& s, unsigned long lon
 // cells shared by several blocks.  -1 = not allocated.
 __device__ __forceinline__ int block_ptr(const SceneDev& s, int x, int y, int z) {
     if (!coord_ok(x, y, z)) return -1;
-    const unsigned long long e = VSG_LDG(s.bindex + bidx_cell(x, y, z, s.bidx_log2));
+    const unsigned long long e = __ldg(s.bindex + bidx_cell(x, y, z, s.bidx_log2));
     if (e == kIdxEmpty) return -1;
     if (e == kIdxShared) return lookup_block(s, pack_key(x, y, z), x, y, z);
     return ((e >> 22) == bidx_tag(x, y, z, s.bidx_log2)) ? (int)(e & kIdxPtrMask) : -1;

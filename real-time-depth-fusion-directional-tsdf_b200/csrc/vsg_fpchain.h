@@ -46,33 +46,38 @@ VSG_HD float vsg_u2f(uint32_t u) {
 // 2^k for -126 <= k <= 127
 VSG_HD float vsg_pow2(int k) { return vsg_u2f((uint32_t)(k + 127) << 23); }
 
-// Advance r along r <- RN(r + h) to the first chain value >= target, or,
-// with stop_before, to the last chain value < target (r itself when the next
-// value already reaches it).  Requires h > 0 finite.  *steps receives the
-// number of additions taken; at most max_steps are taken (the caller's
-// iteration guard).  Values of r that are not positive normal floats, and
-// ties, use plain additions (for h = voxel/2 ties never occur in the binades
-// a ray visits).
-VSG_HD float vsg_chain_advance_ex(float r, float h, float target, int max_steps, int* steps, int stop_before) {
+// Advance r along r <- RN(r + h) to the first chain value >= target.
+// Requires h > 0 finite.  *steps receives the number of additions taken;
+// at most max_steps are taken (the caller's iteration guard).  Values of r
+// that are not positive normal floats, and ties, use plain additions (for
+// h = voxel/2 ties never occur in the binades a ray visits).
+VSG_HD float vsg_chain_advance(float r, float h, float target, int max_steps, int* steps) {
     int taken = 0;
     // every pass takes at least one step or returns, so max_steps bounds it
     while (r < target && taken < max_steps) {
         const uint32_t bits = vsg_f2u(r);
         const int be = (int)((bits >> 23) & 0xFFu);
-        const int serial = (bits >> 31) || be < 24 || be >= 254 - 24;  // non-positive, tiny or huge
-        // H = h / u exactly (power-of-two scaling; h / u < 2^24 since h < r
-        // unless the chain is at its very start, which the serial path takes)
-        const int e = be - 127;
-        const float H = serial ? 0.0f : h * vsg_pow2(23 - e);
-        const float Hf = floorf(H);
-        if (serial || !(h < r) || H - Hf == 0.5f) {  // serial step (ties: rounding depends on R's parity)
-            const float nr = r + h;
-            if (stop_before && !(nr < target)) break;
-            r = nr;
+        if ((bits >> 31) || be < 24 || be >= 254 - 24) {  // non-positive, tiny or huge: serial step
+            r = r + h;
             ++taken;
             continue;
         }
+        const int e = be - 127;
+        // H = h / u exactly (power-of-two scaling; h / u < 2^24 since h < r
+        // unless the chain is at its very start, which the serial path takes)
+        if (!(h < r)) {
+            r = r + h;
+            ++taken;
+            continue;
+        }
+        const float H = h * vsg_pow2(23 - e);
+        const float Hf = floorf(H);
         const float frac = H - Hf;
+        if (frac == 0.5f) {  // tie: rounding depends on the parity of R
+            r = r + h;
+            ++taken;
+            continue;
+        }
         const int D = (int)Hf + (frac > 0.5f ? 1 : 0);
         if (D == 0) {  // r + h rounds back to r: the chain is stuck until max_steps
             taken = max_steps;
@@ -96,28 +101,20 @@ VSG_HD float vsg_chain_advance_ex(float r, float h, float target, int max_steps,
         }
         const int room = max_steps - taken;
         if (kneed <= kmax && kneed <= room) {
-            const int k = stop_before ? kneed - 1 : kneed;  // k = 0 keeps r (R u == r)
-            r = (float)(R + k * D) * vsg_pow2(e - 23);
-            taken += k;
+            r = (float)(R + kneed * D) * vsg_pow2(e - 23);
+            taken += kneed;
             break;
         }
-        // every value up to here stays below the target (kneed > k)
         int k = kmax < room ? kmax : room;
         if (k > 0) {
             r = (float)(R + k * D) * vsg_pow2(e - 23);
             taken += k;
         }
         if (taken < max_steps && r < target) {
-            const float nr = r + h;  // the step that crosses into the next binade
-            if (stop_before && !(nr < target)) break;
-            r = nr;
+            r = r + h;  // the step that crosses into the next binade
             ++taken;
         }
     }
     if (steps) *steps += taken;
     return r;
-}
-
-VSG_HD float vsg_chain_advance(float r, float h, float target, int max_steps, int* steps) {
-    return vsg_chain_advance_ex(r, h, target, max_steps, steps, 0);
 }

@@ -143,12 +143,11 @@ int scene_alloc_device(Scene* sc) {
     VSG_MALLOC(d.block_slot, B * sizeof(int));
     VSG_MALLOC(d.block_fresh, B);
     VSG_MALLOC(d.block_wmask, B * sizeof(unsigned long long));
-    VSG_MALLOC(d.block_pmask, B * sizeof(unsigned long long));
     VSG_MALLOC(d.block_touched, B);
     VSG_MALLOC(d.block_parent, B * sizeof(unsigned long long));
     VSG_MALLOC(d.heap, B * sizeof(uint32_t));
     VSG_MALLOC(d.bindex, sizeof(unsigned long long) << (3 * sc->bidx_log2));
-    VSG_MALLOC(d.dmask, sizeof(ulonglong2) << (3 * sc->bidx_log2));
+    VSG_MALLOC(d.dwm, sizeof(unsigned long long) << (3 * sc->bidx_log2));
     VSG_MALLOC(d.sup, sup_words(sc->bidx_log2) * 4);
     VSG_MALLOC(d.visible, B * sizeof(uint32_t));
     d.pix_world = nullptr;
@@ -186,7 +185,7 @@ int scene_alloc_device(Scene* sc) {
 
 void scene_free_device(Scene* sc) {
     SceneDev& d = sc->dev;
-    void* ptrs[] = {d.block_parent, d.parent_key, d.parent_tag, d.block_touched, d.sup, d.dmask,   d.bindex,    d.block_wmask, d.block_pmask, d.buckets,   d.bucket_next,
+    void* ptrs[] = {d.block_parent, d.parent_key, d.parent_tag, d.block_touched, d.sup, d.dwm,     d.bindex,    d.block_wmask, d.buckets,   d.bucket_next,
                     d.nodes,     d.voxels,  d.block_key, d.block_slot,  d.block_fresh, d.heap,
                     d.visible,   d.pix_world, d.pix_rgb, d.ctr,         d.frame, const_cast<float*>(d.avg_recip)};
     for (void* p : ptrs)
@@ -205,7 +204,7 @@ int scene_reset_device(Scene* sc, cudaStream_t st) {
     cudaMemsetAsync(d.block_fresh, 0, B, st);
     cudaMemsetAsync(d.block_parent, 0, B * sizeof(unsigned long long), st);
     cudaMemsetAsync(d.bindex, 0xFF, sizeof(unsigned long long) << (3 * sc->bidx_log2), st);
-    cudaMemsetAsync(d.dmask, 0, sizeof(ulonglong2) << (3 * sc->bidx_log2), st);
+    cudaMemsetAsync(d.dwm, 0, sizeof(unsigned long long) << (3 * sc->bidx_log2), st);
     cudaMemsetAsync(d.sup, 0, sup_words(sc->bidx_log2) * 4, st);
     k_init_heap<<<(unsigned)((B + 255) / 256), 256, 0, st>>>(d.heap, (int)B);
     k_init_counters<<<1, 1, 0, st>>>(d.ctr, (int)B);

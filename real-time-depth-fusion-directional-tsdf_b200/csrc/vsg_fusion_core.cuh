@@ -340,9 +340,9 @@ static __device__ __forceinline__ void alloc_tile(const AllocArgs& a, int tile_x
     const int py = tile_y * kTile + (tid / kTile);
     if (px < a.W && py < a.H) {
         const size_t pi = (size_t)py * a.W + px;
-        const float p0 = VSG_LDG(a.pm + 3 * pi + 0);
-        const float p1 = VSG_LDG(a.pm + 3 * pi + 1);
-        const float p2 = VSG_LDG(a.pm + 3 * pi + 2);
+        const float p0 = __ldg(a.pm + 3 * pi + 0);
+        const float p1 = __ldg(a.pm + 3 * pi + 1);
+        const float p2 = __ldg(a.pm + 3 * pi + 2);
         // integration validity (VoxelScene.cu:1040-1046) drives the depth band
         float4 prep = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
         if (p0 != 0.0f || p1 != 0.0f || p2 != 0.0f) {
@@ -361,8 +361,8 @@ static __device__ __forceinline__ void alloc_tile(const AllocArgs& a, int tile_x
             }
         }
         s.pix_world[pi] = prep;
-        s.pix_rgb[pi] = (uint32_t)VSG_LDG(a.rgb + 3 * pi) | ((uint32_t)VSG_LDG(a.rgb + 3 * pi + 1) << 8) |
-                        ((uint32_t)VSG_LDG(a.rgb + 3 * pi + 2) << 16);
+        s.pix_rgb[pi] = (uint32_t)__ldg(a.rgb + 3 * pi) | ((uint32_t)__ldg(a.rgb + 3 * pi + 1) << 8) |
+                        ((uint32_t)__ldg(a.rgb + 3 * pi + 2) << 16);
         const float cx = a.pose.T[3], cy = a.pose.T[7], cz = a.pose.T[11];
         if constexpr (!by_normal) {
             // allocBlocksFromDepthMapMethod1Kernel, VoxelScene.cu:547-633:
@@ -381,7 +381,7 @@ static __device__ __forceinline__ void alloc_tile(const AllocArgs& a, int tile_x
             }
         } else if (p0 != 0.0f || p1 != 0.0f || p2 != 0.0f) {
             // allocBlocksFromDepthMapMethod2Kernel, VoxelScene.cu:797-911
-            float n0 = VSG_LDG(a.nm + 3 * pi + 0), n1 = VSG_LDG(a.nm + 3 * pi + 1), n2 = VSG_LDG(a.nm + 3 * pi + 2);
+            float n0 = __ldg(a.nm + 3 * pi + 0), n1 = __ldg(a.nm + 3 * pi + 1), n2 = __ldg(a.nm + 3 * pi + 2);
             float nl = sqrtf(n0 * n0 + n1 * n1 + n2 * n2);
             if (!(nl < 0.1f)) {
                 n0 /= nl;
@@ -611,7 +611,6 @@ static __device__ void integrate_block(const IntegArgs& a, int blk, unsigned lon
     const int ppix = parent_pixel(s, blk, a.W, a.H);
     int cnt = 0;
     unsigned long long wm = 0ull;  // sub-cubes that received a weight this frame
-    unsigned long long pm = 0ull;  // sub-cubes with a voxel whose SDF is > 0 after this frame
 #pragma unroll 1
     for (int k0 = 0; k0 < 16; k0 += kIntegBatch) {
         int pix[kIntegBatch];
@@ -634,7 +633,7 @@ static __device__ void integrate_block(const IntegArgs& a, int blk, unsigned lon
         float4 P[kIntegBatch];
 #pragma unroll
         for (int j = 0; j < kIntegBatch; ++j)
-            P[j] = pix[j] >= 0 ? VSG_LDG(s.pix_world + pix[j]) : make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+            P[j] = pix[j] >= 0 ? __ldg(s.pix_world + pix[j]) : make_float4(0.0f, 0.0f, 0.0f, -1.0f);
         float sdfv[kIntegBatch];
         bool upd[kIntegBatch];
 #pragma unroll
@@ -667,7 +666,7 @@ static __device__ void integrate_block(const IntegArgs& a, int blk, unsigned lon
             col[j] = 0u;
             if (upd[j]) {
                 if (!fresh) old[j] = vb[idx];
-                col[j] = VSG_LDG(s.pix_rgb + pix[j]);
+                col[j] = __ldg(s.pix_rgb + pix[j]);
             }
         }
 #pragma unroll
@@ -677,7 +676,7 @@ static __device__ void integrate_block(const IntegArgs& a, int blk, unsigned lon
                 const uint32_t ow = old[j].rgbw >> 24;
                 const float oldW = (float)ow;
                 const float newW = oldW + 1.0f;
-                const float yw = VSG_LDG(s.avg_recip + ow + 1u);  // RN(1 / newW), 0: IEEE division
+                const float yw = __ldg(s.avg_recip + ow + 1u);  // RN(1 / newW), 0: IEEE division
                 const float nsdf = avg_div(old[j].sdf * oldW + sdfv[j] * 1.0f, newW, yw);
                 const uint32_t nw = (uint32_t)fminf(255.0f, newW);
                 const float nr = avg_div((float)(old[j].rgbw & 0xFFu) * oldW + (float)(col[j] & 0xFFu) * 1.0f, newW, yw);
@@ -692,9 +691,7 @@ static __device__ void integrate_block(const IntegArgs& a, int blk, unsigned lon
                 ++cnt;
                 const int k = k0 + j;
                 const int ly = (lane >> 3) + ((k & 1) << 2), lz = k >> 1;
-                const unsigned long long bit = 1ull << ((((lz >> 1) * 4 + (ly >> 1)) * 4) + (lx >> 1));
-                wm |= bit;
-                if (!(nsdf <= 0.0f)) pm |= bit;
+                wm |= 1ull << ((((lz >> 1) * 4 + (ly >> 1)) * 4) + (lx >> 1));
             } else if (fresh) {
                 vb[idx] = Voxel{0.0f, 0u};
             }
@@ -704,27 +701,19 @@ static __device__ void integrate_block(const IntegArgs& a, int blk, unsigned lon
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, o);
     const unsigned wlo = __reduce_or_sync(0xFFFFFFFFu, (unsigned)wm);
     const unsigned whi = __reduce_or_sync(0xFFFFFFFFu, (unsigned)(wm >> 32));
-    const unsigned plo = __reduce_or_sync(0xFFFFFFFFu, (unsigned)pm);
-    const unsigned phi = __reduce_or_sync(0xFFFFFFFFu, (unsigned)(pm >> 32));
     const unsigned long long old_wm = fresh ? 0ull : s.block_wmask[blk];
-    const unsigned long long old_pm = fresh ? 0ull : s.block_pmask[blk];
-    const unsigned long long npm = ((unsigned long long)phi << 32) | plo;
     const unsigned long long newbits = (((unsigned long long)whi << 32) | wlo) & ~old_wm;
-    const unsigned long long newpos = npm & ~old_pm;
-    if ((newbits | newpos) && lane < 27) {
-        // newly weighted / positive sub-cubes: dilate by one sub-cube into
-        // this block position and its 26 neighbours (one lane per neighbour)
+    if (newbits && lane < 27) {
+        // newly weighted sub-cubes: dilate by one sub-cube into this block
+        // position and its 26 neighbours (one lane per neighbour)
         const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
         const unsigned long long mk = dil_z(dil_y(dil_x(newbits, dx), dy), dz);
-        const unsigned long long mp = dil_z(dil_y(dil_x(newpos, dx), dy), dz);
-        const int nx = bx + dx, ny = by + dy, nz = bz + dz;
-        ulonglong2* cell = s.dmask + bidx_cell(nx, ny, nz, s.bidx_log2);
         if (mk) {
-            atomicOr(&cell->x, mk);
+            const int nx = bx + dx, ny = by + dy, nz = bz + dz;
+            atomicOr(s.dwm + bidx_cell(nx, ny, nz, s.bidx_log2), mk);
             const uint32_t q = grid_bit(nx >> 3, ny >> 3, nz >> 3, s.bidx_log2 - 3);
             atomicOr(s.sup + (q >> 5), 1u << (q & 31));
         }
-        if (mp) atomicOr(&cell->y, mp);
     }
     __syncwarp();
     if (lane == 0) {
@@ -736,11 +725,9 @@ static __device__ void integrate_block(const IntegArgs& a, int blk, unsigned lon
         const unsigned long long nw = ((unsigned long long)whi << 32) | wlo;
         if (fresh) {
             s.block_wmask[blk] = nw;
-            s.block_pmask[blk] = npm;
             s.block_fresh[blk] = 0;
-        } else {
-            if (nw) s.block_wmask[blk] |= nw;
-            if (newpos) s.block_pmask[blk] = old_pm | npm;
+        } else if (nw) {
+            s.block_wmask[blk] |= nw;
         }
     }
 }

@@ -75,6 +75,7 @@ struct Renderer {
     float2* bracket = nullptr;
     double* partials = nullptr;
     unsigned int* skipped = nullptr;
+    float step = 0.0f;  // march step in metres; 0 = the reference's half voxel
 };
 
 int scene_alloc_device(Scene* sc);

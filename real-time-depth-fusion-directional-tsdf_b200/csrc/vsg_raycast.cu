@@ -7,18 +7,11 @@
 // a sample's 8 taps lie in voxels floor(p/v)-1 .. floor(p/v)+2 per axis
 // (RayCastRender.cu:17-25, 127-170, with a voxel of slack for rounding), so
 // it can only be valid if a weighted voxel lies within one 2x2x2 sub-cube of
-// the sample's sub-cube.  The dmask grid holds that bit per sub-cube (.x,
-// one 64-bit word per block position), the sup grid one bit per 8^3 block
+// the sample's sub-cube.  The dwm grid holds that bit per sub-cube (one
+// 64-bit word per block position), the sup grid one bit per 8^3 block
 // positions.  Cells whose bit is clear are skipped whole:
-//   64-voxel cells (sup bit clear), 8-voxel cells (.x word zero),
-//   2-voxel cells (.x bit clear).
-// A zero crossing needs a sample with distance > 0 (RayCastRender.cu:321),
-// hence a tap with SDF > 0;
-// dmask.y holds, dilated the same way, the sub-cubes that have held such a
-// voxel.  In a cell without that bit (8-voxel cell: .y word zero; 2-voxel
-// cell: .y bit clear) no sample starts a crossing and the march state after
-// the cell's samples is that of the last one alone, so only the last sample
-// before the cell's far end is evaluated.
+//   64-voxel cells (sup bit clear), 8-voxel cells (dwm word zero),
+//   2-voxel cells (dwm bit clear).
 // Skipped runs are replayed in O(1) by vsg_chain_advance, which lands on the
 // exact float the serial additions produce.  Surviving samples take the full
 // trilinear interpolation (8 taps, blocks resolved through the dense block
@@ -116,6 +109,7 @@ int render_launch(Renderer* r, Scene* sc, const float cam[3], const float* pose_
     a.cy = cy;
     a.minD = min_depth;
     a.maxD = max_depth;
+    a.step = r->step;
     a.depth = r->depth;
     a.pos = r->position;
     a.col = r->color;

@@ -11,9 +11,6 @@
 namespace vsg {
 
 constexpr int kMaxMarch = 1 << 22;  // iteration guard of one ray
-// Shortest run (in march steps across the cell's remaining length) over which
-// a ray jumps to the run's last sample in a cell without positive voxels.
-constexpr float kMinPosRun = 4.0f;
 
 struct RenderArgs {
     SceneDev s;
@@ -23,6 +20,9 @@ struct RenderArgs {
     Pose pose;
     const float* pose_dev;
     float fx, fy, cx, cy, minD, maxD;
+    // march step (metres); 0: the reference's half voxel (RayCastRender.cu:
+    // 389-392).  Any other value is an opt-in approximation, not the drop-in.
+    float step;
     float* depth;
     float4* pos;
     float4* col;
@@ -169,7 +169,7 @@ static __device__ __forceinline__ bool trilinear(const SceneDev& s, float px, fl
         raw[i] = make_uint2(0u, 0u);
         if (tc.get(i) >= 0) {
             const int li = ((i & 1) ? lx1 : lx0) + ((i & 2) ? ly1 : ly0) + ((i & 4) ? lz1 : lz0);
-            raw[i] = VSG_LDG(reinterpret_cast<const uint2*>(s.voxels + (size_t)tc.get(i) * kVoxPerBlock + li));
+            raw[i] = __ldg(reinterpret_cast<const uint2*>(s.voxels + (size_t)tc.get(i) * kVoxPerBlock + li));
         }
     }
     float d = 0.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f, vws = 0.0f;
@@ -204,6 +204,7 @@ struct RayState {
     RayInv R;          // origin (the camera) and inverse direction
     float wdx, wdy, wdz;
     float d2r, rc, re;
+    float h;           // march step
     float lastSdf, lastAlpha;
     float ba, bad, bb, bbd, bc, mdist;
     TapCache tc;
@@ -226,7 +227,7 @@ static __device__ __forceinline__ bool march_enabled(const RenderArgs& a) {
 static __device__ __forceinline__ void load_pose(const RenderArgs& a, float T[12]) {
     if (a.pose_dev) {
 #pragma unroll
-        for (int i = 0; i < 12; ++i) T[i] = VSG_LDG(a.pose_dev + i);
+        for (int i = 0; i < 12; ++i) T[i] = __ldg(a.pose_dev + i);
     } else {
 #pragma unroll
         for (int i = 0; i < 12; ++i) T[i] = a.pose.T[i];
@@ -262,6 +263,7 @@ static __device__ __forceinline__ void ray_setup(const RenderArgs& a, const floa
     r.lastSdf = 0.0f;
     r.lastAlpha = 0.0f;
     r.lastValid = false;
+    r.h = a.step > 0.0f ? a.step : a.s.voxel * 0.5f;
     r.d2r = 1.0f / cdz;
     r.rc = r.d2r * fmaxf(a.minD, a.minD);
     r.re = r.d2r * fminf(a.maxD, a.maxD);
@@ -291,9 +293,9 @@ static __device__ __forceinline__ void ray_setup(const RenderArgs& a, const floa
 // exactly) or not taking it leaves the outputs as they are.  The margin
 // covers the rounding of the sample position cam + rc * dir.
 static __device__ __forceinline__ void apply_bounds(const RenderArgs& a, int x, int y, RayState& r) {
-    const uint2 b1 = VSG_LDG(a.bounds + (y >> 2) * a.t1x + (x >> 3));
-    const uint2 b2 = VSG_LDG(a.bounds + a.n1 + (y >> 5) * a.t2x + (x >> 6));
-    const uint2 bg = VSG_LDG(a.bounds + a.n1 + a.n2);
+    const uint2 b1 = __ldg(a.bounds + (y >> 2) * a.t1x + (x >> 3));
+    const uint2 b2 = __ldg(a.bounds + a.n1 + (y >> 5) * a.t2x + (x >> 6));
+    const uint2 bg = __ldg(a.bounds + a.n1 + a.n2);
     const uint32_t lo_inv = max(max(b1.x, b2.x), bg.x), hi_bits = max(max(b1.y, b2.y), bg.y);
     if (lo_inv == 0u) {  // no weighted block projects onto the tile
         r.re = r.rc;
@@ -306,7 +308,7 @@ static __device__ __forceinline__ void apply_bounds(const RenderArgs& a, int x, 
     r.re = fminf(r.re, last);
     if (first > r.rc && r.rc < r.re) {
         const int before = r.steps;
-        r.rc = vsg_chain_advance(r.rc, a.s.voxel * 0.5f, fminf(first, r.re), kMaxMarch - r.steps, &r.steps);
+        r.rc = vsg_chain_advance(r.rc, r.h, fminf(first, r.re), kMaxMarch - r.steps, &r.steps);
         r.n_skip += (uint32_t)(r.steps - before);
         ++r.n_jump;
     }
@@ -484,60 +486,32 @@ static __device__ __forceinline__ bool ray_step(const RenderArgs& a, RayState& r
         // global sub-cube (2 voxels) of the sample, its block cell and super-cell
         const int qx = __float2int_rd(spx * invC2), qy = __float2int_rd(spy * invC2), qz = __float2int_rd(spz * invC2);
         float tlo = 0.0f, thi = 0.0f;
-        bool cell = false;  // no sample in the cell can be valid
-        bool npos = false;  // no sample in the cell can read a positive SDF
+        bool cell = false;
         const int k = s.bidx_log2;
         const uint32_t sb = grid_bit(qx >> 5, qy >> 5, qz >> 5, k - 3);
-        if (!((VSG_LDG(s.sup + (sb >> 5)) >> (sb & 31)) & 1u)) {
+        if (!((__ldg(s.sup + (sb >> 5)) >> (sb & 31)) & 1u)) {
             cell_interval(r.R, qx >> 5, qy >> 5, qz >> 5, C8, tlo, thi);  // 64-voxel cell
             cell = true;
         } else {
-            const ulonglong2 w = VSG_LDG(s.dmask + bidx_cell(qx >> 2, qy >> 2, qz >> 2, k));
-            const int bit = ((((qz & 3) << 2) | (qy & 3)) << 2) | (qx & 3);
-            if (w.x == 0ull) {
+            const unsigned long long w = __ldg(s.dwm + bidx_cell(qx >> 2, qy >> 2, qz >> 2, k));
+            if (w == 0ull) {
                 cell_interval(r.R, qx >> 2, qy >> 2, qz >> 2, C, tlo, thi);  // 8-voxel cell
                 cell = true;
-            } else if (!((w.x >> bit) & 1ull)) {
+            } else if (!((w >> ((((qz & 3) << 2) | (qy & 3)) << 2 | (qx & 3))) & 1ull)) {
                 cell_interval(r.R, qx, qy, qz, C2, tlo, thi);  // 2-voxel cell
                 cell = true;
-            } else if (w.y == 0ull) {
-                cell_interval(r.R, qx >> 2, qy >> 2, qz >> 2, C, tlo, thi);  // 8-voxel cell
-                npos = true;
-            } else if (!((w.y >> bit) & 1ull)) {
-                cell_interval(r.R, qx, qy, qz, C2, tlo, thi);  // 2-voxel cell
-                npos = true;
             }
         }
         if (cell) {
             if (r.rc > tlo + m && r.rc < thi - m) {
                 const int before = r.steps;
-                r.rc = vsg_chain_advance(r.rc, v * 0.5f, fminf(thi - m, r.re), kMaxMarch - r.steps, &r.steps);
+                r.rc = vsg_chain_advance(r.rc, r.h, fminf(thi - m, r.re), kMaxMarch - r.steps, &r.steps);
                 r.n_skip += (uint32_t)(r.steps - before);
                 ++r.n_jump;
                 r.lastValid = false;
                 return false;
             }
             ++r.n_single;  // too close to the cell boundary to trust the test
-        } else if (npos) {
-            // Every sample of the cell reads only taps whose SDF is <= 0, so
-            // its distance is <= 0: none of them starts a zero crossing
-            // (lastSdf < 0 && dist > 0, RayCastRender.cu:321), and after a
-            // run of them the march state (lastValid, lastSdf, lastAlpha) is
-            // that of the run's last sample alone.  Replay the chain to the
-            // last sample before the cell's far end and evaluate only that
-            // one -- when the run is long enough for the replay to cost less
-            // than the samples it saves (short runs are sampled in turn).
-            const float end = fminf(thi - m, r.re);
-            if (r.rc > tlo + m && r.rc < thi - m) {
-                if (end - r.rc > kMinPosRun * (v * 0.5f)) {
-                    const int before = r.steps;
-                    r.rc = vsg_chain_advance_ex(r.rc, v * 0.5f, end, kMaxMarch - r.steps, &r.steps, 1);
-                    r.n_skip += (uint32_t)(r.steps - before);
-                    ++r.n_jump;
-                }
-            } else {
-                ++r.n_single;
-            }
         }
         st = r.rc;
     } else {
@@ -565,7 +539,7 @@ static __device__ __forceinline__ bool ray_step(const RenderArgs& a, RayState& r
             r.lastAlpha = r.rc;
         }
         r.lastValid = ok;
-        r.rc += v * 0.5f;
+        r.rc += r.h;
         ++r.steps;
         return false;
     }
@@ -601,7 +575,7 @@ static __device__ __forceinline__ bool ray_step(const RenderArgs& a, RayState& r
         r.lastSdf = r.mdist;
         r.lastAlpha = r.rc;
         r.lastValid = true;
-        r.rc += v * 0.5f;
+        r.rc += r.h;
         ++r.steps;
         r.mode = 0;
     }

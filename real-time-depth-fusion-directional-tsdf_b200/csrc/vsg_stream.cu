@@ -145,7 +145,6 @@ __global__ void k_stream_extract(SceneDev s, const uint32_t* list, uint32_t n, i
             }
             s.block_key[b] = kKeyEmpty;
             s.block_wmask[b] = 0ull;
-            s.block_pmask[b] = 0ull;
             s.block_fresh[b] = 0;
             const int j = atomicAdd(&s.ctr->free_count, 1);
             s.heap[j] = b;
@@ -172,8 +171,8 @@ __device__ int lookup_block_fresh(const SceneDev& s, unsigned long long key, int
 }
 
 // One warp per incoming block: insert (or find) its position, write or merge
-// its voxels, then maintain the sub-cube weight and positive masks and the
-// ray-march skip grid exactly as integration does (streamInHashAllocKernel +
+// its voxels, then maintain the sub-cube weight mask and the ray-march skip
+// grid exactly as integration does (streamInHashAllocKernel +
 // streamInHashInitKernel, VoxelStreamingManager.cu:443-714).
 __global__ void k_stream_insert(SceneDev s, const int4* info, const Voxel* in, uint32_t n, StreamCounters* c) {
     const int lane = threadIdx.x & 31;
@@ -203,8 +202,7 @@ __global__ void k_stream_insert(SceneDev s, const int4* info, const Voxel* in, u
         Voxel* vb = s.voxels + (size_t)ptr * kVoxPerBlock;
         const Voxel* src = in + (size_t)i * kVoxPerBlock;
         const unsigned long long old_wm = merged ? s.block_wmask[ptr] : 0ull;
-        const unsigned long long old_pm = merged ? s.block_pmask[ptr] : 0ull;
-        unsigned long long wm = 0ull, pm = 0ull;
+        unsigned long long wm = 0ull;
         const int lx = lane & 7;
 #pragma unroll 4
         for (int k = 0; k < 16; ++k) {
@@ -214,36 +212,26 @@ __global__ void k_stream_insert(SceneDev s, const int4* info, const Voxel* in, u
             vb[idx] = v;
             if (v.rgbw >> 24) {
                 const int ly = (lane >> 3) + ((k & 1) << 2), lz = k >> 1;
-                const unsigned long long bit = 1ull << ((((lz >> 1) * 4 + (ly >> 1)) * 4) + (lx >> 1));
-                wm |= bit;
-                if (!(v.sdf <= 0.0f)) pm |= bit;
+                wm |= 1ull << ((((lz >> 1) * 4 + (ly >> 1)) * 4) + (lx >> 1));
             }
         }
         const unsigned wlo = __reduce_or_sync(0xFFFFFFFFu, (unsigned)wm);
         const unsigned whi = __reduce_or_sync(0xFFFFFFFFu, (unsigned)(wm >> 32));
-        const unsigned plo = __reduce_or_sync(0xFFFFFFFFu, (unsigned)pm);
-        const unsigned phi = __reduce_or_sync(0xFFFFFFFFu, (unsigned)(pm >> 32));
         const unsigned long long nw = ((unsigned long long)whi << 32) | wlo;
-        const unsigned long long npm = ((unsigned long long)phi << 32) | plo;
         const unsigned long long newbits = nw & ~old_wm;
-        const unsigned long long newpos = npm & ~old_pm;
-        if ((newbits | newpos) && lane < 27) {
+        if (newbits && lane < 27) {
             const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
             const unsigned long long mk = dil_z(dil_y(dil_x(newbits, dx), dy), dz);
-            const unsigned long long mp = dil_z(dil_y(dil_x(newpos, dx), dy), dz);
-            const int nx = d.x + dx, ny = d.y + dy, nz = d.z + dz;
-            ulonglong2* cell = s.dmask + bidx_cell(nx, ny, nz, s.bidx_log2);
             if (mk) {
-                atomicOr(&cell->x, mk);
+                const int nx = d.x + dx, ny = d.y + dy, nz = d.z + dz;
+                atomicOr(s.dwm + bidx_cell(nx, ny, nz, s.bidx_log2), mk);
                 const uint32_t q = grid_bit(nx >> 3, ny >> 3, nz >> 3, s.bidx_log2 - 3);
                 atomicOr(s.sup + (q >> 5), 1u << (q & 31));
             }
-            if (mp) atomicOr(&cell->y, mp);
         }
         __syncwarp();
         if (lane == 0) {
             s.block_wmask[ptr] = old_wm | nw;
-            s.block_pmask[ptr] = old_pm | npm;
             s.block_fresh[ptr] = 0;
             if (merged) atomicAdd(&c->merged, 1u);
         }

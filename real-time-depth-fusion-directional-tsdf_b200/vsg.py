@@ -35,7 +35,7 @@ EXPORTS = [
     "vsg_store_load", "vsg_store_count", "vsg_store_add_records", "vsg_stream_out", "vsg_stream_in", "vsg_scene_save", "vsg_scene_load",
     "vsg_points_create", "vsg_points_destroy", "vsg_extract_points", "vsg_points_count", "vsg_points_buffers",
     "vsg_points_download", "vsg_points_save_ply",
-    "vsg_renderer_record", "vsg_render_backward", "vsg_render_normals", "vsg_scene_lookup_blocks",
+    "vsg_renderer_record", "vsg_renderer_set_step", "vsg_render_backward", "vsg_render_normals", "vsg_scene_lookup_blocks",
     "vsg_depth_to_pointmap", "vsg_integrate_backward", "vsg_render_pose_normal_equations", "vsg_splat_points",
 ]
 
@@ -141,6 +141,7 @@ def lib() -> ctypes.CDLL:
         L.vsg_points_download.argtypes = [_P, _P, _P, _P, ctypes.POINTER(ctypes.c_int64)]
         L.vsg_points_save_ply.argtypes = [_P, ctypes.c_char_p]
         L.vsg_renderer_record.argtypes = [_P, _I]
+        L.vsg_renderer_set_step.argtypes = [_P, _F]
         _i64 = ctypes.c_int64
         L.vsg_splat_points.argtypes = [_P, _i64, _P, _i64, _P, _i64, _I, _I, _F, _F, _F, _F, _F, _F, _I, _P, _P, _P,
                                        _P, ctypes.POINTER(_i64), _P]
@@ -445,6 +446,62 @@ def refine_poses(scenes, renderers, targets, poses, intrinsics, min_depth, max_d
     return T, rms
 
 
+def tune_ray_step(scene, renderer, poses, intrinsics, min_depth, max_depth, truncation,
+                  factors=(0.5, 0.625, 0.75, 0.875, 1.0), tol: float = 1e-3, frac: float = 0.99, reps: int = 3):
+    """Autotune the opt-in march step (vsg_renderer_set_step) on sample poses:
+    for each step = factor x truncation, time the ray casts (CUDA events) and
+    compare their depths with the reference's half-voxel march at the same
+    poses.  Returns (chosen step -- the fastest whose depths stay within `tol`
+    metres of the exact ones on at least `frac` of the pixels both hit, with
+    hit/miss flips counted as misses; 0, the exact march, if none does -- and
+    per candidate {step, ms, frac_within_tol, max_err, rms_err, flips}).  The
+    renderer is left at the chosen step."""
+    import torch
+
+    fx, fy, cx, cy = intrinsics
+
+    def run(step):
+        renderer.set_step(step)
+        outs = []
+        for T in poses:
+            renderer.render(scene, T, fx, fy, cx, cy, min_depth, max_depth)
+            outs.append(renderer.depth_tensor().clone())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            for T in poses:
+                renderer.render(scene, T, fx, fy, cx, cy, min_depth, max_depth)
+        e1.record()
+        torch.cuda.synchronize()
+        return outs, e0.elapsed_time(e1) / (reps * len(poses))
+
+    exact, ms0 = run(0.0)
+    table = [{"step": 0.0, "ms": ms0, "frac_within_tol": 1.0, "max_err": 0.0, "rms_err": 0.0, "flips": 0}]
+    best, best_ms = 0.0, ms0
+    for f in factors:
+        step = float(f) * float(truncation)
+        outs, ms = run(step)
+        ok = tot = flips = 0
+        errs = []
+        for a, b in zip(exact, outs):
+            ha, hb = a < 1e9, b < 1e9
+            both = ha & hb
+            e = (a - b).abs()[both].double()
+            flips += int((ha != hb).sum())
+            ok += int((e <= tol).sum())
+            tot += int(ha.sum())
+            errs.append(e)
+        e = torch.cat(errs)
+        fr = ok / max(tot, 1)
+        row = {"step": step, "ms": ms, "frac_within_tol": fr, "max_err": float(e.max()) if e.numel() else 0.0,
+               "rms_err": float(e.pow(2).mean().sqrt()) if e.numel() else 0.0, "flips": flips}
+        table.append(row)
+        if fr >= frac and ms < best_ms:
+            best, best_ms = step, ms
+    renderer.set_step(best)
+    return best, table
+
+
 def stream_scenes(scenes, stores, centers, r_out: float, r_in: float, streams=None, max_threads: int = 8):
     """One streaming pass for several scenes at once, in the reference main
     loop's order (voxelSG.cpp:503-551): per scene, stream out every block
@@ -640,6 +697,12 @@ class Renderer:
         """Keep each pixel's march bracket in the following renders (needed
         by backward() and normals())."""
         check("vsg_renderer_record", self.L.vsg_renderer_record(self.h, int(enable)))
+
+    def set_step(self, step: float = 0.0):
+        """March step in metres (vsg_renderer_set_step).  0 keeps the
+        reference's half-voxel step and its depths bit for bit; a positive
+        step is an opt-in approximation (see tune_ray_step)."""
+        check("vsg_renderer_set_step", self.L.vsg_renderer_set_step(self.h, _F(step)))
 
     def backward(self, scene: "Scene", pose, fx, fy, cx, cy, grad_depth=None, grad_position=None, grad_sdf=None,
                  min_weight_sum: float = 0.0, stream=None):

@@ -12,24 +12,6 @@ float vsg_test_chain_advance(float r, float h, float target, int max_steps, int*
     return vsg_chain_advance(r, h, target, max_steps, steps);
 }
 
-float vsg_test_chain_last_below(float r, float h, float target, int max_steps, int* steps) {
-    *steps = 0;
-    return vsg_chain_advance_ex(r, h, target, max_steps, steps, 1);
-}
-
-/* reference: serial additions, stopping at the last value below target */
-float vsg_test_chain_serial_below(float r, float h, float target, int max_steps, int* steps) {
-    int n = 0;
-    while (r < target && n < max_steps) {
-        const float nr = r + h;
-        if (!(nr < target)) break;
-        r = nr;
-        ++n;
-    }
-    *steps = n;
-    return r;
-}
-
 /* reference: serial additions */
 float vsg_test_chain_serial(float r, float h, float target, int max_steps, int* steps) {
     int n = 0;

@@ -10,25 +10,20 @@ import pytest
 @pytest.fixture(scope="module")
 def L(hosttest_lib):
     lib = hosttest_lib
-    for f in (lib.vsg_test_chain_advance, lib.vsg_test_chain_serial, lib.vsg_test_chain_last_below,
-              lib.vsg_test_chain_serial_below):
+    for f in (lib.vsg_test_chain_advance, lib.vsg_test_chain_serial):
         f.restype = ctypes.c_float
         f.argtypes = [ctypes.c_float] * 3 + [ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     return lib
 
 
-def _both(L, r, h, tgt, ms, below=False):
+def _both(L, r, h, tgt, ms):
     s1, s2 = ctypes.c_int(), ctypes.c_int()
-    fa = L.vsg_test_chain_last_below if below else L.vsg_test_chain_advance
-    fb = L.vsg_test_chain_serial_below if below else L.vsg_test_chain_serial
-    a = fa(r, h, tgt, ms, ctypes.byref(s1))
-    b = fb(r, h, tgt, ms, ctypes.byref(s2))
+    a = L.vsg_test_chain_advance(r, h, tgt, ms, ctypes.byref(s1))
+    b = L.vsg_test_chain_serial(r, h, tgt, ms, ctypes.byref(s2))
     return np.float32(a), np.float32(b), s1.value, s2.value
 
 
-@pytest.mark.parametrize("below", [False, True])
-def test_random_chains_match_serial(L, below):
-    """below: the stop-one-short form, the last chain value under the target."""
+def test_random_chains_match_serial(L):
     rng = np.random.default_rng(1)
     for i in range(30000):
         v = np.float32(rng.choice([0.004, 0.002, 0.003, 0.005, 0.001, 0.0037, 0.01, 0.0123]))
@@ -36,21 +31,19 @@ def test_random_chains_match_serial(L, below):
         r = float(np.float32(rng.uniform(0.05, 4.0) if i % 3 else rng.uniform(1e-4, 0.3)))
         tgt = float(np.float32(r + rng.uniform(-0.01, 3.5)))
         ms = int(rng.integers(1, 3000)) if i % 4 == 0 else 1 << 22
-        a, b, s1, s2 = _both(L, r, h, tgt, ms, below)
+        a, b, s1, s2 = _both(L, r, h, tgt, ms)
         assert a.view(np.uint32) == b.view(np.uint32) and s1 == s2, (r, h, tgt, ms, a, b, s1, s2)
 
 
-@pytest.mark.parametrize("below", [False, True])
-def test_binade_boundaries_and_ties(L, below):
+def test_binade_boundaries_and_ties(L):
     # chains that start just below a power of two, and steps whose ulp count is
     # an exact half (ties to even)
     for r0 in (0.25, 0.5, 1.0, 2.0):
         for d in range(1, 40):
             r = float(np.nextafter(np.float32(r0), np.float32(0)) - np.float32(d * 1e-6))
             for h in (0.002, float(np.float32(2.0 ** -9)), float(np.float32(3 * 2.0 ** -25)), 1e-3):
-                for tgt in (r0 + 0.05, r0, float(np.nextafter(np.float32(r0), np.float32(1e9)))):
-                    a, b, s1, s2 = _both(L, r, h, tgt, 1 << 22, below)
-                    assert a.view(np.uint32) == b.view(np.uint32) and s1 == s2, (r, h, tgt)
+                a, b, s1, s2 = _both(L, r, h, r0 + 0.05, 1 << 22)
+                assert a.view(np.uint32) == b.view(np.uint32) and s1 == s2, (r, h)
 
 
 def test_no_progress_and_below_target(L):

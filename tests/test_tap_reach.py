@@ -41,13 +41,12 @@ def test_taps_lie_within_one_voxel_of_the_sample(voxel):
 
 @pytest.mark.parametrize("voxel", [0.0005, 0.002, 0.004, 0.01])
 def test_taps_lie_within_one_subcube_of_the_sample(voxel):
-    """The march's skip tests (dmask .x: a weighted voxel within one 2x2x2
-    sub-cube; .y: a positive voxel within one sub-cube) take the sample's
-    sub-cube as the kernel computes it, q = floor(RN(p * RN(1 / RN(2 v)))),
-    and read the bits dilated by one sub-cube.  Every tap voxel's sub-cube
-    is q - 1 .. q + 1, for every sample: the taps span 3 voxels, the
-    dilated range 6, and the voxel of slack on each side absorbs the
-    rounding of q at the sub-cube faces."""
+    """The march's skip test (dwm: a weighted voxel within one 2x2x2
+    sub-cube) takes the sample's sub-cube as the kernel computes it,
+    q = floor(RN(p * RN(1 / RN(2 v)))), and reads the bit dilated by one
+    sub-cube.  Every tap voxel's sub-cube is q - 1 .. q + 1, for every
+    sample: the taps span 3 voxels, the dilated range 6, and the voxel of
+    slack on each side absorbs the rounding of q at the sub-cube faces."""
     rng = np.random.default_rng(int(voxel * 1e5) + 1)
     v = np.float32(voxel)
     n = 1_000_000
