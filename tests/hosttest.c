@@ -51,3 +51,41 @@ long vsg_test_avg_div_mismatches(int d, int stride) {
     }
     return bad;
 }
+
+/* The smallest float D >= 0 with RN(sqrt(D)) >= w (the integration's
+ * squared-distance threshold, sqrt_threshold in the device header),
+ * restated with the C library's correctly rounded sqrtf: stepped from
+ * RN(w * w), else found by bisection over the float order. */
+static float bits_f(uint32_t u) {
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+static uint32_t f_bits(float f) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return u;
+}
+float vsg_test_sqrt_threshold(float w) {
+    float c;
+    int i, ok = 0;
+    if (!(w > 0.0f) || w == INFINITY) return w;
+    c = w * w;
+    if (w >= 0x1p-60f && w <= 0x1p60f) {
+        for (i = 0; i < 8 && sqrtf(c) < w; ++i) c = bits_f(f_bits(c) + 1u);
+        for (i = 0; i < 8 && c > 0.0f && sqrtf(bits_f(f_bits(c) - 1u)) >= w; ++i) c = bits_f(f_bits(c) - 1u);
+        ok = sqrtf(c) >= w && (c == 0.0f || sqrtf(bits_f(f_bits(c) - 1u)) < w);
+    }
+    if (!ok) {
+        uint32_t lo = 0u, hi = 0x7F800000u;
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2u;
+            if (sqrtf(bits_f(mid)) >= w)
+                hi = mid;
+            else
+                lo = mid + 1u;
+        }
+        c = bits_f(lo);
+    }
+    return c;
+}
