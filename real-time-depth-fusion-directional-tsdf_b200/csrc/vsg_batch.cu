@@ -105,12 +105,44 @@ __global__ void __launch_bounds__(256) k_batch_tile_bounds(const BatchHeader* h,
     tile_bounds_range(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
+// The ray-cast tiles of every scene of the step in one order, longest march
+// range first (tile_bucket): one CTA, bucket counts in shared memory, then a
+// scatter of the tiles' step-wide indices.
+__global__ void __launch_bounds__(1024) k_batch_tile_order(const BatchHeader* h, const RenderArgs* args,
+                                                           uint32_t* order) {
+    __shared__ unsigned hist[kOrderBuckets], next[kOrderBuckets];
+    const uint32_t n = h->render_prefix[h->n];
+    if (threadIdx.x < kOrderBuckets) hist[threadIdx.x] = 0u;
+    __syncthreads();
+    for (uint32_t g = threadIdx.x; g < n; g += blockDim.x) {
+        const int i = scene_of(h->render_prefix, h->n, g);
+        const uint32_t t = g - h->render_prefix[i], tx = (uint32_t)h->render_tiles_x[i];
+        atomicAdd(&hist[tile_bucket(args[i], (int)(t % tx), (int)(t / tx))], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned s = 0;
+        for (int b = kOrderBuckets - 1; b >= 0; --b) {  // heaviest bucket first
+            next[b] = s;
+            s += hist[b];
+        }
+    }
+    __syncthreads();
+    for (uint32_t g = threadIdx.x; g < n; g += blockDim.x) {
+        const int i = scene_of(h->render_prefix, h->n, g);
+        const uint32_t t = g - h->render_prefix[i], tx = (uint32_t)h->render_tiles_x[i];
+        order[atomicAdd(&next[tile_bucket(args[i], (int)(t % tx), (int)(t / tx))], 1u)] = g;
+    }
+}
+
 template <int kMinBlocks>
-__global__ void __launch_bounds__(128, kMinBlocks) k_batch_render(const BatchHeader* h, const RenderArgs* args) {
-    const int i = scene_of(h->render_prefix, h->n, blockIdx.x);
+__global__ void __launch_bounds__(128, kMinBlocks) k_batch_render(const BatchHeader* h, const RenderArgs* args,
+                                                                  const uint32_t* __restrict__ order) {
+    const uint32_t g = __ldg(order + blockIdx.x);
+    const int i = scene_of(h->render_prefix, h->n, g);
     const RenderArgs& a = args[i];
     if (a.W <= 0) return;  // scene not ray cast this step
-    const uint32_t t = blockIdx.x - h->render_prefix[i];
+    const uint32_t t = g - h->render_prefix[i];
     const int tx = (int)(t % (uint32_t)h->render_tiles_x[i]), ty = (int)(t / (uint32_t)h->render_tiles_x[i]);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = tx * kRenderTileW + (warp & 1) * 8 + (lane & 7);
@@ -125,6 +157,8 @@ struct Batch {
     std::vector<Scene*> scenes;
     std::vector<Renderer*> renderers;
     unsigned char* d_step = nullptr;     // device copy of the step's argument blocks
+    uint32_t* d_order = nullptr;         // ray-cast tile order of a step (k_batch_tile_order)
+    uint32_t order_cap = 0;              // ray-cast tiles of all renderers together
     unsigned char* h_step[2] = {};       // pinned staging, alternate steps
     cudaEvent_t done[2] = {};            // last step that read h_step[i] finished
     bool pending[2] = {false, false};
@@ -138,13 +172,14 @@ struct Batch {
     std::map<std::vector<int>, Shape> shapes;
 };
 
-static void launch_render_variant(int v, dim3 grid, cudaStream_t st, const BatchHeader* h, const RenderArgs* r) {
+static void launch_render_variant(int v, dim3 grid, cudaStream_t st, const BatchHeader* h, const RenderArgs* r,
+                                  const uint32_t* order) {
     if (v == 1)
-        k_batch_render<4><<<grid, 128, 0, st>>>(h, r);
+        k_batch_render<4><<<grid, 128, 0, st>>>(h, r, order);
     else if (v == 2)
-        k_batch_render<8><<<grid, 128, 0, st>>>(h, r);
+        k_batch_render<8><<<grid, 128, 0, st>>>(h, r, order);
     else
-        k_batch_render<6><<<grid, 128, 0, st>>>(h, r);
+        k_batch_render<6><<<grid, 128, 0, st>>>(h, r, order);
 }
 
 }  // namespace vsg
@@ -165,6 +200,7 @@ static void enqueue_bounds(Batch& b, int n, cudaStream_t st) {
     const int bnd_x = std::max(2, (b.sm_count * 4) / n);
     k_batch_bounds_clear<<<dim3(bnd_x, n), 256, 0, st>>>(h, ra);
     k_batch_tile_bounds<<<dim3(bnd_x, n), 256, 0, st>>>(h, ra);
+    k_batch_tile_order<<<1, 1024, 0, st>>>(h, ra, b.d_order);
 }
 
 // Enqueue the stages of one step (argument blocks already on the device).
@@ -183,7 +219,7 @@ static void enqueue_stages(Batch& b, int n, uint32_t alloc_tiles, uint32_t rende
     k_batch_integrate<<<dim3(integ_x, n), 256, 0, st>>>(h, ia);
     if (render_tiles) {
         enqueue_bounds(b, n, st);
-        launch_render_variant(render_variant, dim3(render_tiles), st, h, ra);
+        launch_render_variant(render_variant, dim3(render_tiles), st, h, ra, b.d_order);
     }
 }
 
@@ -211,13 +247,18 @@ int vsg_batch_create(vsg_scene* const* scenes, vsg_renderer* const* renderers, i
             B.scenes.push_back(&scenes[i]->impl);
             B.renderers.push_back(renderers ? (renderers[i] ? &renderers[i]->impl : nullptr) : nullptr);
         }
+        for (const vsg::Renderer* r : B.renderers)
+            if (r) B.order_cap += (uint32_t)(((r->w + vsg::kRenderTileW - 1) / vsg::kRenderTileW) *
+                                             ((r->h + vsg::kRenderTileH - 1) / vsg::kRenderTileH));
         B.step_bytes = vsg::layout_for(vsg::kMaxBatch).bytes;
-        bool ok = cudaMalloc(&B.d_step, B.step_bytes) == cudaSuccess;
+        bool ok = cudaMalloc(&B.d_step, B.step_bytes) == cudaSuccess &&
+                  cudaMalloc(&B.d_order, sizeof(uint32_t) * std::max<uint32_t>(B.order_cap, 1u)) == cudaSuccess;
         for (int i = 0; i < 2 && ok; ++i)
             ok = cudaMallocHost(&B.h_step[i], B.step_bytes) == cudaSuccess &&
                  cudaEventCreateWithFlags(&B.done[i], cudaEventDisableTiming) == cudaSuccess;
         if (!ok) {
             cudaFree(B.d_step);
+            cudaFree(B.d_order);
             for (int i = 0; i < 2; ++i) {
                 if (B.h_step[i]) cudaFreeHost(B.h_step[i]);
                 if (B.done[i]) cudaEventDestroy(B.done[i]);
@@ -238,6 +279,7 @@ int vsg_batch_destroy(vsg_batch* b) {
         for (int i = 0; i < 2; ++i)
             if (kv.second.exec[i]) cudaGraphExecDestroy(kv.second.exec[i]);
     cudaFree(b->impl.d_step);
+    cudaFree(b->impl.d_order);
     for (int i = 0; i < 2; ++i) {
         cudaFreeHost(b->impl.h_step[i]);
         cudaEventDestroy(b->impl.done[i]);
@@ -386,7 +428,7 @@ int vsg_batch_step(vsg_batch* b, const vsg_batch_frame* frames, int n_frames, vs
                     cudaEventCreate(&e1);
                     for (int v = 0; v < 3; ++v) {
                         cudaEventRecord(e0, st);
-                        launch_render_variant(v, dim3(rt), st, dh, dr);
+                        launch_render_variant(v, dim3(rt), st, dh, dr, B.d_order);
                         cudaEventRecord(e1, st);
                         cudaEventSynchronize(e1);
                         float ms = 0.0f;
@@ -399,7 +441,7 @@ int vsg_batch_step(vsg_batch* b, const vsg_batch_frame* frames, int n_frames, vs
                     cudaEventDestroy(e0);
                     cudaEventDestroy(e1);
                 } else {
-                    launch_render_variant(0, dim3(rt), st, dh, dr);
+                    launch_render_variant(0, dim3(rt), st, dh, dr, B.d_order);
                 }
             }
             shape.render_variant = best;

@@ -284,7 +284,9 @@ int vsg_renderer_create(int w, int h, vsg_renderer** out) {
     const size_t nb = (size_t)((w + 7) / 8) * ((h + 3) / 4) + (size_t)((w + 63) / 64) * ((h + 31) / 32) + 1;
     if (cudaMalloc(&R.depth, n * sizeof(float)) != cudaSuccess || cudaMalloc(&R.position, n * sizeof(float4)) != cudaSuccess ||
         cudaMalloc(&R.color, n * sizeof(float4)) != cudaSuccess || cudaMalloc(&R.normal, n * sizeof(float4)) != cudaSuccess ||
-        cudaMalloc(&R.bounds, nb * sizeof(uint2)) != cudaSuccess) {
+        cudaMalloc(&R.bounds, nb * sizeof(uint2)) != cudaSuccess ||
+        cudaMalloc(&R.tile_order, (size_t)((w + 15) / 16) * ((h + 7) / 8) * sizeof(uint32_t)) != cudaSuccess) {
+        cudaFree(R.tile_order);
         cudaFree(R.depth);
         cudaFree(R.position);
         cudaFree(R.color);
@@ -305,6 +307,7 @@ int vsg_renderer_destroy(vsg_renderer* r) {
     cudaFree(r->impl.color);
     cudaFree(r->impl.normal);
     cudaFree(r->impl.bounds);
+    cudaFree(r->impl.tile_order);
     cudaFree(r->impl.bracket);
     cudaFree(r->impl.partials);
     cudaFree(r->impl.skipped);

@@ -68,6 +68,7 @@ struct Renderer {
     float4* color = nullptr;
     float4* normal = nullptr;
     uint2* bounds = nullptr;  // march distance bounds per pixel tile (k_tile_bounds)
+    uint32_t* tile_order = nullptr;  // ray-cast CTA tiles, longest march range first (k_tile_order)
     int sm_count = 148;
     // adjoint support (vsg_renderer_record): march brackets, per-CTA pose
     // gradient partials, skipped-pixel counter

@@ -30,13 +30,35 @@
 
 namespace vsg {
 
-// One thread per pixel; a CTA covers 16x8 pixels as four 8x4 warp tiles.
-__global__ void __launch_bounds__(128, 6) k_render(RenderArgs a) {
+// One thread per pixel; a CTA covers 16x8 pixels as four 8x4 warp tiles, the
+// CTAs taking the tiles in the order k_tile_order wrote (longest march range
+// first).
+__global__ void __launch_bounds__(128, 6) k_render(RenderArgs a, const uint32_t* __restrict__ order, int gx) {
+    const uint32_t t = __ldg(order + blockIdx.x);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int x = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
-    const int y = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
+    const int x = (int)(t % (uint32_t)gx) * 16 + (warp & 1) * 8 + (lane & 7);
+    const int y = (int)(t / (uint32_t)gx) * 8 + (warp >> 1) * 4 + (lane >> 3);
     if (x >= a.W || y >= a.H) return;
     render_pixel(a, x, y);
+}
+
+// Ray-cast tile order, longest march first (tile_bucket); one CTA: bucket
+// counts in shared memory, then a scatter.
+__global__ void __launch_bounds__(1024) k_tile_order(RenderArgs a, uint32_t* order, int gx, int n) {
+    __shared__ unsigned hist[kOrderBuckets], next[kOrderBuckets];
+    if (threadIdx.x < kOrderBuckets) hist[threadIdx.x] = 0u;
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) atomicAdd(&hist[tile_bucket(a, t % gx, t / gx)], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned s = 0;
+        for (int b = kOrderBuckets - 1; b >= 0; --b) {  // heaviest bucket first
+            next[b] = s;
+            s += hist[b];
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) order[atomicAdd(&next[tile_bucket(a, t % gx, t / gx)], 1u)] = (uint32_t)t;
 }
 
 // The ray-distance bounds of one render (tile_bounds_range), one thread per
@@ -123,11 +145,12 @@ int render_launch(Renderer* r, Scene* sc, const float cam[3], const float* pose_
     a.bounds = r->bounds;
     if (a.touched) cudaMemsetAsync(a.touched, 0, (size_t)sc->dev.num_blocks, st);
     k_render_begin<<<1, 1, 0, st>>>(sc->dev.frame);
-    dim3 grid((r->w + 15) / 16, (r->h + 7) / 8);
+    const int gx = (r->w + 15) / 16, ntiles = gx * ((r->h + 7) / 8);
     timing_begin(sc, kSlotRender, st);
     cudaMemsetAsync(r->bounds, 0, sizeof(uint2) * (size_t)(a.n1 + a.n2 + 1), st);
     k_tile_bounds<<<sc->sm_count * 4, 256, 0, st>>>(a);
-    k_render<<<grid, 128, 0, st>>>(a);
+    k_tile_order<<<1, 1024, 0, st>>>(a, r->tile_order, gx, ntiles);
+    k_render<<<ntiles, 128, 0, st>>>(a, r->tile_order, gx);
     timing_end(sc, kSlotRender, st);
     if (a.touched) k_count_touched<<<sc->sm_count * 2, 256, 0, st>>>(a.touched, sc->dev.ctr, sc->dev.frame);
     return cudaGetLastError() == cudaSuccess ? VSG_OK : VSG_ERR_CUDA;

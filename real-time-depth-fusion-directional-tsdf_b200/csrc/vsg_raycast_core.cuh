@@ -466,6 +466,35 @@ static __device__ __forceinline__ void tile_bounds_range(const RenderArgs& a, ui
     }
 }
 
+// Ray-cast tile order, longest march first.  A CTA tile of 16x8 pixels
+// holds four 8x4 bound tiles; its weight is the largest distance range
+// [nearest, farthest] its rays may march (apply_bounds), bucketed by powers
+// of two of march steps.  The tiles with the longest ranges are cast first,
+// so the last wave of the launch holds short ones instead of a long tail.
+// Each pixel's result does not depend on the order.
+constexpr int kOrderBuckets = 16;
+
+static __device__ __forceinline__ int tile_bucket(const RenderArgs& a, int tx, int ty) {
+    const int t1y = a.n1 / a.t1x;
+    const uint2 bg = __ldg(a.bounds + a.n1 + a.n2);
+    float cost = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int x8 = 2 * tx + (k & 1), y4 = 2 * ty + (k >> 1);
+        if (x8 >= a.t1x || y4 >= t1y) continue;
+        const uint2 b1 = __ldg(a.bounds + y4 * a.t1x + x8);
+        const uint2 b2 = __ldg(a.bounds + a.n1 + (y4 >> 3) * a.t2x + (x8 >> 3));
+        const uint32_t lo_inv = max(max(b1.x, b2.x), bg.x), hi_bits = max(max(b1.y, b2.y), bg.y);
+        if (lo_inv == 0u) continue;
+        cost = fmaxf(cost, __uint_as_float(hi_bits) - __uint_as_float(~lo_inv));
+    }
+    if (!(cost > 0.0f)) return 0;
+    const float steps = cost / (0.5f * a.s.voxel);
+    if (!(steps < 3.0e38f)) return kOrderBuckets - 1;
+    const int e = (int)((__float_as_uint(fmaxf(steps, 1.0f)) >> 23) & 0xFFu) - 127;  // floor(log2(steps))
+    return 1 + min(max(e, 0), kOrderBuckets - 2);
+}
+
 // One iteration of the march: a skip jump, a march sample or a
 // regula-falsi sample.  Returns true when the ray is done.
 static __device__ __forceinline__ bool ray_step(const RenderArgs& a, RayState& r, size_t pi) {
