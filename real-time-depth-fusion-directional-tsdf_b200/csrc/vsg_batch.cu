@@ -82,9 +82,37 @@ __global__ void __launch_bounds__(256) k_batch_select(const BatchHeader* h, cons
     select_blocks(args[blockIdx.y], blockIdx.x * blockDim.x, gridDim.x * blockDim.x);
 }
 
-__global__ void __launch_bounds__(256, 4) k_batch_integrate(const BatchHeader* h, const IntegArgs* args) {
-    if ((int)blockIdx.y >= h->n) return;
-    integrate_work(args[blockIdx.y]);
+// Integration of every scene's visible blocks as one work queue: a prefix of
+// the scenes' visible counts (written by the selection), then every warp of
+// the launch takes the next (scene, visible block) from one counter, so no
+// scene's blocks wait on a fixed share of the GPU while other scenes' share
+// sits idle.  Each visible block is integrated by exactly one warp, as in
+// integrate_work.
+__global__ void k_batch_visible_prefix(const BatchHeader* h, const IntegArgs* args, uint32_t* queue) {
+    if (threadIdx.x != 0) return;
+    uint32_t s = 0;
+    for (int i = 0; i < h->n; ++i) {
+        queue[i] = s;
+        s += *(volatile uint32_t*)&args[i].s.frame->n_visible;
+    }
+    queue[h->n] = s;
+    queue[kMaxBatch + 1] = 0u;  // the work counter
+}
+
+__global__ void __launch_bounds__(256, 4) k_batch_integrate(const BatchHeader* h, const IntegArgs* args,
+                                                           uint32_t* queue) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t total = queue[h->n];
+    for (;;) {
+        uint32_t g = 0;
+        if (lane == 0) g = atomicAdd(queue + kMaxBatch + 1, 1u);
+        g = __shfl_sync(0xFFFFFFFFu, g, 0);
+        if (g >= total) break;
+        const int i = scene_of(queue, h->n, g);
+        const IntegArgs& a = args[i];
+        const uint32_t b = a.s.visible[g - queue[i]];
+        integrate_block(a, (int)b, a.s.block_key[b], a.s.block_fresh[b] != 0, lane);
+    }
 }
 
 // The ray-distance bounds of every scene ray cast this step: cleared, then
@@ -158,6 +186,8 @@ struct Batch {
     std::vector<Renderer*> renderers;
     unsigned char* d_step = nullptr;     // device copy of the step's argument blocks
     uint32_t* d_order = nullptr;         // ray-cast tile order of a step (k_batch_tile_order)
+    uint32_t* d_queue = nullptr;         // integration queue: visible-count prefix, then the work counter
+    int integ_ctas_per_sm = 4;           // resident CTAs of k_batch_integrate
     uint32_t order_cap = 0;              // ray-cast tiles of all renderers together
     unsigned char* h_step[2] = {};       // pinned staging, alternate steps
     cudaEvent_t done[2] = {};            // last step that read h_step[i] finished
@@ -215,8 +245,8 @@ static void enqueue_stages(Batch& b, int n, uint32_t alloc_tiles, uint32_t rende
     if (alloc_tiles) k_batch_alloc<<<alloc_tiles, kTile * kTile, 0, st>>>(h, aa);
     const int sel_x = std::max(2, (b.sm_count * 8) / n);
     k_batch_select<<<dim3(sel_x, n), 256, 0, st>>>(h, ia);
-    const int integ_x = std::max(2, (b.sm_count * 4) / n);
-    k_batch_integrate<<<dim3(integ_x, n), 256, 0, st>>>(h, ia);
+    k_batch_visible_prefix<<<1, 32, 0, st>>>(h, ia, b.d_queue);
+    k_batch_integrate<<<b.sm_count * b.integ_ctas_per_sm, 256, 0, st>>>(h, ia, b.d_queue);
     if (render_tiles) {
         enqueue_bounds(b, n, st);
         launch_render_variant(render_variant, dim3(render_tiles), st, h, ra, b.d_order);
@@ -251,14 +281,19 @@ int vsg_batch_create(vsg_scene* const* scenes, vsg_renderer* const* renderers, i
             if (r) B.order_cap += (uint32_t)(((r->w + vsg::kRenderTileW - 1) / vsg::kRenderTileW) *
                                              ((r->h + vsg::kRenderTileH - 1) / vsg::kRenderTileH));
         B.step_bytes = vsg::layout_for(vsg::kMaxBatch).bytes;
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vsg::k_batch_integrate, 256, 0);
+        B.integ_ctas_per_sm = per_sm > 0 ? per_sm : 4;
         bool ok = cudaMalloc(&B.d_step, B.step_bytes) == cudaSuccess &&
-                  cudaMalloc(&B.d_order, sizeof(uint32_t) * std::max<uint32_t>(B.order_cap, 1u)) == cudaSuccess;
+                  cudaMalloc(&B.d_order, sizeof(uint32_t) * std::max<uint32_t>(B.order_cap, 1u)) == cudaSuccess &&
+                  cudaMalloc(&B.d_queue, sizeof(uint32_t) * (vsg::kMaxBatch + 2)) == cudaSuccess;
         for (int i = 0; i < 2 && ok; ++i)
             ok = cudaMallocHost(&B.h_step[i], B.step_bytes) == cudaSuccess &&
                  cudaEventCreateWithFlags(&B.done[i], cudaEventDisableTiming) == cudaSuccess;
         if (!ok) {
             cudaFree(B.d_step);
             cudaFree(B.d_order);
+            cudaFree(B.d_queue);
             for (int i = 0; i < 2; ++i) {
                 if (B.h_step[i]) cudaFreeHost(B.h_step[i]);
                 if (B.done[i]) cudaEventDestroy(B.done[i]);
@@ -280,6 +315,7 @@ int vsg_batch_destroy(vsg_batch* b) {
             if (kv.second.exec[i]) cudaGraphExecDestroy(kv.second.exec[i]);
     cudaFree(b->impl.d_step);
     cudaFree(b->impl.d_order);
+    cudaFree(b->impl.d_queue);
     for (int i = 0; i < 2; ++i) {
         cudaFreeHost(b->impl.h_step[i]);
         cudaEventDestroy(b->impl.done[i]);
