@@ -134,32 +134,41 @@ __global__ void __launch_bounds__(256) k_batch_tile_bounds(const BatchHeader* h,
 }
 
 // The ray-cast tiles of every scene of the step in one order, longest march
-// range first (tile_bucket): one CTA, bucket counts in shared memory, then a
-// scatter of the tiles' step-wide indices.
-__global__ void __launch_bounds__(1024) k_batch_tile_order(const BatchHeader* h, const RenderArgs* args,
-                                                           uint32_t* order) {
-    __shared__ unsigned hist[kOrderBuckets], next[kOrderBuckets];
-    const uint32_t n = h->render_prefix[h->n];
+// range first (tile_bucket), as for one scene (k_tile_hist, k_tile_scatter)
+// over the tiles' step-wide indices.  The grid covers the largest step
+// (all renderers); counts (16 counts, 16 cursors) is zeroed before.
+__global__ void __launch_bounds__(256) k_batch_tile_hist(const BatchHeader* h, const RenderArgs* args,
+                                                         unsigned* counts) {
+    __shared__ unsigned hist[kOrderBuckets];
     if (threadIdx.x < kOrderBuckets) hist[threadIdx.x] = 0u;
     __syncthreads();
-    for (uint32_t g = threadIdx.x; g < n; g += blockDim.x) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < h->render_prefix[h->n]) {
         const int i = scene_of(h->render_prefix, h->n, g);
         const uint32_t t = g - h->render_prefix[i], tx = (uint32_t)h->render_tiles_x[i];
         atomicAdd(&hist[tile_bucket(args[i], (int)(t % tx), (int)(t / tx))], 1u);
     }
     __syncthreads();
+    if (threadIdx.x < kOrderBuckets && hist[threadIdx.x]) atomicAdd(counts + threadIdx.x, hist[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(256) k_batch_tile_scatter(const BatchHeader* h, const RenderArgs* args,
+                                                            uint32_t* order, unsigned* counts) {
+    __shared__ unsigned start[kOrderBuckets];
     if (threadIdx.x == 0) {
         unsigned s = 0;
         for (int b = kOrderBuckets - 1; b >= 0; --b) {  // heaviest bucket first
-            next[b] = s;
-            s += hist[b];
+            start[b] = s;
+            s += counts[b];
         }
     }
     __syncthreads();
-    for (uint32_t g = threadIdx.x; g < n; g += blockDim.x) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < h->render_prefix[h->n]) {
         const int i = scene_of(h->render_prefix, h->n, g);
         const uint32_t t = g - h->render_prefix[i], tx = (uint32_t)h->render_tiles_x[i];
-        order[atomicAdd(&next[tile_bucket(args[i], (int)(t % tx), (int)(t / tx))], 1u)] = g;
+        const int b = tile_bucket(args[i], (int)(t % tx), (int)(t / tx));
+        order[start[b] + atomicAdd(counts + kOrderBuckets + b, 1u)] = g;
     }
 }
 
@@ -185,7 +194,7 @@ struct Batch {
     std::vector<Scene*> scenes;
     std::vector<Renderer*> renderers;
     unsigned char* d_step = nullptr;     // device copy of the step's argument blocks
-    uint32_t* d_order = nullptr;         // ray-cast tile order of a step (k_batch_tile_order)
+    uint32_t* d_order = nullptr;         // ray-cast tile order of a step, then 32 counters
     uint32_t* d_queue = nullptr;         // integration queue: visible-count prefix, then the work counter
     int integ_ctas_per_sm = 4;           // resident CTAs of k_batch_integrate
     uint32_t order_cap = 0;              // ray-cast tiles of all renderers together
@@ -230,7 +239,11 @@ static void enqueue_bounds(Batch& b, int n, cudaStream_t st) {
     const int bnd_x = std::max(2, (b.sm_count * 4) / n);
     k_batch_bounds_clear<<<dim3(bnd_x, n), 256, 0, st>>>(h, ra);
     k_batch_tile_bounds<<<dim3(bnd_x, n), 256, 0, st>>>(h, ra);
-    k_batch_tile_order<<<1, 1024, 0, st>>>(h, ra, b.d_order);
+    unsigned* counts = b.d_order + b.order_cap;
+    const unsigned grid = std::max(1u, (b.order_cap + 255) / 256);
+    cudaMemsetAsync(counts, 0, 2 * kOrderBuckets * sizeof(unsigned), st);
+    k_batch_tile_hist<<<grid, 256, 0, st>>>(h, ra, counts);
+    k_batch_tile_scatter<<<grid, 256, 0, st>>>(h, ra, b.d_order, counts);
 }
 
 // Enqueue the stages of one step (argument blocks already on the device).
@@ -285,7 +298,7 @@ int vsg_batch_create(vsg_scene* const* scenes, vsg_renderer* const* renderers, i
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vsg::k_batch_integrate, 256, 0);
         B.integ_ctas_per_sm = per_sm > 0 ? per_sm : 4;
         bool ok = cudaMalloc(&B.d_step, B.step_bytes) == cudaSuccess &&
-                  cudaMalloc(&B.d_order, sizeof(uint32_t) * std::max<uint32_t>(B.order_cap, 1u)) == cudaSuccess &&
+                  cudaMalloc(&B.d_order, sizeof(uint32_t) * (B.order_cap + 32)) == cudaSuccess &&
                   cudaMalloc(&B.d_queue, sizeof(uint32_t) * (vsg::kMaxBatch + 2)) == cudaSuccess;
         for (int i = 0; i < 2 && ok; ++i)
             ok = cudaMallocHost(&B.h_step[i], B.step_bytes) == cudaSuccess &&
