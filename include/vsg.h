@@ -491,8 +491,8 @@ typedef struct vsg_batch_frame {
 VSG_API int vsg_batch_create(vsg_scene* const* scenes, vsg_renderer* const* renderers, int n, vsg_batch** out);
 VSG_API int vsg_batch_destroy(vsg_batch* b);
 /* Each scene at most once per step.  The first step of a new shape runs
- * eagerly (and, with autotuning on, times three ray-cast launch variants on
- * its own data) and captures the graph; later steps replay it. */
+ * eagerly (and, with autotuning on, times five ray-cast launch variants, 4
+ * to 8 resident CTAs per SM, on its own data) and captures the graph; later steps replay it. */
 VSG_API int vsg_batch_step(vsg_batch* b, const vsg_batch_frame* frames, int n_frames, vsg_stream_t stream);
 VSG_API int vsg_batch_autotune(vsg_batch* b, int enable);
 

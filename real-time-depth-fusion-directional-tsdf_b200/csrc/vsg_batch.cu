@@ -10,8 +10,8 @@
 // the per-scene device code (vsg_fusion_core.cuh, vsg_raycast_core.cuh), so
 // every scene's results are identical to vsg_integrate + vsg_render.
 //
-// Autotuning: the ray-cast stage exists in three register budgets (CTAs per
-// SM 4, 6, 8); vsg_batch_step with autotune on times each on the step's own
+// Autotuning: the ray-cast stage exists in five register budgets (CTAs per
+// SM 4 to 8); vsg_batch_step with autotune on times each on the step's own
 // data (ray casting does not modify the scene, so repeating it is harmless)
 // and keeps the fastest for the batch's shape.
 #include <cuda_runtime.h>
@@ -206,7 +206,7 @@ struct Batch {
     bool autotune = true;
     struct Shape {
         cudaGraphExec_t exec[2] = {nullptr, nullptr};  // one per staging buffer
-        int render_variant = -1;  // 0: 6 CTAs/SM, 1: 4, 2: 8; -1 = not tuned yet
+        int render_variant = -1;  // 0: 6 CTAs/SM, 1: 4, 2: 8, 3: 5, 4: 7; -1 = not tuned yet
     };
     std::map<std::vector<int>, Shape> shapes;
 };
@@ -217,6 +217,10 @@ static void launch_render_variant(int v, dim3 grid, cudaStream_t st, const Batch
         k_batch_render<4><<<grid, 128, 0, st>>>(h, r, order);
     else if (v == 2)
         k_batch_render<8><<<grid, 128, 0, st>>>(h, r, order);
+    else if (v == 3)
+        k_batch_render<5><<<grid, 128, 0, st>>>(h, r, order);
+    else if (v == 4)
+        k_batch_render<7><<<grid, 128, 0, st>>>(h, r, order);
     else
         k_batch_render<6><<<grid, 128, 0, st>>>(h, r, order);
 }
@@ -475,7 +479,7 @@ int vsg_batch_step(vsg_batch* b, const vsg_batch_frame* frames, int n_frames, vs
                     cudaEvent_t e0, e1;
                     cudaEventCreate(&e0);
                     cudaEventCreate(&e1);
-                    for (int v = 0; v < 3; ++v) {
+                    for (int v = 0; v < 5; ++v) {
                         cudaEventRecord(e0, st);
                         launch_render_variant(v, dim3(rt), st, dh, dr, B.d_order);
                         cudaEventRecord(e1, st);
