@@ -43,6 +43,14 @@ VSG_HD float vsg_u2f(uint32_t u) {
 #endif
 }
 
+// An estimate of x / y for the step count, corrected by exact integer
+// comparisons afterwards, so its last bits do not matter.
+#ifdef __CUDA_ARCH__
+#define VSG_QUOT_EST(x, y) __fdividef((x), (y))
+#else
+#define VSG_QUOT_EST(x, y) ((x) / (y))
+#endif
+
 // 2^k for -126 <= k <= 127
 VSG_HD float vsg_pow2(int k) { return vsg_u2f((uint32_t)(k + 127) << 23); }
 
@@ -84,8 +92,6 @@ VSG_HD float vsg_chain_advance(float r, float h, float target, int max_steps, in
             break;
         }
         const int R = (int)(bits & 0x7FFFFFu) | 0x800000;  // r / u
-        // steps that keep R + k D <= 2^24 - 2 (strictly inside the binade)
-        const int kmax = (0xFFFFFE - R) / D;
         // steps needed to reach target: smallest k >= 1 with R + k D >= T
         const float T = target * vsg_pow2(23 - e);  // exact scaling
         int kneed;
@@ -93,18 +99,21 @@ VSG_HD float vsg_chain_advance(float r, float h, float target, int max_steps, in
             kneed = 0x7FFFFFFF;
         } else {
             const float need = T - (float)R;  // an estimate; corrected below
-            kneed = (int)ceilf(need / (float)D);
+            kneed = (int)ceilf(VSG_QUOT_EST(need, (float)D));
             if (kneed < 1) kneed = 1;
             // correct the float estimate with exact integer comparisons
             while (kneed > 1 && (float)(R + (kneed - 1) * D) >= T) --kneed;
             while ((float)(R + kneed * D) < T) ++kneed;
         }
         const int room = max_steps - taken;
-        if (kneed <= kmax && kneed <= room) {
+        // R + kneed D <= 2^24 - 2: the kneed steps stay strictly inside the binade
+        if (kneed <= room && (long long)R + (long long)kneed * D <= 0xFFFFFE) {
             r = (float)(R + kneed * D) * vsg_pow2(e - 23);
             taken += kneed;
             break;
         }
+        // steps that keep R + k D <= 2^24 - 2
+        const int kmax = (0xFFFFFE - R) / D;
         int k = kmax < room ? kmax : room;
         if (k > 0) {
             r = (float)(R + k * D) * vsg_pow2(e - 23);

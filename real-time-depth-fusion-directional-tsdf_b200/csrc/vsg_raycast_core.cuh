@@ -86,6 +86,40 @@ static __device__ __forceinline__ float div_v(float x, float v, float y, bool fa
     return x / v;
 }
 
+// lookup_block for the ray caster, out of line: the dense block index
+// resolves almost every tap block, and keeping the rare bucket search out of
+// the march loop keeps the loop's code small.
+static __device__ __noinline__ int lookup_far(const Entry* buckets, const int* bucket_next, const Node* nodes,
+                                              uint32_t nb, int max_nodes, int x, int y, int z) {
+    const unsigned long long key = pack_key(x, y, z);
+    const uint32_t b = bucket_of(x, y, z, nb);
+    const Entry* bk = buckets + (size_t)b * kBucketSlots;
+#pragma unroll
+    for (int j = 0; j < kBucketSlots; ++j) {
+        const uint4 e = __ldg(reinterpret_cast<const uint4*>(bk + j));
+        const unsigned long long k = ((unsigned long long)e.y << 32) | e.x;
+        if (k == key) return (int)e.z;
+        if (k == kKeyEmpty) return -1;
+    }
+    int n = __ldg(bucket_next + b);
+    for (int it = 0; n >= 0 && it < max_nodes; ++it) {
+        const uint4 e = __ldg(reinterpret_cast<const uint4*>(nodes + n));
+        const unsigned long long k = ((unsigned long long)e.y << 32) | e.x;
+        if (k == key) return (int)e.z;
+        n = (int)e.w;
+    }
+    return -1;
+}
+
+// block_ptr with the bucket search out of line
+static __device__ __forceinline__ int block_ptr_r(const SceneDev& s, int x, int y, int z) {
+    if (!coord_ok(x, y, z)) return -1;
+    const unsigned long long e = __ldg(s.bindex + bidx_cell(x, y, z, s.bidx_log2));
+    if (e == kIdxEmpty) return -1;
+    if (e == kIdxShared) return lookup_far(s.buckets, s.bucket_next, s.nodes, s.num_buckets, s.max_nodes, x, y, z);
+    return ((e >> 22) == bidx_tag(x, y, z, s.bidx_log2)) ? (int)(e & kIdxPtrMask) : -1;
+}
+
 // getVoxel's block search (RayCastRender.cu:55-121) for the taps' blocks;
 // -1 = block not allocated (the tap reads as weight 0).
 static __device__ __forceinline__ void refill_taps(const SceneDev& s, TapCache& tc, int bx0, int by0, int bz0, int span,
@@ -99,7 +133,7 @@ static __device__ __forceinline__ void refill_taps(const SceneDev& s, TapCache& 
         const int c = i & span;
         if (c == i) {
             const int bx = bx0 + (i & 1), by = by0 + ((i >> 1) & 1), bz = bz0 + ((i >> 2) & 1);
-            const int p = block_ptr(s, bx, by, bz);
+            const int p = block_ptr_r(s, bx, by, bz);
             if (touched && p >= 0) touched[p] = 1;
             tc.set(i, p);
         } else {
@@ -152,11 +186,31 @@ static __device__ __forceinline__ bool trilinear(const SceneDev& s, float px, fl
     const float dx = px - off / 2.0f, dy = py - off / 2.0f, dz = pz - off / 2.0f;
     const bool fast = s.div_fast;
     const float y = s.inv_voxel;
-    const float fx = div_v(dx, v, y, fast), fy = div_v(dy, v, y, fast), fz = div_v(dz, v, y, fast);
+    // the six quotients (sample and sample + one voxel, per axis) take the
+    // verified fixed-divisor path together when all six dividends are in its
+    // range (one test instead of six divergent ones), else one by one
+    const float ex = dx + off, ey = dy + off, ez = dz + off;
+    const float mn = fminf(fminf(fminf(fabsf(dx), fabsf(dy)), fminf(fabsf(dz), fabsf(ex))), fminf(fabsf(ey), fabsf(ez)));
+    const float mx = fmaxf(fmaxf(fmaxf(fabsf(dx), fabsf(dy)), fmaxf(fabsf(dz), fabsf(ex))), fmaxf(fabsf(ey), fabsf(ez)));
+    float fx, fy, fz, gx, gy, gz;
+    if (fast && mn >= kDivTiny && mx < kDivRange) {
+        fx = div_fixed(dx, v, y);
+        fy = div_fixed(dy, v, y);
+        fz = div_fixed(dz, v, y);
+        gx = div_fixed(ex, v, y);
+        gy = div_fixed(ey, v, y);
+        gz = div_fixed(ez, v, y);
+    } else {
+        fx = div_v(dx, v, y, fast);
+        fy = div_v(dy, v, y, fast);
+        fz = div_v(dz, v, y, fast);
+        gx = div_v(ex, v, y, fast);
+        gy = div_v(ey, v, y, fast);
+        gz = div_v(ez, v, y, fast);
+    }
     const float wx = frac01(fx), wy = frac01(fy), wz = frac01(fz);
     const int ax0 = tap_voxel(fx), ay0 = tap_voxel(fy), az0 = tap_voxel(fz);
-    const int ax1 = tap_voxel(div_v(dx + off, v, y, fast)), ay1 = tap_voxel(div_v(dy + off, v, y, fast)),
-              az1 = tap_voxel(div_v(dz + off, v, y, fast));
+    const int ax1 = tap_voxel(gx), ay1 = tap_voxel(gy), az1 = tap_voxel(gz);
     const int bx0 = vox_to_block(ax0), by0 = vox_to_block(ay0), bz0 = vox_to_block(az0);
     const int span = (vox_to_block(ax1) != bx0 ? 1 : 0) | (vox_to_block(ay1) != by0 ? 2 : 0) |
                      (vox_to_block(az1) != bz0 ? 4 : 0);
@@ -518,23 +572,42 @@ static __device__ __forceinline__ bool ray_step(const RenderArgs& a, RayState& r
         bool cell = false;
         const int k = s.bidx_log2;
         const uint32_t sb = grid_bit(qx >> 5, qy >> 5, qz >> 5, k - 3);
-        if (!((__ldg(s.sup + (sb >> 5)) >> (sb & 31)) & 1u)) {
-            cell_interval(r.R, qx >> 5, qy >> 5, qz >> 5, C8, tlo, thi);  // 64-voxel cell
-            cell = true;
+        // Both grid words are loaded together (the dwm word is read even when
+        // the super-cell is empty; every index is inside the grid), and the
+        // empty cell, if any, goes through one cell_interval for all three
+        // sizes, so lanes at different levels do not run separate copies.
+        int sh = -1;  // the empty cell: 64-voxel (5), 8-voxel (2), 2-voxel (0), none (-1)
+        const uint32_t supw = __ldg(s.sup + (sb >> 5));
+        const unsigned long long w = __ldg(s.dwm + bidx_cell(qx >> 2, qy >> 2, qz >> 2, k));
+        if (!((supw >> (sb & 31)) & 1u)) {
+            sh = 5;
+        } else if (w == 0ull) {
+            sh = 2;
         } else {
-            const unsigned long long w = __ldg(s.dwm + bidx_cell(qx >> 2, qy >> 2, qz >> 2, k));
-            if (w == 0ull) {
-                cell_interval(r.R, qx >> 2, qy >> 2, qz >> 2, C, tlo, thi);  // 8-voxel cell
-                cell = true;
-            } else if (!((w >> ((((qz & 3) << 2) | (qy & 3)) << 2 | (qx & 3))) & 1ull)) {
-                cell_interval(r.R, qx, qy, qz, C2, tlo, thi);  // 2-voxel cell
-                cell = true;
-            }
+            if (!((w >> ((((qz & 3) << 2) | (qy & 3)) << 2 | (qx & 3))) & 1ull))
+                sh = 0;
+        }
+        if (sh >= 0) {
+            cell_interval(r.R, qx >> sh, qy >> sh, qz >> sh, sh == 5 ? C8 : (sh == 2 ? C : C2), tlo, thi);
+            cell = true;
         }
         if (cell) {
             if (r.rc > tlo + m && r.rc < thi - m) {
+                // the march's own additions for a short skip (up to 8 steps,
+                // exact by construction and cheaper than the O(1) replay),
+                // vsg_chain_advance for the rest of a longer one
                 const int before = r.steps;
-                r.rc = vsg_chain_advance(r.rc, r.h, fminf(thi - m, r.re), kMaxMarch - r.steps, &r.steps);
+                const float tgt = fminf(thi - m, r.re);
+                float rc = r.rc;
+                int n = 0;
+#pragma unroll 1
+                while (rc < tgt && n < 8 && r.steps + n < kMaxMarch) {
+                    rc = rc + r.h;
+                    ++n;
+                }
+                r.steps += n;
+                if (rc < tgt) rc = vsg_chain_advance(rc, r.h, tgt, kMaxMarch - r.steps, &r.steps);
+                r.rc = rc;
                 r.n_skip += (uint32_t)(r.steps - before);
                 ++r.n_jump;
                 r.lastValid = false;
