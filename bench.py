@@ -315,16 +315,16 @@ def run_ours(args):
             sc.integrate(pm, rgb, nm, W, H, TRUNC, T, K.fx, K.fy, K.cx, K.cy)
             rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
 
-    # per-frame statistics (algorithmic bytes), outside the timed region; the
-    # instrumented mode also counts the distinct blocks each render reads
-    sc.timing(True)
+    # per-frame statistics (algorithmic bytes), outside the timed region; with
+    # march statistics on, renders also count the distinct blocks they read
+    sc.march_stats(True)
     sc.reset()
     per_frame = []
     for pm, rgb, nm, T in dev:
         sc.integrate(pm, rgb, nm, W, H, TRUNC, T, K.fx, K.fy, K.cx, K.cy)
         rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, MAX_D)
         per_frame.append(sc.stats())
-    sc.timing(False)
+    sc.march_stats(False)
     sc.timing_reset()
     for _ in range(args.warmup):
         step()
@@ -734,14 +734,14 @@ def room_measure(peak: float, n_frames: int = 300, reps: int = 2, mc_every: int 
                 if mc_counts is not None:
                     mc_counts.append(mc.count())
 
-    sc.timing(True)
+    sc.march_stats(True)
     sc.reset()
     per = []
     for pm, rgb, nm, T in frames:
         sc.integrate(pm, rgb, nm, W, H, 0.01, T, K.fx, K.fy, K.cx, K.cy)
         rr.render(sc, T, K.fx, K.fy, K.cx, K.cy, MIN_D, 4.0)
         per.append(sc.stats())
-    sc.timing(False)
+    sc.march_stats(False)
     step()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

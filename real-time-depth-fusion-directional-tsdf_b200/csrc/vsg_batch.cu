@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_batch_render(const BatchHea
     const int x = tx * kRenderTileW + (warp & 1) * 8 + (lane & 7);
     const int y = ty * kRenderTileH + (warp >> 1) * 4 + (lane >> 3);
     if (x >= a.W || y >= a.H) return;
-    render_pixel(a, x, y);
+    render_pixel<false>(a, x, y);
 }
 
 struct Batch {

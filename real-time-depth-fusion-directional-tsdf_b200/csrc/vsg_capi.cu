@@ -411,6 +411,12 @@ int vsg_timing_enable(vsg_scene* s, int enable) {
     return VSG_OK;
 }
 
+int vsg_scene_march_stats(vsg_scene* s, int enable) {
+    if (!s) return VSG_ERR_INVALID_ARG;
+    s->impl.march_stats = enable != 0;
+    return VSG_OK;
+}
+
 int vsg_timing_read(vsg_scene* s, double* ms, uint32_t* counts, int n_slots) {
     if (!s || !ms || !counts || n_slots <= 0) return VSG_ERR_INVALID_ARG;
     vsg::timing_drain(&s->impl);

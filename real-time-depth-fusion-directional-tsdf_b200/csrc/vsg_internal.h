@@ -57,6 +57,7 @@ struct Scene {
     int integ_ctas_per_sm = 2;
     uint32_t integrated_frames = 0;
     Timing timing;
+    bool march_stats = false;  // renders count skips, boundary samples and blocks read
     void* stream_stage = nullptr;  // staging buffers of vsg_stream_* (created on first use)
 };
 

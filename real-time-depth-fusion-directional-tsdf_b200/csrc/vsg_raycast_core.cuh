@@ -346,6 +346,7 @@ static __device__ __forceinline__ void ray_setup(const RenderArgs& a, const floa
 // sample outside that range is invalid, so skipping it (the chain replayed
 // exactly) or not taking it leaves the outputs as they are.  The margin
 // covers the rounding of the sample position cam + rc * dir.
+template <bool kCountSkips>
 static __device__ __forceinline__ void apply_bounds(const RenderArgs& a, int x, int y, RayState& r) {
     const uint2 b1 = __ldg(a.bounds + (y >> 2) * a.t1x + (x >> 3));
     const uint2 b2 = __ldg(a.bounds + a.n1 + (y >> 5) * a.t2x + (x >> 6));
@@ -363,7 +364,7 @@ static __device__ __forceinline__ void apply_bounds(const RenderArgs& a, int x, 
     if (first > r.rc && r.rc < r.re) {
         const int before = r.steps;
         r.rc = vsg_chain_advance(r.rc, r.h, fminf(first, r.re), kMaxMarch - r.steps, &r.steps);
-        r.n_skip += (uint32_t)(r.steps - before);
+        if (kCountSkips) r.n_skip += (uint32_t)(r.steps - before);
         ++r.n_jump;
     }
 }
@@ -551,6 +552,7 @@ static __device__ __forceinline__ int tile_bucket(const RenderArgs& a, int tx, i
 
 // One iteration of the march: a skip jump, a march sample or a
 // regula-falsi sample.  Returns true when the ray is done.
+template <bool kCountSkips>
 static __device__ __forceinline__ bool ray_step(const RenderArgs& a, RayState& r, size_t pi) {
     const SceneDev& s = a.s;
     const float v = s.voxel;
@@ -608,12 +610,12 @@ static __device__ __forceinline__ bool ray_step(const RenderArgs& a, RayState& r
                 r.steps += n;
                 if (rc < tgt) rc = vsg_chain_advance(rc, r.h, tgt, kMaxMarch - r.steps, &r.steps);
                 r.rc = rc;
-                r.n_skip += (uint32_t)(r.steps - before);
+                if (kCountSkips) r.n_skip += (uint32_t)(r.steps - before);
                 ++r.n_jump;
                 r.lastValid = false;
                 return false;
             }
-            ++r.n_single;  // too close to the cell boundary to trust the test
+            if (kCountSkips) ++r.n_single;  // too close to the cell boundary to trust the test
         }
         st = r.rc;
     } else {
@@ -718,7 +720,12 @@ static __device__ __forceinline__ void add_stats(const SceneDev& s, unsigned am,
 }
 
 // One ray: pixel (x, y) of the scene in a (in the image).  Warps should
-// cover 8x4 pixel tiles of one scene.
+// cover 8x4 pixel tiles of one scene.  kCountSkips: also count the samples
+// skipped as empty and the samples taken at a skip-cell boundary (the
+// render_samples_skipped / render_singles statistics).  Those two counters
+// cost about 10 % of the march (registers and instructions in the jump path
+// of every iteration), so the kernels count them only in instrumented runs.
+template <bool kCountSkips>
 static __device__ __forceinline__ void render_pixel(const RenderArgs& a, int x, int y) {
     const SceneDev& s = a.s;
     // numActiveBlocks == 0 leaves the outputs untouched (RayCastRender.cu:552-555)
@@ -729,9 +736,9 @@ static __device__ __forceinline__ void render_pixel(const RenderArgs& a, int x, 
     RayState r;
     ray_setup(a, T, x, y, r);
     if (march_enabled(a)) {
-        if (a.bounds) apply_bounds(a, x, y, r);
+        if (a.bounds) apply_bounds<kCountSkips>(a, x, y, r);
 #pragma unroll 1
-        while (!ray_step(a, r, pi)) {
+        while (!ray_step<kCountSkips>(a, r, pi)) {
         }
         const unsigned am = __activemask();
         const uint32_t it = r.n_full + r.n_jump;

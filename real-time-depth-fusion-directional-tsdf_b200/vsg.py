@@ -27,7 +27,7 @@ EXPORTS = [
     "vsg_integrate", "vsg_integrate_noalloc", "vsg_scene_set_alloc_method", "vsg_scene_stats", "vsg_scene_export", "vsg_renderer_create", "vsg_renderer_destroy",
     "vsg_render", "vsg_render_hostpose", "vsg_renderer_outputs", "vsg_renderer_download",
     "vsg_renderer_save_ply",
-    "vsg_timing_enable", "vsg_timing_read", "vsg_timing_reset", "vsg_version",
+    "vsg_timing_enable", "vsg_timing_read", "vsg_timing_reset", "vsg_scene_march_stats", "vsg_version",
     "vsg_batch_create", "vsg_batch_destroy", "vsg_batch_step", "vsg_batch_autotune",
     "vsg_mc_output_create", "vsg_mc_output_destroy", "vsg_mc_run", "vsg_mc_triangle_count",
     "vsg_mc_output_buffers", "vsg_mc_download",
@@ -106,6 +106,7 @@ def lib() -> ctypes.CDLL:
         L.vsg_renderer_outputs.argtypes = [_P] + [ctypes.POINTER(_P)] * 4
         L.vsg_renderer_download.argtypes = [_P, _P, _P, _P, _P]
         L.vsg_timing_enable.argtypes = [_P, _I]
+        L.vsg_scene_march_stats.argtypes = [_P, _I]
         L.vsg_timing_read.argtypes = [_P, _P, _P, _I]
         L.vsg_timing_reset.argtypes = [_P]
         L.vsg_batch_create.argtypes = [_P, _P, _I, ctypes.POINTER(_P)]
@@ -648,6 +649,12 @@ class Scene:
 
     def timing(self, enable: bool):
         check("vsg_timing_enable", self.L.vsg_timing_enable(self.h, int(enable)))
+
+    def march_stats(self, enable: bool):
+        """Count skipped samples, boundary samples and distinct blocks read in
+        the following renders (stats() render_samples_skipped, render_singles,
+        render_blocks_read); the counting ray caster is about 10 % slower."""
+        check("vsg_scene_march_stats", self.L.vsg_scene_march_stats(self.h, int(enable)))
 
     def timing_read(self) -> tuple[np.ndarray, np.ndarray]:
         ms = np.zeros(8, np.float64)
