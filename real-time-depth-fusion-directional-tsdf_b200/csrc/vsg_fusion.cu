@@ -138,7 +138,11 @@ int scene_alloc_device(Scene* sc) {
     VSG_MALLOC(d.buckets, S * kBucketSlots * sizeof(Entry));
     VSG_MALLOC(d.bucket_next, S * sizeof(int));
     VSG_MALLOC(d.nodes, M * sizeof(Node));
-    VSG_MALLOC(d.voxels, B * kVoxPerBlock * sizeof(Voxel));
+    // one block more than the pool: block B stays all zero (weight 0) and
+    // stands for "not allocated" in the ray caster's tap cache, so its tap
+    // loads need no test
+    VSG_MALLOC(d.voxels, (B + 1) * kVoxPerBlock * sizeof(Voxel));
+    if (cudaMemset(d.voxels + B * kVoxPerBlock, 0, kVoxPerBlock * sizeof(Voxel)) != cudaSuccess) return VSG_ERR_CUDA;
     VSG_MALLOC(d.block_key, B * sizeof(unsigned long long));
     VSG_MALLOC(d.block_slot, B * sizeof(int));
     VSG_MALLOC(d.block_fresh, B);

@@ -38,7 +38,8 @@ struct RenderArgs {
 // Pool indices of the blocks holding a sample's 8 trilinear taps.  The taps
 // of one sample span at most two blocks per axis (tap voxels x0 <= x1 <=
 // x0 + 2); tp[i] is the block of tap i.  Consecutive samples mostly reuse
-// the same blocks, so the entry is kept across samples.
+// the same blocks, so the entry is kept across samples.  Unallocated blocks
+// are entered as the pool's zero block (index num_blocks).
 struct TapCache {
     int bx, by, bz, span;
     int t0, t1, t2, t3, t4, t5, t6, t7;
@@ -120,8 +121,9 @@ static __device__ __forceinline__ int block_ptr_r(const SceneDev& s, int x, int 
     return ((e >> 22) == bidx_tag(x, y, z, s.bidx_log2)) ? (int)(e & kIdxPtrMask) : -1;
 }
 
-// getVoxel's block search (RayCastRender.cu:55-121) for the taps' blocks;
-// -1 = block not allocated (the tap reads as weight 0).
+// getVoxel's block search (RayCastRender.cu:55-121) for the taps' blocks; a
+// block that is not allocated is entered as num_blocks, the all-zero block
+// past the pool (its taps read as weight 0).
 static __device__ __forceinline__ void refill_taps(const SceneDev& s, TapCache& tc, int bx0, int by0, int bz0, int span,
                                             uint8_t* touched) {
     tc.bx = bx0;
@@ -135,7 +137,7 @@ static __device__ __forceinline__ void refill_taps(const SceneDev& s, TapCache& 
             const int bx = bx0 + (i & 1), by = by0 + ((i >> 1) & 1), bz = bz0 + ((i >> 2) & 1);
             const int p = block_ptr_r(s, bx, by, bz);
             if (touched && p >= 0) touched[p] = 1;
-            tc.set(i, p);
+            tc.set(i, p >= 0 ? p : s.num_blocks);  // the zero block past the pool
         } else {
             int p = tc.t0;
 #pragma unroll
@@ -220,8 +222,7 @@ static __device__ __forceinline__ bool trilinear(const SceneDev& s, float px, fl
     uint2 raw[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        raw[i] = make_uint2(0u, 0u);
-        if (tc.get(i) >= 0) {
+        {  // an unallocated tap block reads the pool's zero block (weight 0)
             const int li = ((i & 1) ? lx1 : lx0) + ((i & 2) ? ly1 : ly0) + ((i & 4) ? lz1 : lz0);
             raw[i] = __ldg(reinterpret_cast<const uint2*>(s.voxels + (size_t)tc.get(i) * kVoxPerBlock + li));
         }
