@@ -566,7 +566,10 @@ static __device__ __forceinline__ bool ray_step(const RenderArgs& a, RayState& r
             return true;
         }
         const float C = (float)kBlock * v, C2 = 2.0f * v, C8 = 64.0f * v;
-        const float invC2 = 1.0f / C2;
+        // RN(1 / (2 v)) = RN(1 / v) / 2 exactly (halving a normal float is exact);
+        // the batched caster reads the voxel size from memory, where the
+        // division would not leave the loop
+        const float invC2 = 0.5f * s.inv_voxel;
         const float m = 1e-4f;  // keep skipped samples this far inside their cell
         const float spx = ox + r.rc * r.wdx, spy = oy + r.rc * r.wdy, spz = oz + r.rc * r.wdz;
         // global sub-cube (2 voxels) of the sample, its block cell and super-cell
