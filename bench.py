@@ -344,9 +344,9 @@ def run_ours(args):
         import shard
 
         ms = shard.max_over_ranks(ms, dist)
-    # per step: reset (3 kernels) + per frame: frame_begin, alloc, select, integrate, render_begin,
-    # tile_bounds, render
-    launches_per_step = 3 + len(dev) * 7
+    # per step: reset (k_init_heap, k_init_counters, k_frame_begin) + per frame: k_frame_begin,
+    # k_alloc, k_select, k_integrate, k_render_begin, k_tile_bounds, k_tile_order, k_render
+    launches_per_step = 3 + len(dev) * 8
     # per-kernel times (separate pass with events around each launch)
     sc.timing(True)
     sc.timing_reset()
