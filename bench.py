@@ -91,6 +91,13 @@ class ClockSampler:
             self.thr.start()
         except OSError:
             self.proc = None
+        # nvidia-smi takes longer to start than a short timed region lasts:
+        # wait (at most 5 s) until it prints its first row, taken before the
+        # region with the GPU idle, and keep only the rows after it
+        t0 = time.monotonic()
+        while self.proc and not self.rows and self.proc.poll() is None and time.monotonic() - t0 < 5.0:
+            time.sleep(0.01)
+        self.first = len(self.rows)
         return self
 
     def _read(self):
@@ -101,6 +108,11 @@ class ClockSampler:
 
     def __exit__(self, *a):
         if self.proc:
+            # a region shorter than the 100 ms sampling interval may end
+            # before its first row: wait (at most 0.3 s) for one
+            t0 = time.monotonic()
+            while len(self.rows) <= self.first and self.proc.poll() is None and time.monotonic() - t0 < 0.3:
+                time.sleep(0.005)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -108,14 +120,15 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self) -> dict:
-        if not self.rows:
+        rows = self.rows[getattr(self, "first", 0):]
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].strip() == "Active"})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i].strip() == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(rows)}
 
 
 def measured_peak_hbm() -> tuple[float, str]:
