@@ -643,6 +643,8 @@ extern "C" {
 int vsg_renderer_record(vsg_renderer* rh, int enable) {
     if (!rh) return VSG_ERR_INVALID_ARG;
     vsg::Renderer& r = rh->impl;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != r.device) return VSG_ERR_INVALID_ARG;  // buffers go on r's device
     if (enable && !r.bracket) {
         const size_t n = (size_t)r.w * r.h;
         const size_t ctas = (size_t)((r.w + 15) / 16) * ((r.h + 7) / 8);
@@ -685,6 +687,8 @@ int vsg_render_backward(const vsg_renderer* rh, const vsg_scene* s, const float 
 
 int vsg_scene_lookup_blocks(const vsg_scene* s, const int32_t* coords, uint32_t n, int32_t* ptrs) {
     if (!s || (n && (!coords || !ptrs))) return VSG_ERR_INVALID_ARG;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != s->impl.device) return VSG_ERR_INVALID_ARG;
     if (n == 0) return VSG_OK;
     int* d = nullptr;
     if (cudaMalloc(&d, (size_t)n * 4 * sizeof(int)) != cudaSuccess) return VSG_ERR_OUT_OF_MEMORY;

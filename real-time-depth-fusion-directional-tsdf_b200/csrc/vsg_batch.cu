@@ -291,6 +291,10 @@ int vsg_batch_create(vsg_scene* const* scenes, vsg_renderer* const* renderers, i
                 delete b;
                 return VSG_ERR_INVALID_ARG;
             }
+            if (renderers && renderers[i] && renderers[i]->impl.device != B.device) {
+                delete b;
+                return VSG_ERR_INVALID_ARG;
+            }
             B.scenes.push_back(&scenes[i]->impl);
             B.renderers.push_back(renderers ? (renderers[i] ? &renderers[i]->impl : nullptr) : nullptr);
         }

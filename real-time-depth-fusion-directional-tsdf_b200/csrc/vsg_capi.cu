@@ -190,6 +190,8 @@ int vsg_scene_set_alloc_method(vsg_scene* s, int method) {
 
 int vsg_scene_stats(vsg_scene* s, vsg_stats* out) {
     if (!s || !out) return VSG_ERR_INVALID_ARG;
+    // the synchronisation below waits for the current device only
+    if (!on_device(s->impl.device)) return VSG_ERR_INVALID_ARG;
     if (cudaDeviceSynchronize() != cudaSuccess) return VSG_ERR_CUDA;
     vsg::SceneCounters c;
     vsg::FrameCounters f;
@@ -231,6 +233,7 @@ int vsg_scene_stats(vsg_scene* s, vsg_stats* out) {
 int vsg_scene_export(vsg_scene* s, int32_t* coords, uint8_t* voxels, uint32_t max_blocks, uint32_t* n_out) {
     return vsg::host_guard([&]() -> int {
         if (!s || !coords || !n_out) return VSG_ERR_INVALID_ARG;
+        if (!on_device(s->impl.device)) return VSG_ERR_INVALID_ARG;
         if (cudaDeviceSynchronize() != cudaSuccess) return VSG_ERR_CUDA;
         vsg::SceneCounters c;
         if (cudaMemcpy(&c, s->impl.dev.ctr, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return VSG_ERR_CUDA;
@@ -351,6 +354,7 @@ int vsg_renderer_outputs(const vsg_renderer* r, float** depth, float** position,
 
 int vsg_renderer_download(const vsg_renderer* r, float* depth, float* position, float* color, float* normal) {
     if (!r) return VSG_ERR_INVALID_ARG;
+    if (!on_device(r->impl.device)) return VSG_ERR_INVALID_ARG;
     const size_t n = (size_t)r->impl.w * r->impl.h;
     if (cudaDeviceSynchronize() != cudaSuccess) return VSG_ERR_CUDA;
     if (depth && cudaMemcpy(depth, r->impl.depth, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return VSG_ERR_CUDA;
