@@ -115,7 +115,9 @@ def test_cpp_depth_map_generator_matches_binding(cuda, synth_mod, tmp_path):
 
 
 def test_wrong_device_is_refused_before_any_launch(cuda, tmp_path):
-    """vsg_integrate / vsg_scene_reset / vsg_render / vsg_render_hostpose with a
+    """vsg_integrate / vsg_scene_reset / vsg_render / vsg_render_hostpose /
+    vsg_scene_stats / vsg_scene_export / vsg_scene_lookup_blocks /
+    vsg_renderer_record / vsg_renderer_download / vsg_batch_create with a
     handle recorded on another device return VSG_ERR_INVALID_ARG and touch
     nothing (tests/cpp/device_guard.cu)."""
     from test_cpp_dropin_build import build_device_guard
