@@ -36,6 +36,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <new>
 #include <atomic>
 #include <memory>
@@ -612,6 +613,13 @@ int read_blocks(const char* path, float* voxel, std::vector<std::array<int, 3>>*
     FileHeader h{};
     bool ok = std::fread(&h, sizeof(h), 1, f) == 1 && std::memcmp(h.magic, kMagic, 8) == 0 && h.info_bytes == 16 &&
               h.voxel_bytes == 12 && h.n_blocks < (1ull << 32);
+    // the header's block count must be the one the file holds: a truncated or
+    // corrupted file is refused before any buffer is sized from the count
+    if (ok) {
+        std::error_code ec;
+        const uintmax_t size = std::filesystem::file_size(path, ec);
+        ok = !ec && size == sizeof(FileHeader) + h.n_blocks * (16u + 12u * (uint64_t)vsg::kVoxPerBlock);
+    }
     if (ok) {
         coords->resize(h.n_blocks);
         vox->resize(h.n_blocks * vsg::kVoxPerBlock);

@@ -110,6 +110,36 @@ def test_store_rejects_bad_files(tmp_path):
         vsg.Store((0.0, 1.0, 1.0))
 
 
+def test_store_refuses_files_whose_size_disagrees_with_their_header(tmp_path):
+    """A checkpoint whose header counts more (or fewer) blocks than the file
+    holds is refused before any buffer is sized from the count, and the store
+    is left as it was: a truncated file, a header claiming 2^31 blocks over a
+    one-block body, and trailing bytes."""
+    import vsg
+
+    rng = np.random.default_rng(9)
+    coords, vox = _blocks(rng, 20)
+    good = str(tmp_path / "good.vsgb")
+    _file(good, coords, vox, 0.004)
+    raw = open(good, "rb").read()
+    cases = {
+        "truncated": raw[:-1],
+        "huge_count": raw[:16] + struct.pack("<Q", 1 << 31) + raw[24:32] + raw[32:32 + 16] +
+        raw[32 + 16 * len(coords):32 + 16 * len(coords) + 512 * 12],
+        "trailing": raw + b"\0" * 7,
+    }
+    for name, data in cases.items():
+        p = str(tmp_path / f"{name}.vsgb")
+        open(p, "wb").write(data)
+        st = vsg.Store()
+        with pytest.raises(vsg.VsgError):
+            st.load(p)
+        assert st.info()[0] == 0, name
+    st = vsg.Store()
+    st.load(good)
+    assert st.info()[0] == len(coords)
+
+
 def test_store_records_and_counts(oracle_mod):
     """vsg_store_add_records files the reference's streaming records like a
     checkpoint file does (merging repeats), and vsg_store_count reports the
