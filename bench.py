@@ -387,10 +387,12 @@ def run_ours(args):
     for k in ("samples_skipped", "jumps", "singles", "lane_iters", "warp_iters"):
         kern["render"][k + "_per_frame"] = float(np.mean([p["render_" + k] for p in per_frame]))
     dom = max(kern, key=lambda k: kern[k]["ms_per_launch"])
-    traffic = None
+    traffic = issue = None
     try:  # DRAM bytes per launch of the same kernel from one committed ncu capture
         tr = json.load(open(os.path.join(ROOT, "profiles", "roofline_traffic.json")))
         traffic = tr.get("k_" + dom, {}).get("dram_bytes_per_launch")
+        # and, for the issue-bound ray caster, that capture's warp-issue figures
+        issue = tr.get("k_" + dom, {}).get("issue")
     except (OSError, ValueError):
         pass
     peak, peak_kind = measured_peak_hbm()
@@ -407,7 +409,8 @@ def run_ours(args):
             "kernels": kern,
             "frame_bytes": total_bytes, "frame_gbps": total_bytes * fps / world / 1e9,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
-                         "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind},
+                         "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         **({"issue_from_ncu": issue} if issue else {})},
             "clocks": clk.summary()}
     # side measurements after the timed step; a failure is recorded in the
     # line instead of losing it
