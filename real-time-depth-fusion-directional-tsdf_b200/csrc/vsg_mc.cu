@@ -272,6 +272,8 @@ int vsg_mc_run(vsg_scene* s, vsg_mc_output* m, float iso, float voxel_size, vsg_
 
 int vsg_mc_triangle_count(const vsg_mc_output* m, int64_t* count) {
     if (!m || !count) return VSG_ERR_INVALID_ARG;
+    int dev = -1;  // the synchronisation below waits for the current device only
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != m->impl.device) return VSG_ERR_INVALID_ARG;
     if (cudaDeviceSynchronize() != cudaSuccess) return VSG_ERR_CUDA;
     vsg::McCounters c{};
     if (cudaMemcpy(&c, m->impl.ctr, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return VSG_ERR_CUDA;

@@ -254,6 +254,8 @@ int vsg_extract_points(vsg_scene* s, vsg_points* m, float min_sdf, float max_sdf
 
 int vsg_points_count(const vsg_points* m, int64_t* count) {
     if (!m || !count) return VSG_ERR_INVALID_ARG;
+    int dev = -1;  // the synchronisation below waits for the current device only
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != m->impl.device) return VSG_ERR_INVALID_ARG;
     if (cudaDeviceSynchronize() != cudaSuccess) return VSG_ERR_CUDA;
     vsg::PtCounters c{};
     if (cudaMemcpy(&c, m->impl.ctr, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) return VSG_ERR_CUDA;
