@@ -265,10 +265,18 @@ def ref_gpu_measure(frames, K) -> dict:
     return res
 
 
+def headline_config(args, world: int) -> dict:
+    """The headline workload's `config`, the same dict on both arms."""
+    return {"workload": WORKLOAD, "frames_per_step": args.frames,
+            "l2": "inputs larger than L2 (30 resident frames, 250 MB per step)",
+            "parallelism": f"replicas{world}"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     frames, K = make_stream(args)
     res, wall = [], []
     for i in range(args.warmup + args.steps):
@@ -284,9 +292,10 @@ def run_reference(args):
     line = {"metric": METRIC, "value": v, "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.median(wall), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "frames": args.frames, "sample": r["sample"],
-                       "extrapolated": "frames/s of the sample scaled from its ray-cast rows to full frames",
-                       "ms_per_full_frame": 1000.0 / v},
+            "config": headline_config(args, world),
+            "sampling": {"sample": r["sample"],
+                         "extrapolated": "frames/s of the sample scaled from its ray-cast rows to full frames",
+                         "ms_per_full_frame": 1000.0 / v},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "frames/s", "cores": r["cores"], "kind": "port",
                              "cpu": r["cpu"], "sample": r["sample"]},
@@ -402,9 +411,7 @@ def run_ours(args):
     line = {"metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "frames_per_step": args.frames,
-                       "l2": "inputs larger than L2 (30 resident frames, 250 MB per step)",
-                       "parallelism": f"replicas{world}", "mpix_per_s": fps * npx / 1e6},
+            "config": headline_config(args, world), "mpix_per_s": fps * npx / 1e6,
             "gpu_launches": launches_per_step * args.steps,
             "kernels": kern,
             "frame_bytes": total_bytes, "frame_gbps": total_bytes * fps / world / 1e9,

@@ -35,6 +35,11 @@ def test_reference_arm_prints_one_contract_line():
     assert e2e["value"] == line["value"] and e2e["unit"] == line["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
     assert line["config"]["workload"].startswith("tabletop 30x640x480")
+    # the same config dict as the product arm's line (bench.headline_config)
+    assert line["config"] == {"workload": line["config"]["workload"], "frames_per_step": 30,
+                              "l2": "inputs larger than L2 (30 resident frames, 250 MB per step)",
+                              "parallelism": "replicas1"}
+    assert line["sampling"]["sample"] == cb["sample"]
 
 
 def test_reference_arm_other_ranks_exit_quietly():
